@@ -1,0 +1,66 @@
+"""Shared pytest configuration.
+
+Tests marked ``gpu`` need a CUDA device and the built library; everything else
+runs on CPU (``pytest -m "not gpu"``).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU and the built sm_100a library")
+
+
+@pytest.fixture
+def rng() -> np.random.Generator:
+    return np.random.default_rng(seed=42)
+
+
+def load_motion_case(name):
+    """(arrays, meta) for a golden getMotion case."""
+    import json
+
+    with open(os.path.join(GOLDEN, "motion_cases.json")) as fh:
+        meta = json.load(fh)[name]
+    arrays = dict(np.load(os.path.join(GOLDEN, f"motion_{name}.npz")))
+    return arrays, meta
+
+
+def motion_case_names():
+    import json
+
+    with open(os.path.join(GOLDEN, "motion_cases.json")) as fh:
+        return sorted(json.load(fh))
+
+
+def option_from_case(arrays, meta):
+    return {
+        "mask_ref": arrays["mask_ref"].copy(),
+        "mask_mov": arrays["mask_mov"].copy(),
+        "layer": meta["layer"],
+        "iter": meta["iter"],
+        "r": meta["r"],
+        "zRatio": meta["zRatio"],
+        "movRange": meta["movRange"],
+        "motion": arrays.get("motion_init"),
+        "smoothPenalty": meta["smoothPenalty"],
+        "tol": meta["tol"],
+        "save_ite": 100,
+    }
+
+
+def updates_per_layer(arrays, meta):
+    """Number of motion updates the reference performed at each layer."""
+    return {l: len(arrays[f"layer_{l}/max_diff_motion"]) for l in range(meta["layer"] + 1)}

@@ -1,0 +1,179 @@
+"""Generate golden fixtures by running the reference package itself.
+
+Run in a container where the reference checkout is available:
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+It imports the reference's NumPy path (``wholistic_registration.utils``) through
+a stub top-level package, because the package ``__init__`` pulls in I/O
+libraries that the hot path does not need.  Outputs are written next to this
+script as compressed ``.npz`` files and committed; the GPU box never reads the
+reference.
+
+Every array is in the reference's internal (x, y, z) layout.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from wholistic_registration_b200 import synthetic  # noqa: E402
+
+
+def load_reference(root):
+    src = os.path.join(root, "src", "wholistic_registration")
+    if "wholistic_registration" not in sys.modules:
+        pkg = types.ModuleType("wholistic_registration")
+        pkg.__path__ = [src]
+        sys.modules["wholistic_registration"] = pkg
+    mods = {}
+    for name in ("calFlow3d_Wei_v1", "imresize", "preprocess", "calculate"):
+        mods[name] = importlib.import_module(f"wholistic_registration.utils.{name}")
+    return mods
+
+
+def _pair_xyz(zyx, seed, n_blobs, max_disp, drift=0.0):
+    tmpl, mov, field = synthetic.make_pair(zyx, seed, n_blobs=n_blobs, max_disp=max_disp, drift=drift)
+    t = tmpl.to(dtype=__import__("torch").int32).numpy().astype(np.uint16).transpose(2, 1, 0)
+    m = mov.to(dtype=__import__("torch").int32).numpy().astype(np.uint16).transpose(2, 1, 0)
+    f = field.numpy().transpose(2, 1, 0, 3)
+    return np.ascontiguousarray(t), np.ascontiguousarray(m), np.ascontiguousarray(f)
+
+
+# name: (z, y, x), seed, blobs, max_disp, r, layer, iter, zRatio, tol, raw penalty, mask kind, init
+MOTION_CASES = {
+    "tiny_r1_l0": ((4, 24, 24), 1, 40, (1.5, 1.5, 0.5), 1, 0, 5, 1.0, 1e-3, 0.08, "none", False),
+    "small_r2_l1": ((6, 48, 48), 2, 120, (2.0, 2.0, 0.8), 2, 1, 10, 1.0, 1e-3, 0.08, "none", False),
+    "mask_r3_l1_z2": ((8, 64, 64), 3, 200, (2.5, 2.5, 1.0), 3, 1, 10, 2.0, 1e-3, 0.08, "ellipse", False),
+    "init_r4_l2": ((5, 64, 48), 4, 150, (3.0, 3.0, 1.0), 4, 2, 10, 1.0, 1e-4, 0.05, "none", True),
+    "ragged_r3_l2": ((6, 70, 66), 5, 200, (3.0, 2.0, 1.0), 3, 2, 10, 1.0, 1e-3, 0.08, "ellipse", False),
+    "twomask_r2_l1_z5": ((6, 40, 56), 6, 120, (2.0, 2.0, 0.5), 2, 1, 8, 5.0, 1e-3, 0.08, "two", False),
+    "iter1_r2_l1": ((4, 32, 32), 7, 60, (1.0, 1.0, 0.5), 2, 1, 1, 1.0, 1e-3, 0.08, "none", False),
+    "r5_l2_big": ((8, 96, 96), 8, 400, (4.0, 4.0, 1.5), 5, 2, 10, 1.0, 1e-3, 0.08, "none", False),
+}
+
+
+def make_motion_cases(ref, out_dir):
+    cf3 = ref["calFlow3d_Wei_v1"]
+    prep = ref["preprocess"]
+    index = {}
+    for name, (zyx, seed, nb, md, r, layer, it, zr, tol, spr, mk, use_init) in MOTION_CASES.items():
+        tmpl, mov, field = _pair_xyz(zyx, seed, nb, md)
+        shape = tmpl.shape
+        rng = np.random.default_rng(seed + 1000)
+        if mk == "none":
+            mref = np.zeros(shape, bool)
+            mmov = np.zeros(shape, bool)
+        elif mk == "ellipse":
+            inc = synthetic.ellipsoid_inclusion(zyx, 0.7).numpy().transpose(2, 1, 0)
+            mref = ~inc
+            mmov = ~inc
+        else:
+            mref = np.zeros(shape, bool)
+            mref[: shape[0] // 4, :, :] = True
+            mmov = rng.uniform(size=shape) > 0.97
+        opt_mask = {"mask_ref": mref}
+        factor = prep.getSmPnltNormFctr(tmpl.astype(np.float64), opt_mask)
+        init = None
+        if use_init:
+            init = (0.5 * field + rng.normal(scale=0.1, size=field.shape)).astype(np.float32)
+        option = {
+            "mask_ref": mref.copy(), "mask_mov": mmov.copy(), "layer": layer, "iter": it, "r": r,
+            "zRatio": zr, "movRange": 5.0, "motion": init, "smoothPenalty": float(factor * spr),
+            "tol": tol, "save_ite": 100,
+        }
+        motion, err, coords, log = cf3.getMotion(mov.copy(), tmpl.copy(), option)
+        warped = cf3.correctMotion(mov.astype(np.float32), motion)
+        rec = {
+            "mov": mov, "ref": tmpl, "mask_ref": mref, "mask_mov": mmov,
+            "motion": motion.astype(np.float32), "warped": warped.astype(np.float32),
+            "current_error": np.float64(err), "penalty_factor": np.float64(factor),
+        }
+        if init is not None:
+            rec["motion_init"] = init
+        meta = {"layer": layer, "iter": it, "r": r, "zRatio": zr, "movRange": 5.0, "tol": tol,
+                "smoothPenalty": float(factor * spr), "smoothPenalty_raw": spr}
+        for lk, lv in log.items():
+            for key in ("diffError", "penaltyError", "currentError", "max_diff_motion"):
+                rec[f"{lk}/{key}"] = np.asarray(lv[key], dtype=np.float64)
+        np.savez_compressed(os.path.join(out_dir, f"motion_{name}.npz"), **rec)
+        index[name] = meta
+        counts = [len(v["currentError"]) for v in log.values()]
+        print(f"{name}: shape {shape} error {err:.6f} evals/level {counts}")
+    with open(os.path.join(out_dir, "motion_cases.json"), "w") as fh:
+        json.dump(index, fh, indent=1, sort_keys=True)
+
+
+def make_primitive_cases(ref, out_dir):
+    imr = ref["imresize"]
+    cf3 = ref["calFlow3d_Wei_v1"]
+    calc = ref["calculate"]
+    rng = np.random.default_rng(123)
+    rec = {}
+    vol = rng.uniform(0, 4000, (37, 50, 5))
+    rec["resize_in"] = vol
+    for i, shp in enumerate([(18, 25, 5), (9, 12, 5), (4, 6, 5), (37, 50, 5)]):
+        rec[f"resize_bicubic_{i}"] = imr.imresize(vol, output_shape=shp)
+    u16 = rng.integers(0, 65535, (33, 20, 4)).astype(np.uint16)
+    rec["resize_u16_in"] = u16
+    rec["resize_u16_out"] = imr.imresize(u16, output_shape=(16, 10, 4))
+    u8 = rng.integers(0, 255, (21, 18, 3)).astype(np.uint8)
+    rec["resize_u8_in"] = u8
+    rec["resize_u8_out"] = imr.imresize(u8, output_shape=(10, 9, 3))
+    fld = rng.normal(size=(18, 25, 5)).astype(np.float32)
+    rec["resize_bilinear_in"] = fld
+    rec["resize_bilinear_out"] = imr.imresize(fld, output_shape=(37, 50, 5), method="bilinear")
+    mask = np.zeros((40, 36, 4), np.float32)
+    mask[10:25, 5:20, :] = 1
+    rec["resize_mask_in"] = mask
+    rec["resize_mask_out"] = imr.imresize(mask, output_shape=(10, 9, 4))
+
+    data = rng.uniform(0, 1000, (40, 32, 6)).astype(np.float32)
+    motion = (rng.normal(size=(40, 32, 6, 3)) * 2.5).astype(np.float32)
+    motion[0, 0, 0] = (-50, 3, 2)
+    motion[-1, -1, -1] = (40, -60, 9)
+    rec["warp_in"] = data
+    rec["warp_motion"] = motion
+    rec["warp_out"] = cf3.correctMotion(data, motion)
+
+    comps = [rng.normal(size=(5, 4, 3)) for _ in range(9)]
+    spd = np.abs(rng.normal(size=(5, 4, 3))) * 3
+    comps[0] = comps[0] ** 2 + spd
+    comps[3] = comps[3] ** 2 + spd
+    comps[5] = comps[5] ** 2 + spd
+    nei = rng.normal(size=(5, 4, 3, 3)).astype(np.float32)
+    for i, c in enumerate(comps):
+        rec[f"solve_in_{i}"] = c.copy()
+    rec["solve_nei"] = nei
+    rec["solve_out"] = cf3.getFlow3_withPenalty6(*[c.copy() for c in comps], 0.7, nei)
+    cpm = rng.normal(size=(6, 5, 4, 3)).astype(np.float32)
+    rec["neidiff_in"] = cpm
+    rec["neidiff_out"] = cf3.getNeiDiff(cpm, 1)
+    a = rng.normal(size=(9, 7, 3))
+    rec["box_in"] = a
+    rec["box_out_5x3"] = calc.imfilter(a, np.ones((5, 3, 1)), "replicate", "same", "corr")
+    np.savez_compressed(os.path.join(out_dir, "primitives.npz"), **rec)
+    print("primitives written")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    ref = load_reference(args.ref)
+    make_primitive_cases(ref, HERE)
+    make_motion_cases(ref, HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,87 @@
+"""The CPU oracle against fixtures produced by running the reference itself."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_motion_case, motion_case_names, option_from_case
+from oracle import lk_oracle as O
+
+PRIM = os.path.join(GOLDEN, "primitives.npz")
+
+
+@pytest.fixture(scope="module")
+def prim():
+    return dict(np.load(PRIM))
+
+
+def test_imresize_bicubic_matches_reference(prim):
+    vol = prim["resize_in"]
+    for i, shp in enumerate([(18, 25, 5), (9, 12, 5), (4, 6, 5), (37, 50, 5)]):
+        np.testing.assert_allclose(O.imresize(vol, shp), prim[f"resize_bicubic_{i}"], rtol=0, atol=1e-9)
+
+
+def test_imresize_integer_and_mask_inputs(prim):
+    np.testing.assert_allclose(O.imresize(prim["resize_u16_in"], (16, 10, 4)), prim["resize_u16_out"], atol=1e-9)
+    out8 = O.imresize(prim["resize_u8_in"], (10, 9, 3))
+    assert out8.dtype == np.uint8
+    np.testing.assert_array_equal(out8, prim["resize_u8_out"])
+    m = O.imresize(prim["resize_mask_in"], (10, 9, 4))
+    np.testing.assert_allclose(m, prim["resize_mask_out"], atol=1e-12)
+    np.testing.assert_array_equal(m > 0, prim["resize_mask_out"] > 0)
+
+
+def test_imresize_bilinear_upsample(prim):
+    out = O.imresize(prim["resize_bilinear_in"], (37, 50, 5), method="bilinear")
+    np.testing.assert_allclose(out, prim["resize_bilinear_out"], atol=1e-12)
+
+
+def test_correct_motion_matches_reference(prim):
+    out = O.correct_motion(prim["warp_in"], prim["warp_motion"])
+    assert out.dtype == np.float32
+    np.testing.assert_array_equal(out, prim["warp_out"])
+
+
+def test_solve_and_neighbour_difference(prim):
+    comps = [prim[f"solve_in_{i}"] for i in range(9)]
+    keys = ["xx", "xy", "xz", "yy", "yz", "zz", "xt", "yt", "zt"]
+    v = O.solve_flow_with_penalty(dict(zip(keys, comps)), 0.7, prim["solve_nei"])
+    np.testing.assert_allclose(v, prim["solve_out"], rtol=1e-10, atol=1e-12)
+    # the adjugate solve is a linear solve: check against numpy on one CP
+    a = np.array([[comps[0][0, 0, 0] + 0.7, comps[1][0, 0, 0], comps[2][0, 0, 0]],
+                  [comps[1][0, 0, 0], comps[3][0, 0, 0] + 0.7, comps[4][0, 0, 0]],
+                  [comps[2][0, 0, 0], comps[4][0, 0, 0], comps[5][0, 0, 0] + 0.7]])
+    b = np.array([comps[6][0, 0, 0], comps[7][0, 0, 0], comps[8][0, 0, 0]]) + prim["solve_nei"][0, 0, 0]
+    np.testing.assert_allclose(v[0, 0, 0], np.linalg.solve(a, b), rtol=1e-9)
+    nd = O.get_nei_diff(prim["neidiff_in"])
+    np.testing.assert_allclose(nd, prim["neidiff_out"], rtol=0, atol=2e-7)
+
+
+def test_box_filter(prim):
+    np.testing.assert_allclose(O.box_filter_nearest(prim["box_in"], 5, 3), prim["box_out_5x3"], atol=1e-12)
+
+
+@pytest.mark.parametrize("name", motion_case_names())
+def test_get_motion_matches_reference(name):
+    arrays, meta = load_motion_case(name)
+    option = option_from_case(arrays, meta)
+    motion, err, coords, log = O.get_motion(arrays["mov"], arrays["ref"], option)
+    for l in range(meta["layer"] + 1):
+        key = f"layer_{l}"
+        assert len(log[key]["currentError"]) == len(arrays[f"{key}/currentError"]), key
+        np.testing.assert_allclose(log[key]["currentError"], arrays[f"{key}/currentError"], rtol=1e-6)
+        np.testing.assert_allclose(log[key]["max_diff_motion"], arrays[f"{key}/max_diff_motion"], atol=1e-5)
+    assert np.abs(motion - arrays["motion"]).max() < 1e-4
+    np.testing.assert_allclose(err, float(arrays["current_error"]), rtol=1e-6)
+    warped = O.correct_motion(arrays["mov"].astype(np.float32), arrays["motion"])
+    # float64 trilinear rounded to float32: summation order may move 1 ulp
+    np.testing.assert_allclose(warped, arrays["warped"], rtol=1e-6, atol=0)
+
+
+def test_penalty_factor():
+    arrays, meta = load_motion_case("mask_r3_l1_z2")
+    f = O.smooth_penalty_norm_factor(arrays["ref"].astype(np.float64), arrays["mask_ref"])
+    np.testing.assert_allclose(f, float(arrays["penalty_factor"]), rtol=1e-12)
