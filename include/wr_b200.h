@@ -1,0 +1,176 @@
+/*
+ * wr_b200.h - C ABI of the B200-native pyramid Lucas-Kanade registration path.
+ *
+ * The functions below replace, one for one, the reference package's
+ * registration entry points (paths relative to src/wholistic_registration/):
+ *
+ *   wr_lk_register       utils/calFlow3d_Wei_v1.py:295-673   getMotion(dat_mov, dat_ref, option)
+ *   wr_warp_trilinear    utils/calFlow3d_Wei_v1.py:676-706   correctMotion(data_raw, motion_field)
+ *   wr_penalty_factor    utils/preprocess.py:42-66           getSmPnltNormFctr(dat_ref, option)
+ *   wr_resize_table      utils/imresize.py:60-82             contributions(...) (host, no GPU needed)
+ *
+ * Conventions
+ *   - Volumes are C-contiguous (z, y, x): x is the fastest axis.  The reference
+ *     indexes the same memory as (x, y, z) after its (2, 1, 0) transpose
+ *     (utils/registration.py:251,313), so "axis 0" there is x here.
+ *   - Motion fields are (z, y, x, 3) float32 with [...,0] = dx, [...,1] = dy,
+ *     [...,2] = dz: component c displaces axis c, exactly the reference's
+ *     field transposed by (2, 1, 0, 3) (utils/registration.py:346).
+ *   - Exclusion masks are (z, y, x) uint8, nonzero = excluded (outlier), the
+ *     polarity of option["mask_ref"] / option["mask_mov"].  NULL = nothing
+ *     excluded.
+ *   - All data pointers are device pointers owned by the caller; work buffers
+ *     come from the caller too (see wr_lk_workspace_size).  No entry point
+ *     allocates or keeps global state, so calls on different streams with
+ *     different workspaces may run concurrently.
+ *   - Return codes: 0 = ok, > 0 = invalid argument (WR_E_*), < 0 = CUDA
+ *     error (negated cudaError_t).  A message for the last failure on the
+ *     calling thread is available from wr_last_error().
+ */
+#ifndef WR_B200_H
+#define WR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WR_API __attribute__((visibility("default")))
+#else
+#define WR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WR_ABI_VERSION 1
+#define WR_MAX_LEVELS 8
+#define WR_MAX_ITERS 64
+
+/* element types of input volumes */
+enum {
+  WR_U8 = 1,
+  WR_U16 = 2,
+  WR_F32 = 3
+};
+
+/* argument errors */
+enum {
+  WR_OK = 0,
+  WR_E_NULL = 1,        /* a required pointer is NULL */
+  WR_E_SHAPE = 2,       /* shapes disagree or are out of range */
+  WR_E_PARAM = 3,       /* a parameter is out of range */
+  WR_E_DTYPE = 4,       /* unsupported element type */
+  WR_E_WORKSPACE = 5,   /* workspace too small or misaligned */
+  WR_E_NOCP = 6         /* some pyramid level has no control point */
+};
+
+/* storage precision of pyramid levels inside the solver */
+enum {
+  WR_PREC_F32 = 0,   /* plain path: levels, gradients and warps in float32 */
+  WR_PREC_F16 = 1,   /* mixed: levels and gradients stored as float16 */
+  WR_PREC_BF16 = 2   /* mixed: levels and gradients stored as bfloat16 */
+};
+
+/* A volume: device pointer, element type and (z, y, x) extent. */
+typedef struct {
+  const void* data;
+  int32_t dtype;
+  int32_t nz, ny, nx;
+} WrVolume;
+
+/*
+ * Solver parameters: the keys getMotion reads from its option dict
+ * (utils/calFlow3d_Wei_v1.py:318-324,429-431; defaults in utils/__init__.py:79-95).
+ */
+typedef struct {
+  int32_t layer;          /* option["layer"]: levels = layer + 1 */
+  int32_t iter;           /* option["iter"]: max error evaluations per level */
+  int32_t r;              /* option["r"]: patch (2r+1) x (2r+1) x 1, CP stride 2r+1 */
+  float zRatio;           /* option["zRatio"] at full resolution */
+  float movRange;         /* option["movRange"]: max CP update length */
+  double smoothPenalty;   /* option["smoothPenalty"], already normalised */
+  double tol;             /* option["tol"]: |delta error| stopping threshold */
+  int32_t precision;      /* WR_PREC_* */
+  int32_t reserved;
+  /* -1: the reference's stopping rules; n >= 0: perform exactly n motion
+     updates at that level (replays another run's iteration counts) */
+  int32_t forced_updates[WR_MAX_LEVELS];
+} WrLKParams;
+
+/* Per-call statistics (device memory), the scalar part of getMotion's error_log. */
+typedef struct {
+  int32_t levels;                         /* layer + 1 */
+  int32_t evals[WR_MAX_LEVELS];           /* error evaluations per level, index = layer */
+  int32_t updates[WR_MAX_LEVELS];         /* motion updates per level */
+  int32_t nan_solves;                     /* CP solves whose result was NaN (set to 0) */
+  int32_t pad;
+  double current_error;                   /* last evaluated error (returned by getMotion) */
+  double diff_error[WR_MAX_LEVELS][WR_MAX_ITERS];
+  double penalty_error[WR_MAX_LEVELS][WR_MAX_ITERS];
+  double max_diff_motion[WR_MAX_LEVELS][WR_MAX_ITERS];
+} WrLKStats;
+
+/* ABI version of the loaded library (WR_ABI_VERSION). */
+WR_API int wr_abi_version(void);
+
+/* Message describing the last failed call on this thread ("" if none). */
+WR_API const char* wr_last_error(void);
+
+/*
+ * Bytes of device workspace wr_lk_register needs for this volume shape and
+ * parameters.  Host-only; needs no GPU.  Replaces the device arrays getMotion
+ * allocates per level (utils/calFlow3d_Wei_v1.py:346-439).
+ */
+WR_API int wr_lk_workspace_size(int32_t nz, int32_t ny, int32_t nx, const WrLKParams* p,
+                         size_t* bytes);
+
+/*
+ * Register `mov` onto `ref`: getMotion (utils/calFlow3d_Wei_v1.py:295-673).
+ *   mov, ref       : same shape; WR_U8, WR_U16 or WR_F32 elements
+ *   excl_mask_mov  : option["mask_mov"], (z,y,x) uint8 or NULL
+ *   excl_mask_ref  : option["mask_ref"], (z,y,x) uint8 or NULL
+ *   motion_init    : option["motion"], (z,y,x,3) float32 or NULL
+ *   motion_out     : (z,y,x,3) float32 result
+ *   stats          : device WrLKStats or NULL
+ *   workspace      : >= wr_lk_workspace_size bytes, 256-byte aligned
+ * Asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream).
+ */
+WR_API int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                   const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                   float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/*
+ * Pull-warp `src` through `motion`: out(p) = src(p + motion(p)), trilinear,
+ * edge-replicated, float32 result (correctMotion, utils/calFlow3d_Wei_v1.py:676-706).
+ *   motion : (z,y,x,3) float32 device; out : (z,y,x) float32 device.
+ */
+WR_API int wr_warp_trilinear(const WrVolume* src, const float* motion, float* out, void* stream);
+
+/*
+ * Smoothness-penalty normalisation factor of `ref` over voxels not excluded by
+ * excl_mask_ref (getSmPnltNormFctr, utils/preprocess.py:42-66).  Writes one
+ * double to the device pointer `factor_out`.
+ */
+WR_API int wr_penalty_factor(const WrVolume* ref, const uint8_t* excl_mask_ref, double* factor_out,
+                      void* scratch, size_t scratch_bytes, void* stream);
+
+/* Scratch bytes wr_penalty_factor needs for this shape. */
+WR_API int wr_penalty_factor_scratch(int32_t nz, int32_t ny, int32_t nx, size_t* bytes);
+
+/*
+ * Resize tap table along one axis, host-side (contributions,
+ * utils/imresize.py:60-82), before zero-column removal: for each of `out_len`
+ * outputs, `*taps` candidate taps (weights float64 and source indices).
+ * method 0 = bicubic (antialiased when shrinking), 1 = bilinear.
+ * Call with weights == NULL to get `*taps`.
+ */
+WR_API int wr_resize_table(int32_t in_len, int32_t out_len, int32_t method, double* weights,
+                    int32_t* indices, int32_t* taps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WR_B200_H */

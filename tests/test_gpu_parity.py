@@ -1,0 +1,168 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's outputs.
+
+Bars (see the package docs): displacement within 1e-3 voxel max-abs and
+warped volumes within 1e-4 relative L2 of the reference; when the stopping
+rules flip on a borderline decision the per-level update counts of the
+reference run are replayed (``forced_updates``) and the same bars apply.
+"""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_motion_case, motion_case_names, option_from_case, updates_per_layer
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+FLOW_TOL = 1e-3     # voxel, max-abs
+WARP_TOL = 1e-4     # relative L2
+
+
+def _cf3():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from wholistic_registration_b200 import calFlow3d_Wei_v1
+
+    return calFlow3d_Wei_v1
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("name", motion_case_names())
+def test_get_motion_matches_reference_fixture(name):
+    cf3 = _cf3()
+    arrays, meta = load_motion_case(name)
+    option = option_from_case(arrays, meta)
+    motion, err, coords, log = cf3.getMotion(arrays["mov"], arrays["ref"], option)
+    ref_counts = {l: len(arrays[f"layer_{l}/currentError"]) for l in range(meta["layer"] + 1)}
+    counts = {l: len(log[f"layer_{l}"]["currentError"]) for l in range(meta["layer"] + 1)}
+    if counts != ref_counts:
+        option = option_from_case(arrays, meta)
+        option["forced_updates"] = updates_per_layer(arrays, meta)
+        motion, err, coords, log = cf3.getMotion(arrays["mov"], arrays["ref"], option)
+    assert motion.shape == arrays["motion"].shape and motion.dtype == np.float32
+    dmax = float(np.abs(motion - arrays["motion"]).max())
+    assert dmax <= FLOW_TOL, f"{name}: max |dflow| {dmax:.3g} (counts {counts} vs {ref_counts})"
+    for l in range(meta["layer"] + 1):
+        np.testing.assert_allclose(log[f"layer_{l}"]["currentError"][:len(arrays[f"layer_{l}/currentError"])],
+                                   arrays[f"layer_{l}/currentError"][:len(log[f"layer_{l}"]["currentError"])],
+                                   rtol=1e-4)
+    warped = cf3.correctMotion(arrays["mov"].astype(np.float32), motion)
+    assert rel_l2(warped, arrays["warped"]) <= WARP_TOL
+
+
+def test_stopping_rules_reach_reference_counts():
+    """Without replay, the device-side stopping rules give the reference's
+    per-level iteration counts on most fixtures."""
+    cf3 = _cf3()
+    same = 0
+    names = motion_case_names()
+    for name in names:
+        arrays, meta = load_motion_case(name)
+        _, _, _, log = cf3.getMotion(arrays["mov"], arrays["ref"], option_from_case(arrays, meta))
+        same += all(len(log[f"layer_{l}"]["currentError"]) == len(arrays[f"layer_{l}/currentError"])
+                    for l in range(meta["layer"] + 1))
+    assert same >= len(names) - 1
+
+
+def test_correct_motion_matches_reference_fixture():
+    cf3 = _cf3()
+    prim = dict(np.load(os.path.join(GOLDEN, "primitives.npz")))
+    out = cf3.correctMotion(prim["warp_in"], prim["warp_motion"])
+    assert out.dtype == np.float32
+    np.testing.assert_allclose(out, prim["warp_out"], rtol=2e-7, atol=1e-4)
+    u16 = np.clip(prim["warp_in"], 0, 65535).astype(np.uint16)
+    np.testing.assert_allclose(cf3.correctMotion(u16, prim["warp_motion"]),
+                               cf3.correctMotion(u16.astype(np.float32), prim["warp_motion"]), rtol=0, atol=0)
+
+
+def test_penalty_factor_matches_reference_fixture():
+    _cf3()
+    from wholistic_registration_b200 import penalty_factor
+
+    arrays, _ = load_motion_case("mask_r3_l1_z2")
+    ref = torch.from_numpy(np.ascontiguousarray(arrays["ref"].astype(np.float32).transpose(2, 1, 0))).cuda()
+    mref = torch.from_numpy(np.ascontiguousarray(arrays["mask_ref"].transpose(2, 1, 0))).cuda()
+    f = float(penalty_factor(ref, mref))
+    np.testing.assert_allclose(f, float(arrays["penalty_factor"]), rtol=1e-12)
+
+
+def _oracle_case(shape_zyx, seed, r, layer, zratio=1.0, mask=False, max_disp=(3.0, 3.0, 1.0), blobs=600):
+    from oracle import lk_oracle as O
+    from wholistic_registration_b200 import synthetic
+
+    tmpl, mov, field = synthetic.make_pair(shape_zyx, seed, n_blobs=blobs, max_disp=max_disp)
+    t = tmpl.to(torch.int32).numpy().astype(np.uint16).transpose(2, 1, 0)
+    m = mov.to(torch.int32).numpy().astype(np.uint16).transpose(2, 1, 0)
+    shape = t.shape
+    if mask:
+        excl = ~synthetic.ellipsoid_inclusion(shape_zyx, 0.7).numpy().transpose(2, 1, 0)
+    else:
+        excl = np.zeros(shape, bool)
+    factor = O.smooth_penalty_norm_factor(t.astype(np.float64), excl)
+    option = {"mask_ref": excl, "mask_mov": excl, "layer": layer, "iter": 10, "r": r, "zRatio": zratio,
+              "movRange": 5.0, "motion": None, "smoothPenalty": float(factor * 0.08), "tol": 1e-3, "save_ite": 100}
+    return t, m, option
+
+
+@pytest.mark.parametrize("shape,r,layer,zr,mask", [
+    ((16, 128, 128), 8, 2, 1.0, False),
+    ((12, 96, 160), 5, 2, 2.0, True),
+])
+def test_against_oracle_medium(shape, r, layer, zr, mask):
+    cf3 = _cf3()
+    from oracle import lk_oracle as O
+
+    t, m, option = _oracle_case(shape, 11, r, layer, zr, mask)
+    om, oe, _, olog = O.get_motion(m, t, dict(option))
+    gm, ge, _, glog = cf3.getMotion(m, t, dict(option))
+    ocounts = {l: len(olog[f"layer_{l}"]["max_diff_motion"]) for l in range(layer + 1)}
+    gcounts = {l: len(glog[f"layer_{l}"]["max_diff_motion"]) for l in range(layer + 1)}
+    if ocounts != gcounts:
+        opt = dict(option)
+        opt["forced_updates"] = ocounts
+        gm, ge, _, glog = cf3.getMotion(m, t, opt)
+    assert float(np.abs(gm - om).max()) <= FLOW_TOL
+    w_o = O.correct_motion(m.astype(np.float32), om)
+    w_g = cf3.correctMotion(m.astype(np.float32), gm)
+    assert rel_l2(w_g, w_o) <= WARP_TOL
+
+
+def test_deterministic_and_torch_path():
+    cf3 = _cf3()
+    arrays, meta = load_motion_case("r5_l2_big")
+    option = option_from_case(arrays, meta)
+    a = cf3.getMotion(arrays["mov"], arrays["ref"], dict(option))[0]
+    b = cf3.getMotion(arrays["mov"], arrays["ref"], dict(option))[0]
+    np.testing.assert_array_equal(a, b)
+    mov = torch.from_numpy(arrays["mov"].astype(np.float32)).cuda()
+    ref = torch.from_numpy(arrays["ref"].astype(np.float32)).cuda()
+    c, err, coords, _ = cf3.getMotion(mov, ref, dict(option))
+    assert isinstance(c, torch.Tensor) and c.is_cuda and tuple(c.shape) == a.shape
+    np.testing.assert_array_equal(c.cpu().numpy(), a)
+    grid = np.stack(np.meshgrid(*[np.arange(n, dtype=np.float32) for n in a.shape[:3]], indexing="ij"), -1)
+    np.testing.assert_allclose(np.asarray(coords), a + grid)
+
+
+def test_argument_errors_raise_value_error():
+    cf3 = _cf3()
+    arrays, meta = load_motion_case("tiny_r1_l0")
+    option = option_from_case(arrays, meta)
+    with pytest.raises(ValueError):
+        cf3.getMotion(arrays["mov"][:-1], arrays["ref"], dict(option))
+    bad = dict(option)
+    bad["r"] = 0
+    with pytest.raises(ValueError):
+        cf3.getMotion(arrays["mov"], arrays["ref"], bad)
+    big = dict(option)
+    big["layer"] = 4
+    with pytest.raises(ValueError):
+        cf3.getMotion(arrays["mov"], arrays["ref"], big)

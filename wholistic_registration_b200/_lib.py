@@ -1,0 +1,139 @@
+"""ctypes binding of the C ABI in ``include/wr_b200.h``.
+
+The shared library ``_wr_b200.so`` is built in-tree by
+``wholistic_registration_b200.build``.  Loading fails loudly when it is
+missing: there is no CPU fallback for the registration path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_wr_b200.so")
+
+MAX_LEVELS = 8
+MAX_ITERS = 64
+
+WR_U8, WR_U16, WR_F32 = 1, 2, 3
+WR_PREC_F32, WR_PREC_F16, WR_PREC_BF16 = 0, 1, 2
+
+ERRORS = {
+    1: "WR_E_NULL",
+    2: "WR_E_SHAPE",
+    3: "WR_E_PARAM",
+    4: "WR_E_DTYPE",
+    5: "WR_E_WORKSPACE",
+    6: "WR_E_NOCP",
+}
+
+EXPORTS = (
+    "wr_abi_version",
+    "wr_last_error",
+    "wr_lk_workspace_size",
+    "wr_lk_register",
+    "wr_warp_trilinear",
+    "wr_penalty_factor",
+    "wr_penalty_factor_scratch",
+    "wr_resize_table",
+)
+
+
+class WrVolume(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("nx", ctypes.c_int32),
+    ]
+
+
+class WrLKParams(ctypes.Structure):
+    _fields_ = [
+        ("layer", ctypes.c_int32),
+        ("iter", ctypes.c_int32),
+        ("r", ctypes.c_int32),
+        ("zRatio", ctypes.c_float),
+        ("movRange", ctypes.c_float),
+        ("smoothPenalty", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("precision", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("forced_updates", ctypes.c_int32 * MAX_LEVELS),
+    ]
+
+
+class WrLKStats(ctypes.Structure):
+    _fields_ = [
+        ("levels", ctypes.c_int32),
+        ("evals", ctypes.c_int32 * MAX_LEVELS),
+        ("updates", ctypes.c_int32 * MAX_LEVELS),
+        ("nan_solves", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("current_error", ctypes.c_double),
+        ("diff_error", (ctypes.c_double * MAX_ITERS) * MAX_LEVELS),
+        ("penalty_error", (ctypes.c_double * MAX_ITERS) * MAX_LEVELS),
+        ("max_diff_motion", (ctypes.c_double * MAX_ITERS) * MAX_LEVELS),
+    ]
+
+
+class WrError(RuntimeError):
+    """A C-ABI call returned a nonzero status."""
+
+    def __init__(self, fn, code, msg):
+        kind = ERRORS.get(code, f"CUDA error {-code}" if code < 0 else f"code {code}")
+        super().__init__(f"{fn}: {kind}: {msg}")
+        self.code = code
+
+
+class ArgumentError(WrError, ValueError):
+    """Invalid argument reported by the library (maps to the reference's ValueError)."""
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load the library (once) and declare argument types."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m wholistic_registration_b200.build` "
+                "(the registration path has no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        vp, i32, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_size_t
+        lib.wr_abi_version.restype = ctypes.c_int
+        lib.wr_last_error.restype = ctypes.c_char_p
+        lib.wr_lk_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(WrLKParams), ctypes.POINTER(sz)]
+        lib.wr_lk_register.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), vp, vp,
+                                       ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
+        lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
+        lib.wr_penalty_factor.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp, sz, vp]
+        lib.wr_penalty_factor_scratch.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
+        lib.wr_resize_table.argtypes = [i32, i32, i32, vp, vp, ctypes.POINTER(i32)]
+        for name in EXPORTS:
+            getattr(lib, name).restype = ctypes.c_int if name != "wr_last_error" else ctypes.c_char_p
+        if lib.wr_abi_version() != 1:
+            raise ImportError("wr_b200 ABI version mismatch")
+        _lib = lib
+        return lib
+
+
+def check(fn, code):
+    if code != 0:
+        msg = load().wr_last_error().decode(errors="replace")
+        if code > 0:
+            raise ArgumentError(fn, code, msg)
+        raise WrError(fn, code, msg)
+
+
+def volume(ptr, dtype_code, shape_zyx):
+    nz, ny, nx = (int(s) for s in shape_zyx)
+    return WrVolume(ctypes.c_void_p(ptr), dtype_code, nz, ny, nx)

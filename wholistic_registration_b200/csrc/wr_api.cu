@@ -1,0 +1,548 @@
+// C ABI of the B200 registration path: planning, workspace layout and the
+// launch sequence that replaces getMotion / correctMotion
+// (utils/calFlow3d_Wei_v1.py:295-706 of the reference package).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+
+#include "wr_b200.h"
+#include "wr_kernels.cuh"
+#include "wr_plan.h"
+
+namespace wr {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* msg) {
+  g_last_error = msg ? msg : "";
+  return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return -(int)e;
+}
+
+static size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
+
+struct Alloc {
+  size_t cur = 0;
+  size_t take(size_t bytes) {
+    size_t off = cur;
+    cur = align_up(cur + bytes);
+    return off;
+  }
+};
+
+static int level_extent(int n, int layer) { return (int)((double)n / (double)(1 << layer)); }
+
+// number of k >= 0 with r + k(2r+1) < n - 1 (utils/calFlow3d_Wei_v1.py:434-435)
+static int cp_count(int n, int r, int w) {
+  int span = n - 1 - r;
+  return span > 0 ? (span + w - 1) / w : 0;
+}
+
+int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool has_mmov, bool has_init,
+              Plan* plan, const char** why) {
+  *why = "";
+  if (nz < 1 || ny < 1 || nx < 1) { *why = "volume extents must be positive"; return WR_E_SHAPE; }
+  if ((long long)nz * ny * nx > (1LL << 36)) { *why = "volume too large"; return WR_E_SHAPE; }
+  if (p->layer < 0 || p->layer >= WR_MAX_LEVELS) { *why = "layer out of range [0, 7]"; return WR_E_PARAM; }
+  if (p->iter < 1 || p->iter > WR_MAX_ITERS) { *why = "iter out of range [1, 64]"; return WR_E_PARAM; }
+  if (p->r < 1 || p->r > 48) { *why = "r out of range [1, 48]"; return WR_E_PARAM; }
+  if (!(p->zRatio > 0.f) || !(p->movRange > 0.f)) { *why = "zRatio and movRange must be positive"; return WR_E_PARAM; }
+  if (!(p->smoothPenalty >= 0.0) || !(p->tol >= 0.0)) { *why = "smoothPenalty and tol must be >= 0"; return WR_E_PARAM; }
+  if (p->precision != WR_PREC_F32) { *why = "only WR_PREC_F32 is available in this build"; return WR_E_PARAM; }
+  Plan& P = *plan;
+  memset(&P, 0, sizeof(P));
+  P.nz = nz; P.ny = ny; P.nx = nx;
+  P.levels = p->layer + 1;
+  P.r = p->r; P.w = 2 * p->r + 1; P.iter = p->iter;
+  P.has_mref = has_mref; P.has_mmov = has_mmov; P.has_init = has_init;
+  P.dense_all = p->iter == 1;
+  P.precision = p->precision;
+  Alloc A;
+  size_t tmp_a = 0, tmp_b = 0;
+  for (int l = 0; l < P.levels; ++l) {
+    LevelPlan& L = P.lv[l];
+    L.nx = level_extent(nx, l);
+    L.ny = level_extent(ny, l);
+    L.nz = nz;
+    if (L.nx < 1 || L.ny < 1) { *why = "volume too small for this many pyramid levels"; return WR_E_SHAPE; }
+    L.ncx = cp_count(L.nx, P.r, P.w);
+    L.ncy = cp_count(L.ny, P.r, P.w);
+    if (L.ncx < 1 || L.ncy < 1) { *why = "a pyramid level has no control point (volume too small for r)"; return WR_E_NOCP; }
+    L.ntx = L.ncx + (L.nx > L.ncx * P.w ? 1 : 0);
+    L.nty = L.ncy + (L.ny > L.ncy * P.w ? 1 : 0);
+    L.n = (long long)L.nx * L.ny * L.nz;
+    L.ncp = (long long)L.ncx * L.ncy * L.nz;
+    L.nblk = (long long)L.ntx * L.nty * L.nz;
+    L.zratio_d = (double)p->zRatio / (double)(1 << l);
+    L.zratio = (float)L.zratio_d;
+    double sx = resize_scale(nx, L.nx), sy = resize_scale(ny, L.ny);
+    L.x_first = sx <= sy;
+    L.tx_taps = resize_taps(nx, L.nx);
+    L.ty_taps = resize_taps(ny, L.ny);
+    L.ref = A.take((size_t)L.n * 4);
+    L.movg = A.take((size_t)L.n * 16);
+    L.mbits = A.take((size_t)L.n);
+    L.mmov = A.take((size_t)L.n * 4);
+    L.cp = A.take((size_t)L.ncp * 16);
+    L.sums = A.take((size_t)L.ncp * 12 * 4);
+    L.errpart = A.take((size_t)L.nblk * 8);
+    L.penpart = A.take((size_t)L.nblk * 8);
+    L.dense = (P.dense_all || l == P.levels - 1) ? A.take((size_t)L.n * 16) : 0;
+    L.tx_w = A.take((size_t)L.nx * L.tx_taps * 8);
+    L.tx_i = A.take((size_t)L.nx * L.tx_taps * 4);
+    L.ty_w = A.take((size_t)L.ny * L.ty_taps * 8);
+    L.ty_i = A.take((size_t)L.ny * L.ty_taps * 4);
+    L.ux_w = A.take((size_t)L.nx * 2 * 4);
+    L.ux_i = A.take((size_t)L.nx * 2 * 4);
+    L.uy_w = A.take((size_t)L.ny * 2 * 4);
+    L.uy_i = A.take((size_t)L.ny * 2 * 4);
+    if (l > 0) {
+      size_t first = L.x_first ? (size_t)nz * ny * L.nx : (size_t)nz * L.ny * nx;
+      tmp_a = first > tmp_a ? first : tmp_a;
+      tmp_b = (size_t)L.n > tmp_b ? (size_t)L.n : tmp_b;
+    }
+  }
+  for (int l = 0; l + 1 < P.levels; ++l) {
+    double sx = resize_scale(P.lv[l + 1].nx, P.lv[l].nx), sy = resize_scale(P.lv[l + 1].ny, P.lv[l].ny);
+    P.lv[l].up_x_first = sx <= sy;
+  }
+  {
+    // the initial-field resize of the coarsest level reuses the temporaries
+    const LevelPlan& C = P.lv[P.levels - 1];
+    size_t first = C.x_first ? (size_t)nz * ny * C.nx : (size_t)nz * C.ny * nx;
+    tmp_a = first > tmp_a ? first : tmp_a;
+    tmp_b = (size_t)C.n * 3 > tmp_b ? (size_t)C.n * 3 : tmp_b;
+  }
+  P.tmp_a_bytes = tmp_a * 8;
+  P.tmp_b_bytes = tmp_b * 8;
+  P.tmp_a = A.take(P.tmp_a_bytes);
+  P.tmp_b = A.take(P.tmp_b_bytes);
+  P.state = A.take(sizeof(LKState) + 64);
+  P.total = A.cur;
+  return WR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+
+static int grid_for(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  long long cap = 148LL * 16;
+  if (b < 1) b = 1;
+  return (int)(b < cap ? b : cap);
+}
+
+template <typename T> static T* at_off(void* base, size_t off) {
+  return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+}
+
+static size_t iter_smem(int w) {
+  size_t hh = (size_t)(w + 2) * (w + 2);
+  return 4 * ((hh + 3) & ~size_t(3)) + 16 * (size_t)w * w + 4 * 33 * 10;
+}
+
+// Separable resize of a full-resolution volume to a level:
+// first pass (x or y, by scale order) into tmp, second pass into `out`.
+template <typename Tin, typename A, typename Tout>
+static void resize_to_level(const Plan& P, const LevelPlan& L, void* ws, const Tin* in, int stride, int comp,
+                            A* tmp, Tout* out, cudaStream_t s) {
+  const double* txw = at_off<double>(ws, L.tx_w);
+  const int32_t* txi = at_off<int32_t>(ws, L.tx_i);
+  const double* tyw = at_off<double>(ws, L.ty_w);
+  const int32_t* tyi = at_off<int32_t>(ws, L.ty_i);
+  if (L.x_first) {
+    long long n1 = (long long)P.nz * P.ny * L.nx;
+    k_resample_x<Tin, A, A><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, P.nx, L.nx, txw, txi, L.tx_taps,
+                                                               stride, comp);
+    k_resample_y<A, A, Tout><<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi,
+                                                                 L.ty_taps, 1, 0);
+  } else {
+    long long n1 = (long long)P.nz * L.ny * P.nx;
+    k_resample_y<Tin, A, A><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, L.ny, P.nx, tyw, tyi, L.ty_taps,
+                                                               stride, comp);
+    k_resample_x<A, A, Tout><<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, L.ny, P.nx, L.nx, txw, txi,
+                                                                 L.tx_taps, 1, 0);
+  }
+}
+
+// the same for a uint8 exclusion mask, float64 throughout (bit-exact with the
+// reference's float64 resize, whose result is thresholded at > 0)
+static void resize_mask_to_level(const Plan& P, const LevelPlan& L, void* ws, const uint8_t* in, double* tmp,
+                                 double* out, cudaStream_t s) {
+  const double* txw = at_off<double>(ws, L.tx_w);
+  const int32_t* txi = at_off<int32_t>(ws, L.tx_i);
+  const double* tyw = at_off<double>(ws, L.ty_w);
+  const int32_t* tyi = at_off<int32_t>(ws, L.ty_i);
+  if (L.x_first) {
+    long long n1 = (long long)P.nz * P.ny * L.nx;
+    k_resample_x<uint8_t, double, double><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, P.nx, L.nx, txw,
+                                                                             txi, L.tx_taps, 1, 0);
+    k_resample_y_d<<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi, L.ty_taps);
+  } else {
+    long long n1 = (long long)P.nz * L.ny * P.nx;
+    k_resample_y<uint8_t, double, double><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, L.ny, P.nx, tyw,
+                                                                             tyi, L.ty_taps, 1, 0);
+    k_resample_x_d<<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, L.ny, P.nx, L.nx, txw, txi, L.tx_taps);
+  }
+}
+
+template <typename T>
+static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, const uint8_t* mmov_u8,
+                          const uint8_t* mref_u8, cudaStream_t s) {
+  for (int l = 0; l < P.levels; ++l) {
+    const LevelPlan& L = P.lv[l];
+    float* refl = at_off<float>(ws, L.ref);
+    float4* movg = at_off<float4>(ws, L.movg);
+    float* mmov = at_off<float>(ws, L.mmov);
+    uint8_t* bits = at_off<uint8_t>(ws, L.mbits);
+    if (l == 0) {
+      // scale 1 on every axis: the resize is an exact copy
+      k_to_float<T><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
+      k_pack_movg<T><<<grid_for(L.n), kThreads, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
+      if (mmov_u8) k_u8_to_unit_f<<<grid_for(L.n), kThreads, 0, s>>>(mmov_u8, mmov, L.n);
+      if (mmov_u8 || mref_u8)
+        k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(nullptr, mref_u8, mmov_u8 ? mmov : nullptr, bits, L.nz,
+                                                        L.ny, L.nx);
+      continue;
+    }
+    float* tmpf = at_off<float>(ws, P.tmp_a);
+    float* levf = at_off<float>(ws, P.tmp_b);
+    resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, refl, s);
+    resize_to_level<T, float, float>(P, L, ws, mov, 1, 0, tmpf, levf, s);
+    k_pack_movg<float><<<grid_for(L.n), kThreads, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
+    double* tmpd = at_off<double>(ws, P.tmp_a);
+    double* levd = at_off<double>(ws, P.tmp_b);
+    if (mmov_u8) {
+      resize_mask_to_level(P, L, ws, mmov_u8, tmpd, levd, s);
+      k_d_to_f<<<grid_for(L.n), kThreads, 0, s>>>(levd, mmov, L.n);
+    }
+    if (mref_u8) resize_mask_to_level(P, L, ws, mref_u8, tmpd, levd, s);
+    if (mmov_u8 || mref_u8)
+      k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(mref_u8 ? levd : nullptr, nullptr, mmov_u8 ? mmov : nullptr,
+                                                      bits, L.nz, L.ny, L.nx);
+  }
+}
+
+static CPView cp_view(const Plan& P, const LevelPlan& L, void* ws) {
+  CPView v;
+  v.cp = at_off<float4>(ws, L.cp);
+  v.ncx = L.ncx;
+  v.ncy = L.ncy;
+  v.r = P.r;
+  v.w = P.w;
+  return v;
+}
+
+static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
+  const LevelPlan& L = P.lv[l];
+  FieldSrc f;
+  memset(&f, 0, sizeof(f));
+  f.mode = mode;
+  f.nx = L.nx;
+  f.ny = L.ny;
+  f.cpv = cp_view(P, L, ws);
+  f.dense = L.dense ? at_off<float4>(ws, L.dense) : nullptr;
+  if (l + 1 < P.levels) {
+    const LevelPlan& C = P.lv[l + 1];
+    f.up.src = cp_view(P, C, ws);
+    f.up.src_dense = P.dense_all ? at_off<float4>(ws, C.dense) : nullptr;
+    f.up.src_nx = C.nx;
+    f.up.src_ny = C.ny;
+    f.up.wx = at_off<float>(ws, L.ux_w);
+    f.up.ix = at_off<int32_t>(ws, L.ux_i);
+    f.up.wy = at_off<float>(ws, L.uy_w);
+    f.up.iy = at_off<int32_t>(ws, L.uy_i);
+    f.up.x_first = L.up_x_first;
+  }
+  return f;
+}
+
+template <int MODE>
+static void launch_accumulate(const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
+  if (mask) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lk_accumulate<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lk_accumulate<MODE, true><<<grid, kThreads, smem, s>>>(a);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lk_accumulate<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lk_accumulate<MODE, false><<<grid, kThreads, smem, s>>>(a);
+  }
+}
+
+static void accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
+  switch (mode) {
+    case FIELD_CP: launch_accumulate<FIELD_CP>(a, grid, smem, mask, s); break;
+    case FIELD_UP: launch_accumulate<FIELD_UP>(a, grid, smem, mask, s); break;
+    case FIELD_DENSE: launch_accumulate<FIELD_DENSE>(a, grid, smem, mask, s); break;
+    default: launch_accumulate<FIELD_ZERO>(a, grid, smem, mask, s); break;
+  }
+}
+
+template <int MODE0>
+static void level_first(const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f, bool cp_init,
+                        bool diff, cudaStream_t s) {
+  if (cp_init)
+    k_cp_init<MODE0><<<grid_for(L.ncp), kThreads, 0, s>>>(at_off<float4>(ws, L.cp), f, L.ncx, L.ncy, L.nz, P.r, P.w);
+  if (diff) k_diff_first<MODE0><<<grid_for(L.n), kThreads, 0, s>>>(st, f.cpv, f, L.nx, L.ny, L.nz);
+}
+
+static void first_dispatch(int mode, const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f,
+                           bool cp_init, bool diff, cudaStream_t s) {
+  switch (mode) {
+    case FIELD_UP: level_first<FIELD_UP>(P, L, ws, st, f, cp_init, diff, s); break;
+    case FIELD_DENSE: level_first<FIELD_DENSE>(P, L, ws, st, f, cp_init, diff, s); break;
+    default: level_first<FIELD_ZERO>(P, L, ws, st, f, cp_init, diff, s); break;
+  }
+}
+
+static void build_tables(const Plan& P, void* ws, int* err_flag, cudaStream_t s) {
+  for (int l = 0; l < P.levels; ++l) {
+    const LevelPlan& L = P.lv[l];
+    k_build_table<<<(L.nx + 127) / 128, 128, 0, s>>>(at_off<double>(ws, L.tx_w), at_off<int32_t>(ws, L.tx_i), P.nx,
+                                                      L.nx, RESIZE_BICUBIC, L.tx_taps);
+    k_build_table<<<(L.ny + 127) / 128, 128, 0, s>>>(at_off<double>(ws, L.ty_w), at_off<int32_t>(ws, L.ty_i), P.ny,
+                                                      L.ny, RESIZE_BICUBIC, L.ty_taps);
+    if (l + 1 < P.levels) {
+      const LevelPlan& C = P.lv[l + 1];
+      k_build_up_table<<<(L.nx + 127) / 128, 128, 0, s>>>(at_off<float>(ws, L.ux_w), at_off<int32_t>(ws, L.ux_i),
+                                                           C.nx, L.nx, err_flag);
+      k_build_up_table<<<(L.ny + 127) / 128, 128, 0, s>>>(at_off<float>(ws, L.uy_w), at_off<int32_t>(ws, L.uy_i),
+                                                           C.ny, L.ny, err_flag);
+    }
+  }
+}
+
+// coarsest level's initial field from option["motion"] (z, y, x, 3)
+static void init_field(const Plan& P, void* ws, const float* init, cudaStream_t s) {
+  const LevelPlan& C = P.lv[P.levels - 1];
+  float4* dense = at_off<float4>(ws, C.dense);
+  float* comp = at_off<float>(ws, P.tmp_b);
+  double* tmp = at_off<double>(ws, P.tmp_a);
+  if (P.levels == 1) {
+    // scale 1: exact copy
+    for (int c = 0; c < 3; ++c)
+      k_resample_x<float, double, float><<<grid_for(C.n), kThreads, 0, s>>>(
+          init, comp + (size_t)c * C.n, P.nz, P.ny, P.nx, C.nx, at_off<double>(ws, C.tx_w),
+          at_off<int32_t>(ws, C.tx_i), C.tx_taps, 3, c);
+  } else {
+    for (int c = 0; c < 3; ++c)
+      resize_to_level<float, double, float>(P, C, ws, init, 3, c, tmp, comp + (size_t)c * C.n, s);
+  }
+  double dx = (double)P.nx / (double)C.nx, dy = (double)P.ny / (double)C.ny, dz = 1.0;
+  k_dense_init_pack<<<grid_for(C.n), kThreads, 0, s>>>(dense, comp, comp + C.n, comp + 2 * C.n, C.n, dx, dy, dz);
+}
+
+template <typename T>
+static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
+                        const uint8_t* mref, const float* init, float* out, WrLKStats* stats, void* ws,
+                        cudaStream_t s) {
+  LKState* st = at_off<LKState>(ws, P.state);
+  int* err_flag = reinterpret_cast<int*>(reinterpret_cast<char*>(st) + sizeof(LKState));
+  cudaMemsetAsync(err_flag, 0, sizeof(int), s);
+  build_tables(P, ws, err_flag, s);
+  build_pyramid<T>(P, ws, mov, ref, mmov, mref, s);
+  if (init) init_field(P, ws, init, s);
+  const bool mask = mmov || mref;
+  const double sps = p->smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
+  const float sps_f = (float)sps;
+  for (int l = P.levels - 1; l >= 0; --l) {
+    const LevelPlan& L = P.lv[l];
+    const bool coarsest = l == P.levels - 1;
+    k_level_begin<<<1, 1, 0, s>>>(st, l, coarsest ? 1 : 0);
+    int mode0;
+    if (coarsest) mode0 = init ? FIELD_DENSE : FIELD_ZERO;
+    else mode0 = FIELD_UP;
+    if (P.dense_all) {
+      // no update can happen at any level: carry dense fields down the pyramid
+      FieldSrc f = field_src(P, l, mode0, ws);
+      float4* dense = at_off<float4>(ws, L.dense);
+      if (mode0 == FIELD_UP) k_dense_from<FIELD_UP><<<grid_for(L.n), kThreads, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+      else if (mode0 == FIELD_ZERO) k_dense_from<FIELD_ZERO><<<grid_for(L.n), kThreads, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+      mode0 = FIELD_DENSE;
+    }
+    FieldSrc f0 = field_src(P, l, mode0, ws);
+    first_dispatch(mode0, P, L, ws, st, f0, true, false, s);
+    IterArgs a;
+    memset(&a, 0, sizeof(a));
+    a.st = st;
+    a.ref = at_off<float>(ws, L.ref);
+    a.mov.g = at_off<float4>(ws, L.movg);
+    a.mov.nx = L.nx;
+    a.mov.ny = L.ny;
+    a.mov.nz = L.nz;
+    a.mbits = mask ? at_off<uint8_t>(ws, L.mbits) : nullptr;
+    a.mmov = mmov ? at_off<float>(ws, L.mmov) : nullptr;
+    a.sums = at_off<float>(ws, L.sums);
+    a.errpart = at_off<double>(ws, L.errpart);
+    a.penpart = at_off<double>(ws, L.penpart);
+    a.cpv = cp_view(P, L, ws);
+    a.r = P.r;
+    a.w = P.w;
+    a.ntx = L.ntx;
+    a.nty = L.nty;
+    a.zratio = L.zratio;
+    const dim3 grid(L.ntx, L.nty, L.nz);
+    const size_t smem = iter_smem(P.w);
+    const int forced = p->forced_updates[l];
+    for (int it = 0; it < P.iter; ++it) {
+      const int mode = it == 0 ? mode0 : FIELD_CP;
+      a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
+      accumulate(mode, a, grid, smem, mask, s);
+      k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
+      k_update<<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
+                                                     (double)p->movRange, L.zratio_d);
+      if (it == 0) first_dispatch(mode0, P, L, ws, st, f0, false, true, s);
+      k_post<<<1, 1, 0, s>>>(st, l, forced);
+    }
+  }
+  const LevelPlan& L0 = P.lv[0];
+  if (P.dense_all) {
+    FieldSrc f = field_src(P, 0, FIELD_DENSE, ws);
+    k_write_motion<FIELD_DENSE><<<grid_for(L0.n), kThreads, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+  } else {
+    FieldSrc f = field_src(P, 0, FIELD_CP, ws);
+    k_write_motion<FIELD_CP><<<grid_for(L0.n), kThreads, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+  }
+  if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "wr_lk_register launch");
+  return WR_OK;
+}
+
+static int check_volume(const WrVolume* v, const char* name) {
+  if (!v || !v->data) return fail(WR_E_NULL, (std::string(name) + " is NULL").c_str());
+  if (v->dtype != WR_U8 && v->dtype != WR_U16 && v->dtype != WR_F32)
+    return fail(WR_E_DTYPE, (std::string(name) + ": dtype must be WR_U8, WR_U16 or WR_F32").c_str());
+  if (v->nz < 1 || v->ny < 1 || v->nx < 1) return fail(WR_E_SHAPE, (std::string(name) + ": empty volume").c_str());
+  return WR_OK;
+}
+
+}  // namespace wr
+
+using namespace wr;
+
+extern "C" {
+
+int wr_abi_version(void) { return WR_ABI_VERSION; }
+
+const char* wr_last_error(void) { return g_last_error.c_str(); }
+
+int wr_lk_workspace_size(int32_t nz, int32_t ny, int32_t nx, const WrLKParams* p, size_t* bytes) {
+  if (!p || !bytes) return fail(WR_E_NULL, "params or bytes is NULL");
+  Plan P;
+  const char* why;
+  int rc = make_plan(nz, ny, nx, p, true, true, true, &P, &why);
+  if (rc) return fail(rc, why);
+  *bytes = P.total;
+  return WR_OK;
+}
+
+int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                   const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init, float* motion_out,
+                   WrLKStats* stats, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_volume(mov, "mov"))) return rc;
+  if ((rc = check_volume(ref, "ref"))) return rc;
+  if (!p) return fail(WR_E_NULL, "params is NULL");
+  if (!motion_out) return fail(WR_E_NULL, "motion_out is NULL");
+  if (!workspace) return fail(WR_E_NULL, "workspace is NULL");
+  if (mov->nz != ref->nz || mov->ny != ref->ny || mov->nx != ref->nx)
+    return fail(WR_E_SHAPE, "mov and ref shapes differ");
+  if (mov->dtype != ref->dtype) return fail(WR_E_DTYPE, "mov and ref dtypes differ");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256) return fail(WR_E_WORKSPACE, "workspace must be 256-byte aligned");
+  Plan P;
+  const char* why;
+  rc = make_plan(mov->nz, mov->ny, mov->nx, p, true, true, true, &P, &why);
+  if (rc) return fail(rc, why);
+  if (workspace_bytes < P.total) return fail(WR_E_WORKSPACE, "workspace smaller than wr_lk_workspace_size");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (mov->dtype) {
+    case WR_U16:
+      return run_register<uint16_t>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, excl_mask_mov,
+                                    excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+    case WR_U8:
+      return run_register<uint8_t>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, excl_mask_mov,
+                                   excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+    default:
+      return run_register<float>(P, p, (const float*)mov->data, (const float*)ref->data, excl_mask_mov,
+                                 excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+  }
+}
+
+int wr_warp_trilinear(const WrVolume* src, const float* motion, float* out, void* stream) {
+  int rc;
+  if ((rc = check_volume(src, "src"))) return rc;
+  if (!motion || !out) return fail(WR_E_NULL, "motion or out is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  long long n = (long long)src->nz * src->ny * src->nx;
+  switch (src->dtype) {
+    case WR_U16:
+      k_warp<uint16_t><<<grid_for(n), kThreads, 0, s>>>((const uint16_t*)src->data, motion, out, src->nz, src->ny, src->nx);
+      break;
+    case WR_U8:
+      k_warp<uint8_t><<<grid_for(n), kThreads, 0, s>>>((const uint8_t*)src->data, motion, out, src->nz, src->ny, src->nx);
+      break;
+    default:
+      k_warp<float><<<grid_for(n), kThreads, 0, s>>>((const float*)src->data, motion, out, src->nz, src->ny, src->nx);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "wr_warp_trilinear launch");
+  return WR_OK;
+}
+
+int wr_penalty_factor_scratch(int32_t nz, int32_t ny, int32_t nx, size_t* bytes) {
+  if (!bytes) return fail(WR_E_NULL, "bytes is NULL");
+  if (nz < 1 || ny < 1 || nx < 1) return fail(WR_E_SHAPE, "empty volume");
+  *bytes = (size_t)grid_for((long long)nz * ny * nx) * 4 * sizeof(double);
+  return WR_OK;
+}
+
+int wr_penalty_factor(const WrVolume* ref, const uint8_t* excl_mask_ref, double* factor_out, void* scratch,
+                      size_t scratch_bytes, void* stream) {
+  int rc;
+  if ((rc = check_volume(ref, "ref"))) return rc;
+  if (!factor_out || !scratch) return fail(WR_E_NULL, "factor_out or scratch is NULL");
+  if (ref->nx < 3 || ref->ny < 3) return fail(WR_E_SHAPE, "ref needs at least 3 voxels along x and y");
+  long long n = (long long)ref->nz * ref->ny * ref->nx;
+  int nblk = grid_for(n);
+  if (scratch_bytes < (size_t)nblk * 4 * sizeof(double)) return fail(WR_E_WORKSPACE, "scratch too small");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* part = static_cast<double*>(scratch);
+  switch (ref->dtype) {
+    case WR_U16:
+      k_penalty_partial<uint16_t><<<nblk, kThreads, 0, s>>>((const uint16_t*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+      break;
+    case WR_U8:
+      k_penalty_partial<uint8_t><<<nblk, kThreads, 0, s>>>((const uint8_t*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+      break;
+    default:
+      k_penalty_partial<float><<<nblk, kThreads, 0, s>>>((const float*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+  }
+  k_penalty_final<<<1, 1024, 0, s>>>(part, nblk, factor_out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "wr_penalty_factor launch");
+  return WR_OK;
+}
+
+int wr_resize_table(int32_t in_len, int32_t out_len, int32_t method, double* weights, int32_t* indices,
+                    int32_t* taps) {
+  if (!taps) return fail(WR_E_NULL, "taps is NULL");
+  if (in_len < 1 || out_len < 1) return fail(WR_E_SHAPE, "lengths must be positive");
+  if (method != RESIZE_BICUBIC && method != RESIZE_BILINEAR) return fail(WR_E_PARAM, "method must be 0 or 1");
+  int P = resize_taps(in_len, out_len);
+  *taps = P;
+  if (!weights) return WR_OK;
+  if (!indices) return fail(WR_E_NULL, "indices is NULL");
+  for (int k = 0; k < out_len; ++k)
+    resize_row(in_len, out_len, method, k, weights + (size_t)k * P, indices + (size_t)k * P);
+  return WR_OK;
+}
+
+}  // extern "C"

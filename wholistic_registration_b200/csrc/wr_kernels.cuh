@@ -1,0 +1,937 @@
+// Device kernels of the pyramid patch-wise Lucas-Kanade registration path.
+//
+// Layout: every volume is C-contiguous (z, y, x), x fastest.  A level's moving
+// volume is stored as float4 (m, Gx, Gy, Gz): the value and its clamped
+// central differences, so that the warp sample and the three gradient samples
+// of utils/calFlow3d_Wei_v1.py:134-206 come out of one set of 8 corner loads
+// (see lk_accumulate).  Control points (CP) are float4 (dx, dy, dz, 0).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "wr_plan.h"
+#include "wr_resize_table.cuh"
+
+namespace wr {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// element loads
+// ---------------------------------------------------------------------------
+
+template <typename T> __device__ __forceinline__ float load_f(const T* p, size_t i);
+template <> __device__ __forceinline__ float load_f<uint16_t>(const uint16_t* p, size_t i) {
+  return (float)__ldg(p + i);
+}
+template <> __device__ __forceinline__ float load_f<uint8_t>(const uint8_t* p, size_t i) {
+  return (float)__ldg(p + i);
+}
+template <> __device__ __forceinline__ float load_f<float>(const float* p, size_t i) {
+  return __ldg(p + i);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// f32 coordinate -> (lower tap, fraction); huge values are pinned so the
+// integer conversion stays defined (the taps are clamped anyway).
+__device__ __forceinline__ void split_coord(float c, int& i0, float& t) {
+  c = fminf(fmaxf(c, -1048576.f), 1048576.f);
+  float f = floorf(c);
+  t = c - f;
+  i0 = (int)f;
+}
+
+// ---------------------------------------------------------------------------
+// resize tables (utils/imresize.py:60-82)
+// ---------------------------------------------------------------------------
+
+// One thread per output row: P candidate taps, float64, unmodified order.
+__global__ void k_build_table(double* w, int32_t* idx, int in_len, int out_len, int method, int P) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= out_len) return;
+  resize_row(in_len, out_len, method, k, w + (size_t)k * P, idx + (size_t)k * P);
+}
+
+// Bilinear up-sampling table compacted to the (at most two) taps with nonzero
+// weight.  Dropping exact-zero terms does not change the weighted sum.
+__global__ void k_build_up_table(float* w2, int32_t* i2, int in_len, int out_len, int* err_flag) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= out_len) return;
+  double w[16];
+  int32_t ix[16];
+  int P = resize_taps(in_len, out_len);
+  if (P > 16) { atomicOr(err_flag, 1); return; }
+  resize_row(in_len, out_len, RESIZE_BILINEAR, k, w, ix);
+  int n = 0;
+  float ow[2] = {0.f, 0.f};
+  int32_t oi[2] = {0, 0};
+  for (int t = 0; t < P; ++t) {
+    if (w[t] != 0.0) {
+      if (n < 2) { ow[n] = (float)w[t]; oi[n] = ix[t]; }
+      ++n;
+    }
+  }
+  if (n > 2) atomicOr(err_flag, 2);
+  w2[2 * k] = ow[0]; w2[2 * k + 1] = ow[1];
+  i2[2 * k] = oi[0]; i2[2 * k + 1] = oi[1];
+}
+
+// ---------------------------------------------------------------------------
+// separable resample (utils/imresize.py:121-137, 185-187)
+// ---------------------------------------------------------------------------
+
+// Float64 accumulation without contraction reproduces the reference's
+// float64 products and tap-order sums exactly; float32 uses FMA.
+template <typename A> struct Acc;
+template <> struct Acc<double> {
+  static __device__ __forceinline__ double madd(double acc, double w, double v) {
+    return __dadd_rn(acc, __dmul_rn(w, v));
+  }
+};
+template <> struct Acc<float> {
+  static __device__ __forceinline__ float madd(float acc, double w, float v) {
+    return fmaf((float)w, v, acc);
+  }
+};
+
+// out[z][y][xo] = sum_t w[xo][t] * in[z][y][idx[xo][t]]   (stride/comp select
+// one component of an interleaved input)
+template <typename Tin, typename A, typename Tout>
+__global__ void k_resample_x(const Tin* __restrict__ in, Tout* __restrict__ out, int nz, int ny,
+                             int nx_in, int nx_out, const double* __restrict__ w,
+                             const int32_t* __restrict__ idx, int P, int stride, int comp) {
+  long long total = (long long)nz * ny * nx_out;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    int xo = (int)(o % nx_out);
+    long long row = o / nx_out;
+    const Tin* src = in + (size_t)row * nx_in * stride + comp;
+    const double* wr = w + (size_t)xo * P;
+    const int32_t* ir = idx + (size_t)xo * P;
+    A acc = 0;
+    for (int t = 0; t < P; ++t) acc = Acc<A>::madd(acc, wr[t], (A)__ldg(src + (size_t)ir[t] * stride));
+    out[o] = (Tout)acc;
+  }
+}
+
+template <typename Tin, typename A, typename Tout>
+__global__ void k_resample_y(const Tin* __restrict__ in, Tout* __restrict__ out, int nz, int ny_in,
+                             int ny_out, int nx, const double* __restrict__ w,
+                             const int32_t* __restrict__ idx, int P, int stride, int comp) {
+  long long total = (long long)nz * ny_out * nx;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(o % nx);
+    long long rest = o / nx;
+    int yo = (int)(rest % ny_out);
+    int z = (int)(rest / ny_out);
+    const Tin* src = in + (size_t)z * ny_in * nx * stride + (size_t)x * stride + comp;
+    const double* wr = w + (size_t)yo * P;
+    const int32_t* ir = idx + (size_t)yo * P;
+    A acc = 0;
+    for (int t = 0; t < P; ++t)
+      acc = Acc<A>::madd(acc, wr[t], (A)__ldg(src + (size_t)ir[t] * nx * stride));
+    out[o] = (Tout)acc;
+  }
+}
+
+// double-exact variant of the y pass reading float64 input
+__global__ void k_resample_y_d(const double* __restrict__ in, double* __restrict__ out, int nz,
+                               int ny_in, int ny_out, int nx, const double* __restrict__ w,
+                               const int32_t* __restrict__ idx, int P) {
+  long long total = (long long)nz * ny_out * nx;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(o % nx);
+    long long rest = o / nx;
+    int yo = (int)(rest % ny_out);
+    int z = (int)(rest / ny_out);
+    const double* src = in + (size_t)z * ny_in * nx + x;
+    double acc = 0.0;
+    for (int t = 0; t < P; ++t)
+      acc = __dadd_rn(acc, __dmul_rn(w[(size_t)yo * P + t], src[(size_t)idx[(size_t)yo * P + t] * nx]));
+    out[o] = acc;
+  }
+}
+
+__global__ void k_resample_x_d(const double* __restrict__ in, double* __restrict__ out, int nz,
+                               int ny, int nx_in, int nx_out, const double* __restrict__ w,
+                               const int32_t* __restrict__ idx, int P) {
+  long long total = (long long)nz * ny * nx_out;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    int xo = (int)(o % nx_out);
+    long long row = o / nx_out;
+    const double* src = in + (size_t)row * nx_in;
+    double acc = 0.0;
+    for (int t = 0; t < P; ++t)
+      acc = __dadd_rn(acc, __dmul_rn(w[(size_t)xo * P + t], src[idx[(size_t)xo * P + t]]));
+    out[o] = acc;
+  }
+}
+
+// uint8 mask -> float64 0/1 (first pass input for the float64 mask resize)
+__global__ void k_mask_to_d(const uint8_t* __restrict__ m, double* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = m[i] ? 1.0 : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// level packing
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_to_float(const T* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = load_f<T>(in, i);
+}
+
+// movg[p] = (m, Gx, Gy, Gz) with G = half the clamped central difference.
+template <typename T>
+__global__ void k_pack_movg(const T* __restrict__ m, float4* __restrict__ movg, int nz, int ny, int nx) {
+  long long n = (long long)nz * ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(i % nx);
+    long long rest = i / nx;
+    int y = (int)(rest % ny);
+    int z = (int)(rest / ny);
+    size_t sy = nx, sz = (size_t)nx * ny;
+    float c = load_f<T>(m, i);
+    float xp = load_f<T>(m, i - x + min(x + 1, nx - 1));
+    float xm = load_f<T>(m, i - x + max(x - 1, 0));
+    float yp = load_f<T>(m, i + (size_t)(min(y + 1, ny - 1) - y) * sy);
+    float ym = load_f<T>(m, i - (size_t)(y - max(y - 1, 0)) * sy);
+    float zp = load_f<T>(m, i + (size_t)(min(z + 1, nz - 1) - z) * sz);
+    float zm = load_f<T>(m, i - (size_t)(z - max(z - 1, 0)) * sz);
+    movg[i] = make_float4(c, 0.5f * (xp - xm), 0.5f * (yp - ym), 0.5f * (zp - zm));
+  }
+}
+
+// mask bits of a level: bit0 = resized mask_ref > 0; bits 1-2 = class of the
+// trilinear cell whose lower corner is this voxel in the resized mask_mov:
+// 0 = all 8 corners <= 0, 1 = all > 0, 2 = mixed (needs the exact sum).
+__global__ void k_mask_bits(const double* __restrict__ mref_d, const uint8_t* __restrict__ mref_u8,
+                            const float* __restrict__ mmov, uint8_t* __restrict__ bits, int nz,
+                            int ny, int nx) {
+  long long n = (long long)nz * ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(i % nx);
+    long long rest = i / nx;
+    int y = (int)(rest % ny);
+    int z = (int)(rest / ny);
+    uint8_t b = 0;
+    if (mref_d) b |= (mref_d[i] > 0.0) ? 1 : 0;
+    else if (mref_u8) b |= mref_u8[i] ? 1 : 0;
+    if (mmov) {
+      int pos = 0, tot = 0;
+      for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+          for (int dx = 0; dx < 2; ++dx) {
+            int xx = min(x + dx, nx - 1), yy = min(y + dy, ny - 1), zz = min(z + dz, nz - 1);
+            pos += mmov[((size_t)zz * ny + yy) * nx + xx] > 0.f;
+            ++tot;
+          }
+      int code = pos == 0 ? 0 : (pos == tot ? 1 : 2);
+      b |= (uint8_t)(code << 1);
+    }
+    bits[i] = b;
+  }
+}
+
+__global__ void k_d_to_f(const double* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__global__ void k_u8_to_unit_f(const uint8_t* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i] ? 1.f : 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// motion field evaluation
+// ---------------------------------------------------------------------------
+
+struct CPView {
+  const float4* cp;
+  int ncx, ncy, r, w;
+};
+
+// Dense motion of a voxel from the CP grid: trilinear map_coordinates on the
+// CP grid at ((x-r)/(2r+1), (y-r)/(2r+1), z), coordinates clamped to
+// [0, ncp] then taps edge-clamped (utils/calFlow3d_Wei_v1.py:265-292,626-640).
+__device__ __forceinline__ float3 cp_field(const CPView& g, int x, int y, int z) {
+  float gx = __fdiv_rn((float)(x - g.r), (float)g.w);
+  float gy = __fdiv_rn((float)(y - g.r), (float)g.w);
+  gx = fminf(fmaxf(gx, 0.f), (float)g.ncx);
+  gy = fminf(fmaxf(gy, 0.f), (float)g.ncy);
+  float fx = floorf(gx), fy = floorf(gy);
+  float tx = gx - fx, ty = gy - fy;
+  int ix0 = min((int)fx, g.ncx - 1), ix1 = min((int)fx + 1, g.ncx - 1);
+  int iy0 = min((int)fy, g.ncy - 1), iy1 = min((int)fy + 1, g.ncy - 1);
+  const float4* b = g.cp + (size_t)z * g.ncy * g.ncx;
+  float4 a00 = b[iy0 * g.ncx + ix0], a01 = b[iy0 * g.ncx + ix1];
+  float4 a10 = b[iy1 * g.ncx + ix0], a11 = b[iy1 * g.ncx + ix1];
+  float w00 = (1.f - tx) * (1.f - ty), w01 = tx * (1.f - ty), w10 = (1.f - tx) * ty, w11 = tx * ty;
+  float3 r;
+  r.x = w00 * a00.x + w01 * a01.x + w10 * a10.x + w11 * a11.x;
+  r.y = w00 * a00.y + w01 * a01.y + w10 * a10.y + w11 * a11.y;
+  r.z = w00 * a00.z + w01 * a01.z + w10 * a10.z + w11 * a11.z;
+  return r;
+}
+
+// Up-sampled field of the previous (coarser) level: bilinear imresize of its
+// dense field, x and y components doubled (utils/calFlow3d_Wei_v1.py:381-410).
+struct UpView {
+  CPView src;                 // coarser level's CP grid
+  const float4* src_dense;    // or its dense field (used when non-null)
+  int src_nx, src_ny;
+  const float* wx; const int32_t* ix;
+  const float* wy; const int32_t* iy;
+  int x_first;
+};
+
+__device__ __forceinline__ float3 coarse_value(const UpView& u, int x, int y, int z) {
+  if (u.src_dense) {
+    float4 v = u.src_dense[((size_t)z * u.src_ny + y) * u.src_nx + x];
+    return make_float3(v.x, v.y, v.z);
+  }
+  return cp_field(u.src, x, y, z);
+}
+
+__device__ __forceinline__ float3 up_field(const UpView& u, int x, int y, int z) {
+  float wx0 = u.wx[2 * x], wx1 = u.wx[2 * x + 1];
+  int ix0 = u.ix[2 * x], ix1 = u.ix[2 * x + 1];
+  float wy0 = u.wy[2 * y], wy1 = u.wy[2 * y + 1];
+  int iy0 = u.iy[2 * y], iy1 = u.iy[2 * y + 1];
+  float3 f00 = coarse_value(u, ix0, iy0, z), f01 = coarse_value(u, ix1, iy0, z);
+  float3 f10 = coarse_value(u, ix0, iy1, z), f11 = coarse_value(u, ix1, iy1, z);
+  float3 r;
+  if (u.x_first) {
+    float3 r0 = make_float3(wx0 * f00.x + wx1 * f01.x, wx0 * f00.y + wx1 * f01.y, wx0 * f00.z + wx1 * f01.z);
+    float3 r1 = make_float3(wx0 * f10.x + wx1 * f11.x, wx0 * f10.y + wx1 * f11.y, wx0 * f10.z + wx1 * f11.z);
+    r = make_float3(wy0 * r0.x + wy1 * r1.x, wy0 * r0.y + wy1 * r1.y, wy0 * r0.z + wy1 * r1.z);
+  } else {
+    float3 c0 = make_float3(wy0 * f00.x + wy1 * f10.x, wy0 * f00.y + wy1 * f10.y, wy0 * f00.z + wy1 * f10.z);
+    float3 c1 = make_float3(wy0 * f01.x + wy1 * f11.x, wy0 * f01.y + wy1 * f11.y, wy0 * f01.z + wy1 * f11.z);
+    r = make_float3(wx0 * c0.x + wx1 * c1.x, wx0 * c0.y + wx1 * c1.y, wx0 * c0.z + wx1 * c1.z);
+  }
+  r.x *= 2.f;
+  r.y *= 2.f;
+  return r;
+}
+
+struct FieldSrc {
+  int mode;            // FieldMode
+  CPView cpv;          // FIELD_CP
+  UpView up;           // FIELD_UP
+  const float4* dense; // FIELD_DENSE
+  int nx, ny;
+};
+
+template <int MODE>
+__device__ __forceinline__ float3 eval_field(const FieldSrc& f, int x, int y, int z) {
+  if (MODE == FIELD_CP) return cp_field(f.cpv, x, y, z);
+  if (MODE == FIELD_UP) return up_field(f.up, x, y, z);
+  if (MODE == FIELD_DENSE) {
+    float4 v = f.dense[((size_t)z * f.ny + y) * f.nx + x];
+    return make_float3(v.x, v.y, v.z);
+  }
+  return make_float3(0.f, 0.f, 0.f);
+}
+
+// ---------------------------------------------------------------------------
+// trilinear sampling
+// ---------------------------------------------------------------------------
+
+struct VolView {
+  const float4* g;   // (m, Gx, Gy, Gz)
+  int nx, ny, nz;
+};
+
+__device__ __forceinline__ const float4& at(const VolView& v, int x, int y, int z) {
+  return v.g[((size_t)z * v.ny + y) * v.nx + x];
+}
+
+// Trilinear sample of the m channel at an arbitrary coordinate (map_coordinates
+// order=1, mode="nearest").
+__device__ __forceinline__ float sample_m(const VolView& v, float cx, float cy, float cz) {
+  int x0, y0, z0;
+  float tx, ty, tz;
+  split_coord(cx, x0, tx);
+  split_coord(cy, y0, ty);
+  split_coord(cz, z0, tz);
+  int xa = clampi(x0, 0, v.nx - 1), xb = clampi(x0 + 1, 0, v.nx - 1);
+  int ya = clampi(y0, 0, v.ny - 1), yb = clampi(y0 + 1, 0, v.ny - 1);
+  int za = clampi(z0, 0, v.nz - 1), zb = clampi(z0 + 1, 0, v.nz - 1);
+  float c000 = at(v, xa, ya, za).x, c001 = at(v, xb, ya, za).x;
+  float c010 = at(v, xa, yb, za).x, c011 = at(v, xb, yb, za).x;
+  float c100 = at(v, xa, ya, zb).x, c101 = at(v, xb, ya, zb).x;
+  float c110 = at(v, xa, yb, zb).x, c111 = at(v, xb, yb, zb).x;
+  float e00 = fmaf(tx, c001 - c000, c000), e01 = fmaf(tx, c011 - c010, c010);
+  float e10 = fmaf(tx, c101 - c100, c100), e11 = fmaf(tx, c111 - c110, c110);
+  float f0 = fmaf(ty, e01 - e00, e00), f1 = fmaf(ty, e11 - e10, e10);
+  return fmaf(tz, f1 - f0, f0);
+}
+
+// float64 trilinear of a float32 volume, cast to float32 (scipy's arithmetic
+// for the warped exclusion mask).
+__device__ __forceinline__ float sample_f64(const float* v, int nx, int ny, int nz, float cx, float cy, float cz) {
+  int x0, y0, z0;
+  float tx_f, ty_f, tz_f;
+  split_coord(cx, x0, tx_f);
+  split_coord(cy, y0, ty_f);
+  split_coord(cz, z0, tz_f);
+  double tx = tx_f, ty = ty_f, tz = tz_f;
+  int xs[2] = {clampi(x0, 0, nx - 1), clampi(x0 + 1, 0, nx - 1)};
+  int ys[2] = {clampi(y0, 0, ny - 1), clampi(y0 + 1, 0, ny - 1)};
+  int zs[2] = {clampi(z0, 0, nz - 1), clampi(z0 + 1, 0, nz - 1)};
+  double acc = 0.0;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        double wgt = (a ? tx : 1.0 - tx) * (b ? ty : 1.0 - ty) * (c ? tz : 1.0 - tz);
+        acc += wgt * (double)v[((size_t)zs[c] * ny + ys[b]) * nx + xs[a]];
+      }
+  return (float)acc;
+}
+
+// ---------------------------------------------------------------------------
+// block reductions
+// ---------------------------------------------------------------------------
+
+template <int N>
+__device__ __forceinline__ void block_sum(float (&v)[N], float* red /* [32*N] */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) red[warp * N + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < N) {
+    float s = 0.f;
+    for (int wi = 0; wi < nw; ++wi) s += red[wi * N + threadIdx.x];
+    red[32 * N + threadIdx.x] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = red[32 * N + k];
+}
+
+__device__ __forceinline__ float block_max(float v, float* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int wi = 0; wi < nw; ++wi) m = fmaxf(m, red[wi]);
+    red[32] = m;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// ---------------------------------------------------------------------------
+// fused LK iteration: warp + masked smoothed It + gradients + window sums
+// (utils/calFlow3d_Wei_v1.py:442-588)
+// ---------------------------------------------------------------------------
+
+struct IterArgs {
+  LKState* st;
+  const float* __restrict__ ref;
+  VolView mov;
+  const uint8_t* __restrict__ mbits;   // null: no masks
+  const float* __restrict__ mmov;      // null: no moving mask
+  float* __restrict__ sums;            // ncp * 12: 9 window sums + 3 neighbour differences
+  double* __restrict__ errpart;        // per tile
+  double* __restrict__ penpart;        // per tile
+  CPView cpv;                          // this level's CPs (motion_current at CPs)
+  FieldSrc field;                      // motion used for this iteration
+  int r, w, ntx, nty;
+  float zratio;
+};
+
+// One CTA per (window or leftover tile, z slice).  Pass 1 samples the warped
+// moving volume on the tile plus a one-voxel halo (the 3x3 It smoothing reads
+// it) and, inside the tile, the three gradients and the exclusion mask.
+// Pass 2 smooths It, applies the mask, accumulates It^2 for the error and the
+// nine gradient products for the window sum.  A window hanging over the
+// volume edge counts the edge voxel once per replicated position
+// (mode="nearest" of the (2r+1)^2 box filter, utils/calculate.py:51).
+template <int MODE, bool MASK>
+__global__ void __launch_bounds__(kThreads) k_lk_accumulate(IterArgs a) {
+  if (!a.st->active) return;
+  extern __shared__ float smem[];
+  const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
+  const int tx = blockIdx.x, ty = blockIdx.y, z = blockIdx.z;
+  const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
+  const bool window = (tx < ncx) && (ty < ncy);
+  const int x0 = tx * a.w, y0 = ty * a.w;
+  const int xe = min(x0 + a.w, nx), ye = min(y0 + a.w, ny);
+  const int wx = xe - x0, wy = ye - y0;
+  const int hw = wx + 2, hh = wy + 2;
+  float* it_raw = smem;                                   // hh * hw
+  float4* gsm = reinterpret_cast<float4*>(smem + ((hh * hw + 3) & ~3));   // wy * wx
+  float* red = reinterpret_cast<float*>(gsm + wx * wy);   // reduction scratch
+
+  // pass 1
+  for (int h = threadIdx.x; h < hh * hw; h += blockDim.x) {
+    const int hy = h / hw, hx = h - hy * hw;
+    const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
+    const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
+    const bool inner = hx >= 1 && hx <= wx && hy >= 1 && hy <= wy;
+    const float3 m = eval_field<MODE>(a.field, gx, gy, z);
+    const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = (float)z + m.z;
+    int ix0, iy0, iz0;
+    float fx, fy, fz;
+    split_coord(cx, ix0, fx);
+    split_coord(cy, iy0, fy);
+    split_coord(cz, iz0, fz);
+    const int xa = clampi(ix0, 0, nx - 1), xb = clampi(ix0 + 1, 0, nx - 1);
+    const int ya = clampi(iy0, 0, ny - 1), yb = clampi(iy0 + 1, 0, ny - 1);
+    const int za = clampi(iz0, 0, nz - 1), zb = clampi(iz0 + 1, 0, nz - 1);
+    const float4 c000 = at(a.mov, xa, ya, za), c001 = at(a.mov, xb, ya, za);
+    const float4 c010 = at(a.mov, xa, yb, za), c011 = at(a.mov, xb, yb, za);
+    const float4 c100 = at(a.mov, xa, ya, zb), c101 = at(a.mov, xb, ya, zb);
+    const float4 c110 = at(a.mov, xa, yb, zb), c111 = at(a.mov, xb, yb, zb);
+    // interpolate all four channels with shared weights
+    float4 e00, e01, e10, e11, f0, f1, s;
+#define WR_LERP4(o, p, q, t) \
+  o.x = fmaf(t, q.x - p.x, p.x); o.y = fmaf(t, q.y - p.y, p.y); \
+  o.z = fmaf(t, q.z - p.z, p.z); o.w = fmaf(t, q.w - p.w, p.w);
+    WR_LERP4(e00, c000, c001, fx)
+    WR_LERP4(e01, c010, c011, fx)
+    WR_LERP4(e10, c100, c101, fx)
+    WR_LERP4(e11, c110, c111, fx)
+    WR_LERP4(f0, e00, e01, fy)
+    WR_LERP4(f1, e10, e11, fy)
+    WR_LERP4(s, f0, f1, fz)
+#undef WR_LERP4
+    const size_t p = ((size_t)z * ny + gy) * nx + gx;
+    it_raw[h] = __ldg(a.ref + p) - s.x;
+    if (inner) {
+      // central differences of samples at c +- e_k, clipped to the volume:
+      // inside [1, n-2] they equal the sample of the precomputed difference
+      float gxv, gyv, gzv;
+      if (cx >= 1.f && cx <= (float)(nx - 2)) gxv = s.y;
+      else gxv = 0.5f * (sample_m(a.mov, fminf(fmaxf(cx + 1.f, 0.f), (float)(nx - 1)), cy, cz) -
+                         sample_m(a.mov, fminf(fmaxf(cx - 1.f, 0.f), (float)(nx - 1)), cy, cz));
+      if (cy >= 1.f && cy <= (float)(ny - 2)) gyv = s.z;
+      else gyv = 0.5f * (sample_m(a.mov, cx, fminf(fmaxf(cy + 1.f, 0.f), (float)(ny - 1)), cz) -
+                         sample_m(a.mov, cx, fminf(fmaxf(cy - 1.f, 0.f), (float)(ny - 1)), cz));
+      if (cz >= 1.f && cz <= (float)(nz - 2)) gzv = s.w;
+      else gzv = 0.5f * (sample_m(a.mov, cx, cy, fminf(fmaxf(cz + 1.f, 0.f), (float)(nz - 1))) -
+                         sample_m(a.mov, cx, cy, fminf(fmaxf(cz - 1.f, 0.f), (float)(nz - 1))));
+      float excl = 0.f;
+      if (MASK) {
+        bool ex = (a.mbits[p] & 1) != 0;
+        if (!ex && a.mmov) {
+          bool in_range = cx >= 0.f && cx <= (float)(nx - 1) && cy >= 0.f && cy <= (float)(ny - 1) &&
+                          cz >= 0.f && cz <= (float)(nz - 1);
+          int code = 2;
+          if (in_range) code = (a.mbits[((size_t)iz0 * ny + iy0) * nx + ix0] >> 1) & 3;
+          if (code == 1) ex = true;
+          else if (code == 2) ex = sample_f64(a.mmov, nx, ny, nz, cx, cy, cz) > 0.f;
+        }
+        excl = ex ? 1.f : 0.f;
+      }
+      gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
+    }
+  }
+  __syncthreads();
+
+  // pass 2
+  float acc[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) acc[k] = 0.f;
+  for (int i = threadIdx.x; i < wx * wy; i += blockDim.x) {
+    const int ly = i / wx, lx = i - ly * wx;
+    const float* rp = it_raw + ly * hw + lx;
+    float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
+               (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
+    it *= (1.f / 9.f);
+    float4 g = gsm[i];
+    if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
+    acc[9] += it * it;
+    if (window) {
+      const int gx = x0 + lx, gy = y0 + ly;
+      const float mx = (gx == nx - 1) ? (float)(x0 + a.w - (nx - 1)) : 1.f;
+      const float my = (gy == ny - 1) ? (float)(y0 + a.w - (ny - 1)) : 1.f;
+      const float wt = mx * my;
+      const float iz = g.z / a.zratio;
+      const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
+      acc[0] += wgx * g.x;
+      acc[1] += wgx * g.y;
+      acc[2] += wgx * iz;
+      acc[3] += wgy * g.y;
+      acc[4] += wgy * iz;
+      acc[5] += wgz * iz;
+      acc[6] += wgx * it;
+      acc[7] += wgy * it;
+      acc[8] += wgz * it;
+    }
+  }
+  block_sum<10>(acc, red);
+
+  const long long blk = ((long long)z * a.nty + ty) * a.ntx + tx;
+  if (threadIdx.x == 0) {
+    a.errpart[blk] = (double)acc[9];
+    double pen = 0.0;
+    if (window) {
+      const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
+      float* s = a.sums + cpi * 12;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) s[k] = acc[k];
+      // neighbour difference on the CP grid (getNeiDiff with r = 1,
+      // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
+      // neighbours (edge-replicated) minus the centre, float64 then float32
+      const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
+      double sx = 0.0, sy = 0.0, sz = 0.0;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          if (dx == 0 && dy == 0) continue;
+          const float4 v = b[clampi(ty + dy, 0, ncy - 1) * ncx + clampi(tx + dx, 0, ncx - 1)];
+          sx += 0.125 * (double)v.x;
+          sy += 0.125 * (double)v.y;
+          sz += 0.125 * (double)v.z;
+        }
+      const float4 c = b[ty * ncx + tx];
+      const float ndx = (float)(sx - (double)c.x);
+      const float ndy = (float)(sy - (double)c.y);
+      const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
+      s[9] = ndx;
+      s[10] = ndy;
+      s[11] = ndz;
+      pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
+    }
+    a.penpart[blk] = pen;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// error evaluation and stopping rules (utils/calFlow3d_Wei_v1.py:101-131,501-530)
+// ---------------------------------------------------------------------------
+
+__global__ void k_decide(LKState* st, const double* __restrict__ errpart, const double* __restrict__ penpart,
+                         long long nblk, double n_vox, double sps, int level, int it, int iter, double tol,
+                         int forced) {
+  if (!st->active) return;
+  __shared__ double red[2][1024];
+  double e = 0.0, p = 0.0;
+  for (long long i = threadIdx.x; i < nblk; i += blockDim.x) {
+    e += errpart[i];
+    p += penpart[i];
+  }
+  red[0][threadIdx.x] = e;
+  red[1][threadIdx.x] = p;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double diff = red[0][0] / n_vox;
+  const double pen = red[1][0] * sps / n_vox;
+  const double cur = diff + pen;
+  WrLKStats& S = st->stats;
+  const int e_idx = S.evals[level];
+  if (e_idx < WR_MAX_ITERS) {
+    S.diff_error[level][e_idx] = diff;
+    S.penalty_error[level][e_idx] = pen;
+  }
+  S.evals[level] = e_idx + 1;
+  S.current_error = cur;
+  bool stop;
+  if (forced >= 0) {
+    stop = st->n_updates >= forced;
+  } else if (it == iter - 1) {
+    stop = true;
+  } else {
+    int n_le = (st->old_err[0] <= cur) + (st->old_err[1] <= cur) + (st->old_err[2] <= cur);
+    if (n_le > 1) stop = true;
+    else if (fabs(st->old_err[2] - cur) < tol) stop = true;
+    else {
+      stop = false;
+      st->old_err[0] = st->old_err[1];
+      st->old_err[1] = st->old_err[2];
+      st->old_err[2] = cur;
+    }
+  }
+  if (stop) {
+    st->active = 0;
+    st->do_update = 0;
+  } else {
+    st->do_update = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CP solve and update (utils/calFlow3d_Wei_v1.py:209-262,591-624)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, const float* __restrict__ sums,
+                                                    long long ncp, double sps, float sps_f, double mov_range,
+                                                    double zratio_d) {
+  if (!st->do_update) return;
+  __shared__ float red[64];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float dmax = 0.f;
+  int nan_count = 0;
+  if (i < ncp) {
+    const float* s = sums + i * 12;
+    const double ixx = (double)s[0] + sps, ixy = s[1], ixz = s[2];
+    const double iyy = (double)s[3] + sps, iyz = s[4], izz = (double)s[5] + sps;
+    const double ixt = (double)s[6] + (double)__fmul_rn(sps_f, s[9]);
+    const double iyt = (double)s[7] + (double)__fmul_rn(sps_f, s[10]);
+    const double izt = (double)s[8] + (double)__fmul_rn(sps_f, s[11]);
+    const double det = ixx * (iyy * izz - iyz * iyz) - ixy * (ixy * izz - iyz * ixz) + ixz * (ixy * iyz - iyy * ixz);
+    const double m11 = iyy * izz - iyz * iyz;
+    const double m12 = -(ixy * izz - iyz * ixz);
+    const double m13 = ixy * iyz - iyy * ixz;
+    const double m22 = ixx * izz - ixz * ixz;
+    const double m23 = -(ixx * iyz - ixy * ixz);
+    const double m33 = ixx * iyy - ixy * ixy;
+    double vx = (m11 * ixt + m12 * iyt + m13 * izt) / det;
+    double vy = (m12 * ixt + m22 * iyt + m23 * izt) / det;
+    double vz = (m13 * ixt + m23 * iyt + m33 * izt) / det;
+    if (isnan(vx)) { vx = 0.0; ++nan_count; }
+    if (isnan(vy)) { vy = 0.0; ++nan_count; }
+    if (isnan(vz)) { vz = 0.0; ++nan_count; }
+    double dist = sqrt(vx * vx + vy * vy + vz * vz);
+    dist = fmax(dist / mov_range, 1.0);
+    vx /= dist;
+    vy /= dist;
+    vz = (vz / dist) / zratio_d;
+    const float4 old = cp[i];
+    const float nx = (float)((double)old.x + vx);
+    const float ny = (float)((double)old.y + vy);
+    const float nz = (float)((double)old.z + vz);
+    cp[i] = make_float4(nx, ny, nz, 0.f);
+    dmax = fmaxf(fmaxf(fabsf(nx - old.x), fabsf(ny - old.y)), fabsf(nz - old.z));
+  }
+  if (nan_count) atomicAdd(&st->stats.nan_solves, nan_count);
+  const float m = block_max(dmax, red);
+  if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
+}
+
+// max |new - old| over every voxel at a level's first iteration, where the
+// old field is not a function of this level's CPs.
+template <int MODE0>
+__global__ void __launch_bounds__(kThreads) k_diff_first(LKState* st, CPView cpv, FieldSrc old, int nx, int ny, int nz) {
+  if (!st->do_update) return;
+  __shared__ float red[64];
+  const long long n = (long long)nx * ny * nz;
+  float dmax = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long rest = i / nx;
+    const int y = (int)(rest % ny);
+    const int z = (int)(rest / ny);
+    const float3 a = cp_field(cpv, x, y, z);
+    const float3 b = eval_field<MODE0>(old, x, y, z);
+    dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(a.x - b.x), fabsf(a.y - b.y)), fabsf(a.z - b.z)));
+  }
+  const float m = block_max(dmax, red);
+  if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
+}
+
+// after an update: log max |delta motion| and apply the 1e-3 rule
+// (utils/calFlow3d_Wei_v1.py:641-654)
+__global__ void k_post(LKState* st, int level, int forced) {
+  if (!st->do_update) return;
+  const float md = __uint_as_float(st->maxdiff_bits);
+  WrLKStats& S = st->stats;
+  const int u = st->n_updates;
+  if (u < WR_MAX_ITERS) S.max_diff_motion[level][u] = (double)md;
+  st->n_updates = u + 1;
+  S.updates[level] = u + 1;
+  if (forced < 0 && (double)md < 1e-3) st->active = 0;
+  st->maxdiff_bits = 0u;
+  st->do_update = 0;
+}
+
+__global__ void k_level_begin(LKState* st, int level, int first) {
+  if (first) {
+    WrLKStats z = {};
+    st->stats = z;
+  }
+  st->active = 1;
+  st->do_update = 0;
+  st->level = level;
+  st->n_updates = 0;
+  st->maxdiff_bits = 0u;
+  st->old_err[0] = st->old_err[1] = st->old_err[2] = INFINITY;
+  st->stats.evals[level] = 0;
+  st->stats.updates[level] = 0;
+}
+
+// motion_current at the CP voxels at a level's start
+template <int MODE0>
+__global__ void k_cp_init(float4* cp, FieldSrc f, int ncx, int ncy, int nz, int r, int w) {
+  const long long n = (long long)ncx * ncy * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int cx = (int)(i % ncx);
+    const long long rest = i / ncx;
+    const int cy = (int)(rest % ncy);
+    const int z = (int)(rest / ncy);
+    const float3 v = eval_field<MODE0>(f, r + cx * w, r + cy * w, z);
+    cp[i] = make_float4(v.x, v.y, v.z, 0.f);
+  }
+}
+
+// dense field of a level from a field source (used when no update can occur
+// at some level, and for the coarsest level's initial field)
+template <int MODE0>
+__global__ void k_dense_from(float4* out, FieldSrc f, int nx, int ny, int nz) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long rest = i / nx;
+    const int y = (int)(rest % ny);
+    const int z = (int)(rest / ny);
+    const float3 v = eval_field<MODE0>(f, x, y, z);
+    out[i] = make_float4(v.x, v.y, v.z, 0.f);
+  }
+}
+
+// coarsest-level initial field from option["motion"] resized per component,
+// divided by the full-res/level size ratio (utils/calFlow3d_Wei_v1.py:362-377)
+__global__ void k_dense_init_pack(float4* out, const float* c0, const float* c1, const float* c2, long long n,
+                                  double dx, double dy, double dz) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = make_float4((float)((double)c0[i] / dx), (float)((double)c1[i] / dy), (float)((double)c2[i] / dz), 0.f);
+}
+
+// final motion (z, y, x, 3)
+template <int MODE>
+__global__ void k_write_motion(float* __restrict__ out, FieldSrc f, int nx, int ny, int nz) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long rest = i / nx;
+    const int y = (int)(rest % ny);
+    const int z = (int)(rest / ny);
+    const float3 v = eval_field<MODE>(f, x, y, z);
+    out[3 * i + 0] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// correctMotion (utils/calFlow3d_Wei_v1.py:676-706): pull warp, float64
+// trilinear arithmetic on float32 values, float32 result
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_warp(const T* __restrict__ src, const float* __restrict__ motion,
+                                                  float* __restrict__ out, int nz, int ny, int nx) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long rest = i / nx;
+    const int y = (int)(rest % ny);
+    const int z = (int)(rest / ny);
+    const float cx = (float)x + __ldg(motion + 3 * i + 0);
+    const float cy = (float)y + __ldg(motion + 3 * i + 1);
+    const float cz = (float)z + __ldg(motion + 3 * i + 2);
+    int x0, y0, z0;
+    float tx_f, ty_f, tz_f;
+    split_coord(cx, x0, tx_f);
+    split_coord(cy, y0, ty_f);
+    split_coord(cz, z0, tz_f);
+    const double tx = tx_f, ty = ty_f, tz = tz_f;
+    const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
+    const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
+    const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
+    const size_t sy = nx, sz = (size_t)nx * ny;
+    const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
+    const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
+    const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
+    const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
+    const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
+    const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
+                     wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
+    out[i] = (float)v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// smoothness-penalty normalisation factor (utils/preprocess.py:42-66)
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_penalty_partial(const T* __restrict__ ref, const uint8_t* __restrict__ excl,
+                                                             double* __restrict__ part, int nz, int ny, int nx) {
+  __shared__ double red[4][kThreads];
+  const long long n = (long long)nx * ny * nz;
+  double sxx = 0.0, syy = 0.0, cx = 0.0, cy = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long rest = i / nx;
+    const int y = (int)(rest % ny);
+    const bool keep = excl == nullptr || excl[i] == 0;
+    if (!keep) continue;
+    if (x >= 1 && x <= nx - 2) {
+      const double d = ((double)load_f<T>(ref, i + 1) - (double)load_f<T>(ref, i - 1)) / 2.0;
+      sxx += d * d;
+      cx += 1.0;
+    }
+    if (y >= 1 && y <= ny - 2) {
+      const double d = ((double)load_f<T>(ref, i + nx) - (double)load_f<T>(ref, i - nx)) / 2.0;
+      syy += d * d;
+      cy += 1.0;
+    }
+  }
+  red[0][threadIdx.x] = sxx;
+  red[1][threadIdx.x] = syy;
+  red[2][threadIdx.x] = cx;
+  red[3][threadIdx.x] = cy;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[4 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_penalty_final(const double* __restrict__ part, int nblk, double* out) {
+  __shared__ double red[4][1024];
+  double v[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+    for (int k = 0; k < 4; ++k) v[k] += part[4 * b + k];
+  for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = (red[0][0] / red[2][0] + red[1][0] / red[3][0]) / 2.0;
+}
+
+}  // namespace wr

@@ -1,0 +1,63 @@
+// Host-side plan of one registration call: level geometry, workspace layout
+// and the device-resident control state.
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "wr_b200.h"
+
+namespace wr {
+
+// Field sources of a level's first iteration.
+enum FieldMode { FIELD_CP = 0, FIELD_UP = 1, FIELD_DENSE = 2, FIELD_ZERO = 3 };
+
+struct LevelPlan {
+  int nx, ny, nz;     // level extent (x fastest)
+  int ncx, ncy;       // control points per slice along x and y
+  int ntx, nty;       // tiles: one per window plus a leftover tile if needed
+  long long n;        // voxels
+  long long ncp;      // control points (ncx * ncy * nz)
+  long long nblk;     // tiles of the fused iteration kernel
+  float zratio;       // zRatio / 2^layer
+  double zratio_d;
+  // pass order of the separable resize from full resolution (x first when
+  // the x scale is not larger than the y scale, like a stable argsort)
+  int x_first;
+  int up_x_first;
+  int tx_taps, ty_taps;   // candidate taps of the full-res -> level tables
+  // workspace byte offsets
+  size_t ref, movg, mbits, mmov, cp, sums, dense, errpart, penpart;
+  size_t tx_w, tx_i, ty_w, ty_i;      // bicubic tables full-res -> level (float64)
+  size_t ux_w, ux_i, uy_w, uy_i;      // bilinear tables level+1 -> level (2 taps, float)
+};
+
+struct Plan {
+  int nz, ny, nx;
+  int levels;          // layer + 1, index = layer
+  int r, w, iter;
+  bool has_mref, has_mmov, has_init, dense_all;
+  int precision;
+  LevelPlan lv[WR_MAX_LEVELS];
+  size_t tmp_a, tmp_a_bytes, tmp_b, tmp_b_bytes;
+  size_t state;
+  size_t total;
+};
+
+// Device control state of one call (lives in the workspace).
+struct LKState {
+  int active;          // the current level is still iterating
+  int do_update;       // the last error evaluation asked for a motion update
+  int level;
+  int n_updates;       // updates done at the current level
+  unsigned maxdiff_bits;
+  int flags;
+  double old_err[3];
+  WrLKStats stats;
+};
+
+// Fills `plan` for a (nz, ny, nx) volume; returns WR_OK or an argument error.
+int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool has_mmov,
+              bool has_init, Plan* plan, const char** why);
+
+}  // namespace wr

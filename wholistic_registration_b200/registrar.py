@@ -1,0 +1,195 @@
+"""Device-level entry point: (z, y, x) CUDA tensors in, (z, y, x, 3) motion out.
+
+``LKRegistrar`` owns a workspace for one volume shape and parameter set and
+calls the C ABI (``wr_lk_register``, ``wr_warp_trilinear``) on the current
+torch CUDA stream.  ``getMotion`` / ``correctMotion`` in
+``calFlow3d_Wei_v1`` wrap it with the reference's NumPy calling convention.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib
+
+_DTYPES = {
+    torch.uint16: _lib.WR_U16,
+    torch.uint8: _lib.WR_U8,
+    torch.float32: _lib.WR_F32,
+}
+
+
+@dataclass
+class LKParams:
+    """The getMotion option keys (utils/calFlow3d_Wei_v1.py:318-324,429-431).
+
+    ``forced_updates`` (layer -> count) replays another run's per-level update
+    counts instead of applying the stopping rules.
+    """
+
+    layer: int = 3
+    iter: int = 10
+    r: int = 5
+    zRatio: float = 27.693
+    movRange: float = 5.0
+    smoothPenalty: float = 0.0
+    tol: float = 1e-4
+    precision: int = _lib.WR_PREC_F32
+    forced_updates: dict = field(default_factory=dict)
+
+    @classmethod
+    def from_option(cls, option) -> "LKParams":
+        return cls(
+            layer=int(option["layer"]), iter=int(option["iter"]), r=int(option["r"]),
+            zRatio=float(option["zRatio"]), movRange=float(option.get("movRange", 5.0)),
+            smoothPenalty=float(option["smoothPenalty"]), tol=float(option["tol"]),
+            precision=int(option.get("precision", _lib.WR_PREC_F32)),
+            forced_updates=dict(option.get("forced_updates") or {}),
+        )
+
+    def to_c(self) -> _lib.WrLKParams:
+        p = _lib.WrLKParams()
+        p.layer, p.iter, p.r = self.layer, self.iter, self.r
+        p.zRatio, p.movRange = self.zRatio, self.movRange
+        p.smoothPenalty, p.tol = self.smoothPenalty, self.tol
+        p.precision = self.precision
+        for i in range(_lib.MAX_LEVELS):
+            p.forced_updates[i] = int(self.forced_updates.get(i, -1))
+        return p
+
+
+def _stream_ptr(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def _require_cuda(t: torch.Tensor, name: str):
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous (z, y, x)")
+
+
+def _vol(t: torch.Tensor, name: str) -> _lib.WrVolume:
+    _require_cuda(t, name)
+    if t.dim() != 3:
+        raise ValueError(f"{name} must be a 3-D (z, y, x) volume")
+    if t.dtype not in _DTYPES:
+        raise ValueError(f"{name}: dtype {t.dtype} not supported (uint8, uint16, float32)")
+    return _lib.volume(t.data_ptr(), _DTYPES[t.dtype], t.shape)
+
+
+def stats_to_log(st: _lib.WrLKStats, layers: int) -> tuple[dict, float]:
+    """error_log dict in the reference's shape (utils/calFlow3d_Wei_v1.py:329-335)."""
+    log = {}
+    for layer in range(layers - 1, -1, -1):
+        e, u = st.evals[layer], st.updates[layer]
+        diff = [st.diff_error[layer][i] for i in range(e)]
+        pen = [st.penalty_error[layer][i] for i in range(e)]
+        log[f"layer_{layer}"] = {
+            "diffError": diff,
+            "penaltyError": pen,
+            "currentError": [a + b for a, b in zip(diff, pen)],
+            "max_diff_motion": [st.max_diff_motion[layer][i] for i in range(u)],
+            "motion_current": [],
+            "data_mov_corrected": [],
+        }
+    return log, float(st.current_error)
+
+
+class LKRegistrar:
+    """Pyramid Lucas-Kanade registration of (z, y, x) volumes on one GPU."""
+
+    def __init__(self, shape_zyx, params: LKParams, device=None):
+        self.lib = _lib.load()
+        self.shape = tuple(int(s) for s in shape_zyx)
+        self.params = params
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self._cp = params.to_c()
+        nbytes = ctypes.c_size_t(0)
+        _lib.check("wr_lk_workspace_size",
+                   self.lib.wr_lk_workspace_size(*self.shape, ctypes.byref(self._cp), ctypes.byref(nbytes)))
+        self.workspace_bytes = int(nbytes.value)
+        self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
+        base = self.workspace.data_ptr()
+        self._ws_ptr = (base + 255) // 256 * 256
+        self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
+
+    def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
+                 motion_init=None, out=None, stream=None) -> torch.Tensor:
+        """Motion (z, y, x, 3) float32 registering ``mov`` onto ``ref``.
+
+        Masks are (z, y, x) uint8/bool exclusion masks (True = excluded) or
+        None; ``motion_init`` is a (z, y, x, 3) float32 initial field or None.
+        """
+        if tuple(mov.shape) != self.shape or tuple(ref.shape) != self.shape:
+            raise ValueError(f"volumes must have shape {self.shape}")
+        vm, vr = _vol(mov, "mov"), _vol(ref, "ref")
+        ptrs = []
+        for m, name in ((mask_mov, "mask_mov"), (mask_ref, "mask_ref")):
+            if m is None:
+                ptrs.append(None)
+                continue
+            _require_cuda(m, name)
+            if tuple(m.shape) != self.shape:
+                raise ValueError(f"{name} must have shape {self.shape}")
+            if m.dtype == torch.bool:
+                m = m.view(torch.uint8)
+            if m.dtype != torch.uint8:
+                raise ValueError(f"{name} must be bool or uint8")
+            ptrs.append(m.data_ptr())
+        init_ptr = None
+        if motion_init is not None:
+            _require_cuda(motion_init, "motion_init")
+            if tuple(motion_init.shape) != self.shape + (3,) or motion_init.dtype != torch.float32:
+                raise ValueError("motion_init must be float32 (z, y, x, 3)")
+            init_ptr = motion_init.data_ptr()
+        if out is None:
+            out = torch.empty(self.shape + (3,), dtype=torch.float32, device=self.device)
+        _lib.check("wr_lk_register", self.lib.wr_lk_register(
+            ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
+            out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream)))
+        return out
+
+    def stats(self) -> _lib.WrLKStats:
+        """Statistics of the last call (synchronises the stream)."""
+        host = self.stats_dev.cpu().numpy().tobytes()
+        return _lib.WrLKStats.from_buffer_copy(host)
+
+    def error_log(self):
+        return stats_to_log(self.stats(), self.params.layer + 1)
+
+
+def warp(src: torch.Tensor, motion: torch.Tensor, out=None, stream=None) -> torch.Tensor:
+    """correctMotion on the device: out(p) = src(p + motion(p)), float32."""
+    lib = _lib.load()
+    vs = _vol(src, "src")
+    _require_cuda(motion, "motion")
+    if tuple(motion.shape) != tuple(src.shape) + (3,) or motion.dtype != torch.float32:
+        raise ValueError("motion must be float32 (z, y, x, 3) matching src")
+    if out is None:
+        out = torch.empty(tuple(src.shape), dtype=torch.float32, device=src.device)
+    _lib.check("wr_warp_trilinear", lib.wr_warp_trilinear(ctypes.byref(vs), motion.data_ptr(), out.data_ptr(),
+                                                         _stream_ptr(stream)))
+    return out
+
+
+def penalty_factor(ref: torch.Tensor, mask_ref=None, stream=None) -> torch.Tensor:
+    """getSmPnltNormFctr (utils/preprocess.py:42-66) on the device; returns a
+    0-d float64 CUDA tensor."""
+    lib = _lib.load()
+    vr = _vol(ref, "ref")
+    nbytes = ctypes.c_size_t(0)
+    _lib.check("wr_penalty_factor_scratch", lib.wr_penalty_factor_scratch(*ref.shape, ctypes.byref(nbytes)))
+    scratch = torch.empty(int(nbytes.value), dtype=torch.uint8, device=ref.device)
+    out = torch.empty((), dtype=torch.float64, device=ref.device)
+    mptr = None
+    if mask_ref is not None:
+        _require_cuda(mask_ref, "mask_ref")
+        mptr = (mask_ref.view(torch.uint8) if mask_ref.dtype == torch.bool else mask_ref).data_ptr()
+    _lib.check("wr_penalty_factor", lib.wr_penalty_factor(ctypes.byref(vr), mptr, out.data_ptr(),
+                                                         scratch.data_ptr(), int(nbytes.value), _stream_ptr(stream)))
+    return out
