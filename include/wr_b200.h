@@ -142,6 +142,30 @@ WR_API int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_
                    void* stream);
 
 /*
+ * Instrumentation of one wr_lk_register_profiled call.  The caller creates
+ * timing-enabled CUDA events; the library records acc_begin[i] / acc_end[i]
+ * on the call's stream around the i-th launch of the fused iteration kernel
+ * (the dominant kernel), in launch order: levels from coarsest to finest,
+ * `iter` launches per level.  `launches` returns the number of kernels the
+ * call put on the stream.
+ */
+typedef struct {
+  void* const* acc_begin;   /* cudaEvent_t[capacity] */
+  void* const* acc_end;     /* cudaEvent_t[capacity] */
+  int32_t capacity;
+  int32_t recorded;         /* out: event pairs recorded */
+  int32_t launches;         /* out: kernels launched */
+  int32_t pad;
+} WrProfile;
+
+/* wr_lk_register with instrumentation (prof may be NULL). No reference counterpart:
+   it exists to time the fused iteration kernel inside a full registration. */
+WR_API int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                                   const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                                   float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                                   void* stream, WrProfile* prof);
+
+/*
  * Pull-warp `src` through `motion`: out(p) = src(p + motion(p)), trilinear,
  * edge-replicated, float32 result (correctMotion, utils/calFlow3d_Wei_v1.py:676-706).
  *   motion : (z,y,x,3) float32 device; out : (z,y,x) float32 device.

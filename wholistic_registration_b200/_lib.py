@@ -34,6 +34,7 @@ EXPORTS = (
     "wr_last_error",
     "wr_lk_workspace_size",
     "wr_lk_register",
+    "wr_lk_register_profiled",
     "wr_warp_trilinear",
     "wr_penalty_factor",
     "wr_penalty_factor_scratch",
@@ -80,6 +81,17 @@ class WrLKStats(ctypes.Structure):
     ]
 
 
+class WrProfile(ctypes.Structure):
+    _fields_ = [
+        ("acc_begin", ctypes.POINTER(ctypes.c_void_p)),
+        ("acc_end", ctypes.POINTER(ctypes.c_void_p)),
+        ("capacity", ctypes.c_int32),
+        ("recorded", ctypes.c_int32),
+        ("launches", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+
 class WrError(RuntimeError):
     """A C-ABI call returned a nonzero status."""
 
@@ -114,6 +126,7 @@ def load():
         lib.wr_lk_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(WrLKParams), ctypes.POINTER(sz)]
         lib.wr_lk_register.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), vp, vp,
                                        ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
+        lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
         lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_penalty_factor.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp, sz, vp]
         lib.wr_penalty_factor_scratch.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]

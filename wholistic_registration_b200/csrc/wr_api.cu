@@ -339,10 +339,30 @@ static void init_field(const Plan& P, void* ws, const float* init, cudaStream_t 
   k_dense_init_pack<<<grid_for(C.n), kThreads, 0, s>>>(dense, comp, comp + C.n, comp + 2 * C.n, C.n, dx, dy, dz);
 }
 
+// Number of kernels run_register launches for a plan (kept next to the launch
+// sequence it mirrors).
+static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_init) {
+  int n = 0;
+  for (int l = 0; l < P.levels; ++l) {
+    n += 2 + (l + 1 < P.levels ? 2 : 0);                       // tables
+    if (l == 0) n += 2 + (has_mmov ? 1 : 0) + ((has_mmov || has_mref) ? 1 : 0);
+    else n += 5 + (has_mmov ? 3 : 0) + (has_mref ? 2 : 0) + ((has_mmov || has_mref) ? 1 : 0);
+  }
+  if (has_init) n += (P.levels == 1 ? 3 : 6) + 1;
+  for (int l = P.levels - 1; l >= 0; --l) {
+    n += 1;                                                    // level begin
+    if (P.dense_all && !(l == P.levels - 1 && has_init)) n += 1; // dense field
+    n += 1;                                                    // cp init
+    n += 4 * P.iter + 1;                                       // iterations + first diff
+  }
+  return n + 1;                                                // final motion
+}
+
 template <typename T>
 static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
                         const uint8_t* mref, const float* init, float* out, WrLKStats* stats, void* ws,
-                        cudaStream_t s) {
+                        cudaStream_t s, WrProfile* prof) {
+  int recorded = 0;
   LKState* st = at_off<LKState>(ws, P.state);
   int* err_flag = reinterpret_cast<int*>(reinterpret_cast<char*>(st) + sizeof(LKState));
   cudaMemsetAsync(err_flag, 0, sizeof(int), s);
@@ -394,7 +414,10 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     for (int it = 0; it < P.iter; ++it) {
       const int mode = it == 0 ? mode0 : FIELD_CP;
       a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
+      const bool rec = prof && recorded < prof->capacity;
+      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
       accumulate(mode, a, grid, smem, mask, s);
+      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
       k_update<<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
                                                      (double)p->movRange, L.zratio_d);
@@ -411,6 +434,10 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     k_write_motion<FIELD_CP><<<grid_for(L0.n), kThreads, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   }
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
+  if (prof) {
+    prof->recorded = recorded;
+    prof->launches = count_launches(P, mmov != nullptr, mref != nullptr, init != nullptr);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "wr_lk_register launch");
   return WR_OK;
@@ -447,6 +474,14 @@ int wr_lk_workspace_size(int32_t nz, int32_t ny, int32_t nx, const WrLKParams* p
 int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
                    const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init, float* motion_out,
                    WrLKStats* stats, void* workspace, size_t workspace_bytes, void* stream) {
+  return wr_lk_register_profiled(mov, ref, excl_mask_mov, excl_mask_ref, p, motion_init, motion_out, stats,
+                                 workspace, workspace_bytes, stream, nullptr);
+}
+
+int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                            const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                            float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                            void* stream, WrProfile* prof) {
   int rc;
   if ((rc = check_volume(mov, "mov"))) return rc;
   if ((rc = check_volume(ref, "ref"))) return rc;
@@ -466,13 +501,13 @@ int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl
   switch (mov->dtype) {
     case WR_U16:
       return run_register<uint16_t>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, excl_mask_mov,
-                                    excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+                                    excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
     case WR_U8:
       return run_register<uint8_t>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, excl_mask_mov,
-                                   excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+                                   excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
     default:
       return run_register<float>(P, p, (const float*)mov->data, (const float*)ref->data, excl_mask_mov,
-                                 excl_mask_ref, motion_init, motion_out, stats, workspace, s);
+                                 excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
   }
 }
 

@@ -119,7 +119,7 @@ class LKRegistrar:
         self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
 
     def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
-                 motion_init=None, out=None, stream=None) -> torch.Tensor:
+                 motion_init=None, out=None, stream=None, profile=None) -> torch.Tensor:
         """Motion (z, y, x, 3) float32 registering ``mov`` onto ``ref``.
 
         Masks are (z, y, x) uint8/bool exclusion masks (True = excluded) or
@@ -149,9 +149,13 @@ class LKRegistrar:
             init_ptr = motion_init.data_ptr()
         if out is None:
             out = torch.empty(self.shape + (3,), dtype=torch.float32, device=self.device)
-        _lib.check("wr_lk_register", self.lib.wr_lk_register(
-            ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
-            out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream)))
+        args = (ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
+                out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream))
+        if profile is None:
+            _lib.check("wr_lk_register", self.lib.wr_lk_register(*args))
+        else:
+            _lib.check("wr_lk_register_profiled",
+                       self.lib.wr_lk_register_profiled(*args, ctypes.byref(profile.begin_call())))
         return out
 
     def stats(self) -> _lib.WrLKStats:
@@ -161,6 +165,59 @@ class LKRegistrar:
 
     def error_log(self):
         return stats_to_log(self.stats(), self.params.layer + 1)
+
+
+class KernelProfile:
+    """CUDA events around every launch of the fused iteration kernel.
+
+    ``begin_call`` hands a fresh slice of events to one registration call;
+    ``durations_ms`` (after a synchronize) returns one list per call.
+    """
+
+    def __init__(self, calls: int, per_call: int):
+        self.per_call = per_call
+        self.begin = [torch.cuda.Event(enable_timing=True) for _ in range(calls * per_call)]
+        self.end = [torch.cuda.Event(enable_timing=True) for _ in range(calls * per_call)]
+        for e in self.begin + self.end:
+            e.record()  # creates the underlying cudaEvent_t
+        torch.cuda.synchronize()
+        self._bh = (ctypes.c_void_p * len(self.begin))(*[e.cuda_event for e in self.begin])
+        self._eh = (ctypes.c_void_p * len(self.end))(*[e.cuda_event for e in self.end])
+        self.calls = 0
+        self.launches = []
+        self.recorded = []
+        self._prof = None
+
+    def begin_call(self) -> _lib.WrProfile:
+        if self._prof is not None:
+            self.recorded.append(self._prof.recorded)
+            self.launches.append(self._prof.launches)
+        off = self.calls * self.per_call
+        if off + self.per_call > len(self.begin):
+            raise RuntimeError("KernelProfile: out of events")
+        p = _lib.WrProfile()
+        p.acc_begin = ctypes.cast(ctypes.byref(self._bh, off * ctypes.sizeof(ctypes.c_void_p)),
+                                  ctypes.POINTER(ctypes.c_void_p))
+        p.acc_end = ctypes.cast(ctypes.byref(self._eh, off * ctypes.sizeof(ctypes.c_void_p)),
+                                ctypes.POINTER(ctypes.c_void_p))
+        p.capacity = self.per_call
+        self.calls += 1
+        self._prof = p
+        return p
+
+    def finish(self):
+        if self._prof is not None:
+            self.recorded.append(self._prof.recorded)
+            self.launches.append(self._prof.launches)
+            self._prof = None
+
+    def durations_ms(self):
+        self.finish()
+        out = []
+        for c in range(self.calls):
+            base = c * self.per_call
+            out.append([self.begin[base + i].elapsed_time(self.end[base + i]) for i in range(self.recorded[c])])
+        return out
 
 
 def warp(src: torch.Tensor, motion: torch.Tensor, out=None, stream=None) -> torch.Tensor:
