@@ -79,7 +79,8 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.nty = L.ncy + (L.ny > L.ncy * P.w ? 1 : 0);
     L.n = (long long)L.nx * L.ny * L.nz;
     L.ncp = (long long)L.ncx * L.ncy * L.nz;
-    L.nblk = (long long)L.ntx * L.nty * L.nz;
+    L.nstrips = (L.ntx + strip_windows(P.w) - 1) / strip_windows(P.w);
+    L.nblk = (long long)L.nstrips * L.nty * L.nz;
     L.zratio_d = (double)p->zRatio / (double)(1 << l);
     L.zratio = (float)L.zratio_d;
     double sx = resize_scale(nx, L.nx), sy = resize_scale(ny, L.ny);
@@ -145,8 +146,8 @@ template <typename T> static T* at_off(void* base, size_t off) {
 }
 
 static size_t iter_smem(int w) {
-  size_t hh = (size_t)(w + 2) * (w + 2);
-  return 4 * ((hh + 3) & ~size_t(3)) + 16 * (size_t)w * w + 4 * 33 * 10;
+  const int m = strip_windows(w);
+  return 16 * 3 * (size_t)(m + 2) + 4 * 10 * (size_t)strip_threads(w) + 4 * (size_t)m;
 }
 
 // Separable resize of a full-resolution volume to a level:
@@ -267,13 +268,9 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
 
 template <int MODE>
 static void launch_accumulate(const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
-  if (mask) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lk_accumulate<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lk_accumulate<MODE, true><<<grid, kThreads, smem, s>>>(a);
-  } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lk_accumulate<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lk_accumulate<MODE, false><<<grid, kThreads, smem, s>>>(a);
-  }
+  const int threads = strip_threads(a.w);
+  if (mask) k_lk_accumulate<MODE, true><<<grid, threads, smem, s>>>(a);
+  else k_lk_accumulate<MODE, false><<<grid, threads, smem, s>>>(a);
 }
 
 static void accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
@@ -407,8 +404,10 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     a.w = P.w;
     a.ntx = L.ntx;
     a.nty = L.nty;
+    a.wins_per_strip = strip_windows(P.w);
+    a.nstrips = L.nstrips;
     a.zratio = L.zratio;
-    const dim3 grid(L.ntx, L.nty, L.nz);
+    const dim3 grid(L.nz, L.nstrips, L.nty);
     const size_t smem = iter_smem(P.w);
     const int forced = p->forced_updates[l];
     for (int it = 0; it < P.iter; ++it) {

@@ -456,167 +456,286 @@ struct IterArgs {
   const uint8_t* __restrict__ mbits;   // null: no masks
   const float* __restrict__ mmov;      // null: no moving mask
   float* __restrict__ sums;            // ncp * 12: 9 window sums + 3 neighbour differences
-  double* __restrict__ errpart;        // per tile
-  double* __restrict__ penpart;        // per tile
+  double* __restrict__ errpart;        // per CTA
+  double* __restrict__ penpart;        // per CTA
   CPView cpv;                          // this level's CPs (motion_current at CPs)
   FieldSrc field;                      // motion used for this iteration
   int r, w, ntx, nty;
+  int wins_per_strip, nstrips;
   float zratio;
 };
 
-// One CTA per (window or leftover tile, z slice).  Pass 1 samples the warped
-// moving volume on the tile plus a one-voxel halo (the 3x3 It smoothing reads
-// it) and, inside the tile, the three gradients and the exclusion mask.
-// Pass 2 smooths It, applies the mask, accumulates It^2 for the error and the
-// nine gradient products for the window sum.  A window hanging over the
-// volume edge counts the edge voxel once per replicated position
-// (mode="nearest" of the (2r+1)^2 box filter, utils/calculate.py:51).
+// Central difference of two trilinear samples at c +- e_axis with the shifted
+// coordinate clipped to the volume (utils/calFlow3d_Wei_v1.py:134-206); the
+// general form, used within one voxel of the volume faces.
+__device__ __noinline__ float clipped_gradient(VolView v, float cx, float cy, float cz, int axis) {
+  if (axis == 0) {
+    const float hi = fminf(fmaxf(cx + 1.f, 0.f), (float)(v.nx - 1)), lo = fminf(fmaxf(cx - 1.f, 0.f), (float)(v.nx - 1));
+    return 0.5f * (sample_m(v, hi, cy, cz) - sample_m(v, lo, cy, cz));
+  }
+  if (axis == 1) {
+    const float hi = fminf(fmaxf(cy + 1.f, 0.f), (float)(v.ny - 1)), lo = fminf(fmaxf(cy - 1.f, 0.f), (float)(v.ny - 1));
+    return 0.5f * (sample_m(v, cx, hi, cz) - sample_m(v, cx, lo, cz));
+  }
+  const float hi = fminf(fmaxf(cz + 1.f, 0.f), (float)(v.nz - 1)), lo = fminf(fmaxf(cz - 1.f, 0.f), (float)(v.nz - 1));
+  return 0.5f * (sample_m(v, cx, cy, hi) - sample_m(v, cx, cy, lo));
+}
+
+// warped moving exclusion mask > 0, evaluated exactly (float64 sum, float32 result)
+__device__ __noinline__ bool warped_mask_exact(const float* mmov, int nx, int ny, int nz, float cx, float cy, float cz) {
+  return sample_f64(mmov, nx, ny, nz, cx, cy, cz) > 0.f;
+}
+
+constexpr int kOutPerWarp = 30;   // lanes 1..30 of a warp own output columns; 0 and 31 are halo
+
+// Threads per CTA of the column walk and windows per strip for a patch width.
+__host__ __device__ inline int strip_windows(int w) { int m = 240 / w; return m < 1 ? 1 : m; }
+__host__ __device__ inline int strip_threads(int w) {
+  int cols = strip_windows(w) * w;
+  return 32 * ((cols + kOutPerWarp - 1) / kOutPerWarp);
+}
+
+__device__ __forceinline__ float3 lerp3(const float3& a, const float3& b, float t) {
+  return make_float3(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z));
+}
+__device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float t) {
+  return make_float4(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z),
+                     fmaf(t, b.w - a.w, a.w));
+}
+
+// Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588) as a column walk.
+//
+// A CTA owns one z slice, one row of windows (2r+1 rows) and a strip of
+// whole windows along x.  Each lane owns one column and walks down the rows
+// (plus a halo row above and below): per voxel it evaluates the motion,
+// samples the warped moving level and its gradients with one set of 8 float4
+// corner loads (the previous row's corners are reused when the sample row
+// advances by one), and forms It_raw = ref - warped.  The 3x3 box smoothing
+// of It is a running 3-row sum per lane plus the two neighbouring lanes'
+// sums (warps overlap by two columns, so no CTA barrier is needed in the
+// walk).  Smoothed It, masked gradients and their nine products accumulate
+// per lane; a fixed-order reduction then gives each window's sums (a window
+// hanging over the volume edge counts the edge voxel once per replicated
+// position, mode="nearest" of utils/calculate.py:51) and the CTA's It^2 sum.
 template <int MODE, bool MASK>
-__global__ void __launch_bounds__(kThreads) k_lk_accumulate(IterArgs a) {
+__global__ void __launch_bounds__(256, 3) k_lk_accumulate(IterArgs a) {
   if (!a.st->active) return;
   extern __shared__ float smem[];
   const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
-  const int tx = blockIdx.x, ty = blockIdx.y, z = blockIdx.z;
+  const int w = a.w, r = a.r;
   const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
-  const bool window = (tx < ncx) && (ty < ncy);
-  const int x0 = tx * a.w, y0 = ty * a.w;
-  const int xe = min(x0 + a.w, nx), ye = min(y0 + a.w, ny);
-  const int wx = xe - x0, wy = ye - y0;
-  const int hw = wx + 2, hh = wy + 2;
-  float* it_raw = smem;                                   // hh * hw
-  float4* gsm = reinterpret_cast<float4*>(smem + ((hh * hw + 3) & ~3));   // wy * wx
-  float* red = reinterpret_cast<float*>(gsm + wx * wy);   // reduction scratch
+  const int z = blockIdx.x, strip = blockIdx.y, ty = blockIdx.z;
+  const int wa = strip * a.wins_per_strip;
+  const int wb = min(wa + a.wins_per_strip, a.ntx);
+  const int x0 = wa * w, xe = min(wb * w, nx);
+  const int y0 = ty * w, ye = min(y0 + w, ny);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = x0 - 1 + warp * kOutPerWarp + lane;
+  const bool own = lane >= 1 && lane <= kOutPerWarp && col >= x0 && col < xe;
+  const bool warp_active = x0 + warp * kOutPerWarp < xe;
+  const int gx = clampi(col, 0, nx - 1);
 
-  // pass 1
-  for (int h = threadIdx.x; h < hh * hw; h += blockDim.x) {
-    const int hy = h / hw, hx = h - hy * hw;
-    const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
-    const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
-    const bool inner = hx >= 1 && hx <= wx && hy >= 1 && hy <= wy;
-    const float3 m = eval_field<MODE>(a.field, gx, gy, z);
-    const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = (float)z + m.z;
-    int ix0, iy0, iz0;
-    float fx, fy, fz;
-    split_coord(cx, ix0, fx);
-    split_coord(cy, iy0, fy);
-    split_coord(cz, iz0, fz);
-    const int xa = clampi(ix0, 0, nx - 1), xb = clampi(ix0 + 1, 0, nx - 1);
-    const int ya = clampi(iy0, 0, ny - 1), yb = clampi(iy0 + 1, 0, ny - 1);
-    const int za = clampi(iz0, 0, nz - 1), zb = clampi(iz0 + 1, 0, nz - 1);
-    const float4 c000 = at(a.mov, xa, ya, za), c001 = at(a.mov, xb, ya, za);
-    const float4 c010 = at(a.mov, xa, yb, za), c011 = at(a.mov, xb, yb, za);
-    const float4 c100 = at(a.mov, xa, ya, zb), c101 = at(a.mov, xb, ya, zb);
-    const float4 c110 = at(a.mov, xa, yb, zb), c111 = at(a.mov, xb, yb, zb);
-    // interpolate all four channels with shared weights
-    float4 e00, e01, e10, e11, f0, f1, s;
-#define WR_LERP4(o, p, q, t) \
-  o.x = fmaf(t, q.x - p.x, p.x); o.y = fmaf(t, q.y - p.y, p.y); \
-  o.z = fmaf(t, q.z - p.z, p.z); o.w = fmaf(t, q.w - p.w, p.w);
-    WR_LERP4(e00, c000, c001, fx)
-    WR_LERP4(e01, c010, c011, fx)
-    WR_LERP4(e10, c100, c101, fx)
-    WR_LERP4(e11, c110, c111, fx)
-    WR_LERP4(f0, e00, e01, fy)
-    WR_LERP4(f1, e10, e11, fy)
-    WR_LERP4(s, f0, f1, fz)
-#undef WR_LERP4
-    const size_t p = ((size_t)z * ny + gy) * nx + gx;
-    it_raw[h] = __ldg(a.ref + p) - s.x;
-    if (inner) {
-      // central differences of samples at c +- e_k, clipped to the volume:
-      // inside [1, n-2] they equal the sample of the precomputed difference
-      float gxv, gyv, gzv;
-      if (cx >= 1.f && cx <= (float)(nx - 2)) gxv = s.y;
-      else gxv = 0.5f * (sample_m(a.mov, fminf(fmaxf(cx + 1.f, 0.f), (float)(nx - 1)), cy, cz) -
-                         sample_m(a.mov, fminf(fmaxf(cx - 1.f, 0.f), (float)(nx - 1)), cy, cz));
-      if (cy >= 1.f && cy <= (float)(ny - 2)) gyv = s.z;
-      else gyv = 0.5f * (sample_m(a.mov, cx, fminf(fmaxf(cy + 1.f, 0.f), (float)(ny - 1)), cz) -
-                         sample_m(a.mov, cx, fminf(fmaxf(cy - 1.f, 0.f), (float)(ny - 1)), cz));
-      if (cz >= 1.f && cz <= (float)(nz - 2)) gzv = s.w;
-      else gzv = 0.5f * (sample_m(a.mov, cx, cy, fminf(fmaxf(cz + 1.f, 0.f), (float)(nz - 1))) -
-                         sample_m(a.mov, cx, cy, fminf(fmaxf(cz - 1.f, 0.f), (float)(nz - 1))));
-      float excl = 0.f;
-      if (MASK) {
-        bool ex = (a.mbits[p] & 1) != 0;
-        if (!ex && a.mmov) {
-          bool in_range = cx >= 0.f && cx <= (float)(nx - 1) && cy >= 0.f && cy <= (float)(ny - 1) &&
-                          cz >= 0.f && cz <= (float)(nz - 1);
-          int code = 2;
-          if (in_range) code = (a.mbits[((size_t)iz0 * ny + iy0) * nx + ix0] >> 1) & 3;
-          if (code == 1) ex = true;
-          else if (code == 2) ex = sample_f64(a.mmov, nx, ny, nz, cx, cy, cz) > 0.f;
-        }
-        excl = ex ? 1.f : 0.f;
-      }
-      gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
-    }
+  // CP tile: rows ty-1..ty+1, columns wa-1..wb (edge-clamped)
+  const int tile_w = wb - wa + 2;
+  float4* cpt = reinterpret_cast<float4*>(smem);
+  float* part = smem + 4 * 3 * tile_w;            // blockDim.x * 10 per-lane partials
+  float* wpen = part + blockDim.x * 10;           // per-window penalty
+  for (int i = threadIdx.x; i < 3 * tile_w; i += blockDim.x) {
+    const int jr = i / tile_w, jc = i - jr * tile_w;
+    const int cy = clampi(ty - 1 + jr, 0, ncy - 1), cx = clampi(wa - 1 + jc, 0, ncx - 1);
+    cpt[i] = a.cpv.cp[((size_t)z * ncy + cy) * ncx + cx];
   }
   __syncthreads();
 
-  // pass 2
   float acc[10];
 #pragma unroll
   for (int k = 0; k < 10; ++k) acc[k] = 0.f;
-  for (int i = threadIdx.x; i < wx * wy; i += blockDim.x) {
-    const int ly = i / wx, lx = i - ly * wx;
-    const float* rp = it_raw + ly * hw + lx;
-    float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
-               (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
-    it *= (1.f / 9.f);
-    float4 g = gsm[i];
-    if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
-    acc[9] += it * it;
-    if (window) {
-      const int gx = x0 + lx, gy = y0 + ly;
-      const float mx = (gx == nx - 1) ? (float)(x0 + a.w - (nx - 1)) : 1.f;
-      const float my = (gy == ny - 1) ? (float)(y0 + a.w - (ny - 1)) : 1.f;
-      const float wt = mx * my;
-      const float iz = g.z / a.zratio;
-      const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
-      acc[0] += wgx * g.x;
-      acc[1] += wgx * g.y;
-      acc[2] += wgx * iz;
-      acc[3] += wgy * g.y;
-      acc[4] += wgy * iz;
-      acc[5] += wgz * iz;
-      acc[6] += wgx * it;
-      acc[7] += wgy * it;
-      acc[8] += wgz * it;
+
+  if (warp_active) {
+    // x part of the CP interpolation is fixed for the column
+    int cx0 = 0, cx1 = 0;
+    float txc = 0.f;
+    if (MODE == FIELD_CP) {
+      float gxc = __fdiv_rn((float)(gx - r), (float)w);
+      gxc = fminf(fmaxf(gxc, 0.f), (float)ncx);
+      const float fxc = floorf(gxc);
+      txc = gxc - fxc;
+      cx0 = min((int)fxc, ncx - 1) - (wa - 1);
+      cx1 = min((int)fxc + 1, ncx - 1) - (wa - 1);
+    }
+    const int wx_idx = gx / w;      // window column of an owned voxel
+    const bool win_col = own && (col / w) < ncx && ty < ncy;
+    const float mx = (gx == nx - 1) ? (float)(wx_idx * w + w - (nx - 1)) : 1.f;
+    const size_t zoff = (size_t)z * ny * nx;
+    // corners of the upper y tap row, kept for the next row: (za,xa) (za,xb) (zb,xa) (zb,xb)
+    float4 cb0 = make_float4(0.f, 0.f, 0.f, 0.f), cb1 = cb0, cb2 = cb0, cb3 = cb0;
+    int pxa = -1, pxb = -1, pyb = -1, pza = -1, pzb = -1;
+    float r0 = 0.f, r1 = 0.f;                        // It_raw of the two rows above
+    float4 gprev = make_float4(0.f, 0.f, 0.f, 0.f);  // gradients + exclusion of the previous row
+    const int R = (ye - y0) + 2;
+    for (int i = 0; i < R; ++i) {
+      const int gyu = y0 - 1 + i;
+      const int gy = clampi(gyu, 0, ny - 1);
+      float3 m;
+      if (MODE == FIELD_CP) {
+        float gyc = __fdiv_rn((float)(gy - r), (float)w);
+        gyc = fminf(fmaxf(gyc, 0.f), (float)ncy);
+        const float fyc = floorf(gyc), tyc = gyc - fyc;
+        const int j0 = (min((int)fyc, ncy - 1) - ty + 1) * tile_w;
+        const int j1 = (min((int)fyc + 1, ncy - 1) - ty + 1) * tile_w;
+        const float4 p0 = cpt[j0 + cx0], p1 = cpt[j0 + cx1], q0 = cpt[j1 + cx0], q1 = cpt[j1 + cx1];
+        const float3 B0 = make_float3(fmaf(txc, p1.x - p0.x, p0.x), fmaf(txc, p1.y - p0.y, p0.y),
+                                      fmaf(txc, p1.z - p0.z, p0.z));
+        const float3 B1 = make_float3(fmaf(txc, q1.x - q0.x, q0.x), fmaf(txc, q1.y - q0.y, q0.y),
+                                      fmaf(txc, q1.z - q0.z, q0.z));
+        m = lerp3(B0, B1, tyc);
+      } else {
+        m = eval_field<MODE>(a.field, gx, gy, z);
+      }
+      const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = (float)z + m.z;
+      int ix0, iy0, iz0;
+      float fx, fy, fz;
+      split_coord(cx, ix0, fx);
+      split_coord(cy, iy0, fy);
+      split_coord(cz, iz0, fz);
+      const int xa = clampi(ix0, 0, nx - 1), xb = clampi(ix0 + 1, 0, nx - 1);
+      const int ya = clampi(iy0, 0, ny - 1), yb = clampi(iy0 + 1, 0, ny - 1);
+      const int za = clampi(iz0, 0, nz - 1), zb = clampi(iz0 + 1, 0, nz - 1);
+      const float4* G = a.mov.g;
+      const size_t oza = (size_t)za * ny * nx, ozb = (size_t)zb * ny * nx;
+      float4 ca0, ca1, ca2, ca3;
+      const bool same_xz = xa == pxa && xb == pxb && za == pza && zb == pzb;
+      if (same_xz && ya == pyb) {
+        // the sample row advanced by one: the old upper row is the new lower row
+        ca0 = cb0; ca1 = cb1; ca2 = cb2; ca3 = cb3;
+      } else {
+        const size_t ra = (size_t)ya * nx;
+        ca0 = __ldg(G + oza + ra + xa); ca1 = __ldg(G + oza + ra + xb);
+        ca2 = __ldg(G + ozb + ra + xa); ca3 = __ldg(G + ozb + ra + xb);
+      }
+      if (!(same_xz && yb == pyb)) {
+        const size_t rb = (size_t)yb * nx;
+        cb0 = __ldg(G + oza + rb + xa); cb1 = __ldg(G + oza + rb + xb);
+        cb2 = __ldg(G + ozb + rb + xa); cb3 = __ldg(G + ozb + rb + xb);
+      }
+      pxa = xa; pxb = xb; pyb = yb; pza = za; pzb = zb;
+      const float4 e0 = lerp4(ca0, ca1, fx), e1 = lerp4(cb0, cb1, fx);
+      const float4 e2 = lerp4(ca2, ca3, fx), e3 = lerp4(cb2, cb3, fx);
+      const float4 s = lerp4(lerp4(e0, e1, fy), lerp4(e2, e3, fy), fz);
+      const float r2 = __ldg(a.ref + zoff + (size_t)gy * nx + gx) - s.x;
+
+      // output row i-1 once its lower neighbour row is known
+      if (i >= 2) {
+        const float v = r0 + r1 + r2;
+        const float vl = __shfl_up_sync(0xffffffffu, v, 1);
+        const float vr = __shfl_down_sync(0xffffffffu, v, 1);
+        if (own) {
+          float it = (vl + v + vr) * (1.f / 9.f);
+          float4 g = gprev;
+          if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
+          acc[9] = fmaf(it, it, acc[9]);
+          if (win_col) {
+            const int gyo = gyu - 1;
+            const float my = (gyo == ny - 1) ? (float)(ty * w + w - (ny - 1)) : 1.f;
+            const float wt = mx * my;
+            const float iz = g.z / a.zratio;
+            const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
+            acc[0] = fmaf(wgx, g.x, acc[0]);
+            acc[1] = fmaf(wgx, g.y, acc[1]);
+            acc[2] = fmaf(wgx, iz, acc[2]);
+            acc[3] = fmaf(wgy, g.y, acc[3]);
+            acc[4] = fmaf(wgy, iz, acc[4]);
+            acc[5] = fmaf(wgz, iz, acc[5]);
+            acc[6] = fmaf(wgx, it, acc[6]);
+            acc[7] = fmaf(wgy, it, acc[7]);
+            acc[8] = fmaf(wgz, it, acc[8]);
+          }
+        }
+      }
+      // gradients and exclusion of this row (used when the next row arrives)
+      if (own && i >= 1 && i <= R - 2) {
+        float gxv = s.y, gyv = s.z, gzv = s.w;
+        if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient(a.mov, cx, cy, cz, 0);
+        if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient(a.mov, cx, cy, cz, 1);
+        if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient(a.mov, cx, cy, cz, 2);
+        float excl = 0.f;
+        if (MASK) {
+          bool ex = (__ldg(a.mbits + zoff + (size_t)gy * nx + gx) & 1) != 0;
+          if (!ex && a.mmov) {
+            const bool in_range = cx >= 0.f && cx <= (float)(nx - 1) && cy >= 0.f && cy <= (float)(ny - 1) &&
+                                  cz >= 0.f && cz <= (float)(nz - 1);
+            int code = 2;
+            if (in_range) code = (__ldg(a.mbits + ((size_t)iz0 * ny + iy0) * nx + ix0) >> 1) & 3;
+            if (code == 1) ex = true;
+            else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
+          }
+          excl = ex ? 1.f : 0.f;
+        }
+        gprev = make_float4(gxv, gyv, gzv, excl);
+      }
+      r0 = r1;
+      r1 = r2;
     }
   }
-  block_sum<10>(acc, red);
 
-  const long long blk = ((long long)z * a.nty + ty) * a.ntx + tx;
-  if (threadIdx.x == 0) {
-    a.errpart[blk] = (double)acc[9];
-    double pen = 0.0;
-    if (window) {
-      const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
-      float* s = a.sums + cpi * 12;
+  // fixed-order reduction: per-lane partials -> windows and CTA error
 #pragma unroll
-      for (int k = 0; k < 9; ++k) s[k] = acc[k];
+  for (int k = 0; k < 10; ++k) part[threadIdx.x * 10 + k] = acc[k];
+  __syncthreads();
+  const long long blk = ((long long)ty * a.nstrips + strip) * nz + z;
+  const int nwin = wb - wa;
+  if (threadIdx.x < nwin) {
+    const int k = wa + threadIdx.x;
+    if (k < ncx && ty < ncy) {
+      float s[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) s[q] = 0.f;
+      const int c0 = k * w, c1 = min(c0 + w, nx);
+      for (int c = c0; c < c1; ++c) {
+        const int rel = c - x0;
+        const int t = (rel / kOutPerWarp) * 32 + rel % kOutPerWarp + 1;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) s[q] += part[t * 10 + q];
+      }
+      const long long cpi = ((long long)z * ncy + ty) * ncx + k;
+      float* o = a.sums + cpi * 12;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) o[q] = s[q];
       // neighbour difference on the CP grid (getNeiDiff with r = 1,
       // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
       // neighbours (edge-replicated) minus the centre, float64 then float32
-      const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
       double sx = 0.0, sy = 0.0, sz = 0.0;
       for (int dy = -1; dy <= 1; ++dy)
         for (int dx = -1; dx <= 1; ++dx) {
           if (dx == 0 && dy == 0) continue;
-          const float4 v = b[clampi(ty + dy, 0, ncy - 1) * ncx + clampi(tx + dx, 0, ncx - 1)];
+          const int cy = clampi(ty + dy, 0, ncy - 1) - ty + 1;
+          const int cxi = clampi(k + dx, 0, ncx - 1) - (wa - 1);
+          const float4 v = cpt[cy * tile_w + cxi];
           sx += 0.125 * (double)v.x;
           sy += 0.125 * (double)v.y;
           sz += 0.125 * (double)v.z;
         }
-      const float4 c = b[ty * ncx + tx];
+      const float4 c = cpt[tile_w + (k - (wa - 1))];
       const float ndx = (float)(sx - (double)c.x);
       const float ndy = (float)(sy - (double)c.y);
       const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
-      s[9] = ndx;
-      s[10] = ndy;
-      s[11] = ndz;
-      pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
+      o[9] = ndx;
+      o[10] = ndy;
+      o[11] = ndz;
+      wpen[threadIdx.x] = ndx * ndx + ndy * ndy + ndz * ndz;
     }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    for (int c = x0; c < xe; ++c) {
+      const int rel = c - x0;
+      e += (double)part[((rel / kOutPerWarp) * 32 + rel % kOutPerWarp + 1) * 10 + 9];
+    }
+    a.errpart[blk] = e;
+    double pen = 0.0;
+    for (int t = 0; t < nwin; ++t)
+      if (wa + t < ncx && ty < ncy) pen += (double)wpen[t];
     a.penpart[blk] = pen;
   }
 }

@@ -16,9 +16,10 @@ struct LevelPlan {
   int nx, ny, nz;     // level extent (x fastest)
   int ncx, ncy;       // control points per slice along x and y
   int ntx, nty;       // tiles: one per window plus a leftover tile if needed
+  int nstrips;        // CTAs along x of the fused iteration kernel
   long long n;        // voxels
   long long ncp;      // control points (ncx * ncy * nz)
-  long long nblk;     // tiles of the fused iteration kernel
+  long long nblk;     // CTAs of the fused iteration kernel
   float zratio;       // zRatio / 2^layer
   double zratio_d;
   // pass order of the separable resize from full resolution (x first when
