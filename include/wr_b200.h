@@ -180,6 +180,26 @@ WR_API int wr_warp_trilinear(const WrVolume* src, const float* motion, float* ou
 WR_API int wr_penalty_factor(const WrVolume* ref, const uint8_t* excl_mask_ref, double* factor_out,
                       void* scratch, size_t scratch_bytes, void* stream);
 
+/*
+ * wr_penalty_factor for callers that cannot allocate device memory: no
+ * counterpart in the reference (whose NumPy/CuPy code allocates freely).
+ * Callers that embed the library in a host application whose device memory
+ * is owned by its own pool (a stray cudaMalloc would fail or break the pool's
+ * accounting), or acquisition loops that must not enter the allocator
+ * between frames, call this form: it takes the same inputs and output as
+ * wr_penalty_factor and allocates nothing.  Its per-block partial sums live
+ * in a 256 KiB static device array that every device loading the library
+ * holds until exit; volumes above 134,217,728 voxels (128 x 1024 x 1024) are
+ * rejected with WR_E_SHAPE.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current, so
+ * make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  Nothing in the array needs to start
+ * at zero; each call writes every slot it reads.
+ */
+WR_API int wr_penalty_factor_noalloc(const WrVolume* ref, const uint8_t* excl_mask_ref, double* factor_out,
+                                     void* stream);
+
 /* Scratch bytes wr_penalty_factor needs for this shape. */
 WR_API int wr_penalty_factor_scratch(int32_t nz, int32_t ny, int32_t nx, size_t* bytes);
 

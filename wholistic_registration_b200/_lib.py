@@ -37,6 +37,7 @@ EXPORTS = (
     "wr_lk_register_profiled",
     "wr_warp_trilinear",
     "wr_penalty_factor",
+    "wr_penalty_factor_noalloc",
     "wr_penalty_factor_scratch",
     "wr_resize_table",
 )
@@ -129,6 +130,7 @@ def load():
         lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
         lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_penalty_factor.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp, sz, vp]
+        lib.wr_penalty_factor_noalloc.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_penalty_factor_scratch.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
         lib.wr_resize_table.argtypes = [i32, i32, i32, vp, vp, ctypes.POINTER(i32)]
         for name in EXPORTS:

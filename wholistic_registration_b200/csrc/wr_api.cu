@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 
 #include "wr_b200.h"
@@ -442,6 +443,40 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   return WR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// penalty factor without allocation: per-block partial sums in a static array
+// ---------------------------------------------------------------------------
+
+// Each block of the no-alloc variant reduces a fixed 16,384-voxel span, so a
+// volume needs ceil(n / 16384) partial slots; 8,192 slots of 4 doubles
+// (256 KiB, resident on every device that loads the library) cover volumes of
+// up to 134,217,728 voxels (128 x 1024 x 1024).
+constexpr int kNoAllocVoxelsPerBlock = kThreads * 64;
+constexpr int kNoAllocSlots = 8192;
+constexpr long long kNoAllocMaxVoxels = (long long)kNoAllocSlots * kNoAllocVoxelsPerBlock;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocSlots * 4];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_dev_ptr[128] = {};
+
+// Device address of the static scratch for the current device, looked up once
+// per device (host code may not use the symbol itself as a device pointer).
+static int noalloc_partials(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "wr_penalty_factor_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 128) return fail(WR_E_PARAM, "wr_penalty_factor_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_dev_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess) return cuda_fail(e, "wr_penalty_factor_noalloc: cudaGetSymbolAddress");
+    g_noalloc_dev_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_dev_ptr[dev];
+  return WR_OK;
+}
+
 static int check_volume(const WrVolume* v, const char* name) {
   if (!v || !v->data) return fail(WR_E_NULL, (std::string(name) + " is NULL").c_str());
   if (v->dtype != WR_U8 && v->dtype != WR_U16 && v->dtype != WR_F32)
@@ -562,6 +597,37 @@ int wr_penalty_factor(const WrVolume* ref, const uint8_t* excl_mask_ref, double*
   k_penalty_final<<<1, 1024, 0, s>>>(part, nblk, factor_out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "wr_penalty_factor launch");
+  return WR_OK;
+}
+
+int wr_penalty_factor_noalloc(const WrVolume* ref, const uint8_t* excl_mask_ref, double* factor_out,
+                              void* stream) {
+  int rc;
+  if ((rc = check_volume(ref, "ref"))) return rc;
+  if (!factor_out) return fail(WR_E_NULL, "factor_out is NULL");
+  if (ref->nx < 3 || ref->ny < 3) return fail(WR_E_SHAPE, "ref needs at least 3 voxels along x and y");
+  const long long n = (long long)ref->nz * ref->ny * ref->nx;
+  if (n > kNoAllocMaxVoxels)
+    return fail(WR_E_SHAPE, "wr_penalty_factor_noalloc: volume exceeds the 134217728-voxel capacity of its static "
+                            "scratch; use wr_penalty_factor with caller-provided scratch");
+  double* part = nullptr;
+  if ((rc = noalloc_partials(&part))) return rc;
+  const int nblk = (int)((n + kNoAllocVoxelsPerBlock - 1) / kNoAllocVoxelsPerBlock);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // every slot read by the final reduction is written by this call's blocks
+  switch (ref->dtype) {
+    case WR_U16:
+      k_penalty_partial<uint16_t><<<nblk, kThreads, 0, s>>>((const uint16_t*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+      break;
+    case WR_U8:
+      k_penalty_partial<uint8_t><<<nblk, kThreads, 0, s>>>((const uint8_t*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+      break;
+    default:
+      k_penalty_partial<float><<<nblk, kThreads, 0, s>>>((const float*)ref->data, excl_mask_ref, part, ref->nz, ref->ny, ref->nx);
+  }
+  k_penalty_final<<<1, 1024, 0, s>>>(part, nblk, factor_out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "wr_penalty_factor_noalloc launch");
   return WR_OK;
 }
 
