@@ -209,9 +209,13 @@ def run_ours(args, wl, rank, world, local_rank):
     warped = torch.empty(wl["shape"], dtype=torch.float32, device=device)
     stats_hist = torch.zeros((args.steps, reg.stats_dev.numel()), dtype=torch.uint8, device=device)
 
+    ref_ready = [False]
+
     def step(k, prof=None, keep_stats=False):
         f = frames[k % len(frames)]
-        reg.register(f, template, excl, excl, None, out=motion, profile=prof)
+        # the template's pyramid is built by the first call and reused for the series
+        reg.register(f, template, excl, excl, None, out=motion, profile=prof, reuse_reference=ref_ready[0])
+        ref_ready[0] = True
         warp(f, motion, out=warped)
         if keep_stats:
             stats_hist[k].copy_(reg.stats_dev, non_blocking=True)

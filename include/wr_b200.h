@@ -72,6 +72,14 @@ enum {
   WR_PREC_BF16 = 2   /* mixed: levels and gradients stored as bfloat16 */
 };
 
+/* WrLKParams.flags */
+enum {
+  /* The workspace already holds the pyramid of this `ref` and `excl_mask_ref`
+     from an earlier call with the same shape and parameters: skip rebuilding
+     them (a time series registered against one template). */
+  WR_LK_REUSE_REFERENCE = 1
+};
+
 /* A volume: device pointer, element type and (z, y, x) extent. */
 typedef struct {
   const void* data;
@@ -92,7 +100,7 @@ typedef struct {
   double smoothPenalty;   /* option["smoothPenalty"], already normalised */
   double tol;             /* option["tol"]: |delta error| stopping threshold */
   int32_t precision;      /* WR_PREC_* */
-  int32_t reserved;
+  int32_t flags;          /* WR_LK_* bits */
   /* -1: the reference's stopping rules; n >= 0: perform exactly n motion
      updates at that level (replays another run's iteration counts) */
   int32_t forced_updates[WR_MAX_LEVELS];

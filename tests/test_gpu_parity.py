@@ -166,3 +166,23 @@ def test_argument_errors_raise_value_error():
     big["layer"] = 4
     with pytest.raises(ValueError):
         cf3.getMotion(arrays["mov"], arrays["ref"], big)
+
+
+def test_reuse_reference_matches_fresh_registration():
+    """Registering a second frame with the template pyramid kept from the
+    first call gives the same field as a fresh registration."""
+    _cf3()
+    from wholistic_registration_b200 import LKParams, LKRegistrar, synthetic
+
+    shape = (8, 96, 80)
+    tmpl, mov1, _ = synthetic.make_pair(shape, 21, n_blobs=300, max_disp=(2.5, 2.5, 0.8))
+    _, mov2, _ = synthetic.make_pair(shape, 22, n_blobs=300, max_disp=(2.5, 2.5, 0.8), template=tmpl.float())
+    excl = (~synthetic.ellipsoid_inclusion(shape, 0.75)).to(torch.uint8)
+    t, m1, m2, e = (x.cuda().contiguous() for x in (tmpl, mov1, mov2, excl))
+    p = LKParams(layer=2, iter=10, r=4, zRatio=1.0, movRange=5.0, smoothPenalty=200.0, tol=1e-3)
+    a = LKRegistrar(shape, p)
+    a.register(m1, t, e, e)
+    kept = a.register(m2, t, e, e, reuse_reference=True).clone()
+    b = LKRegistrar(shape, p)
+    fresh = b.register(m2, t, e, e)
+    torch.testing.assert_close(kept, fresh, rtol=0, atol=0)

@@ -19,6 +19,7 @@ MAX_ITERS = 64
 
 WR_U8, WR_U16, WR_F32 = 1, 2, 3
 WR_PREC_F32, WR_PREC_F16, WR_PREC_BF16 = 0, 1, 2
+WR_LK_REUSE_REFERENCE = 1
 
 ERRORS = {
     1: "WR_E_NULL",
@@ -63,7 +64,7 @@ class WrLKParams(ctypes.Structure):
         ("smoothPenalty", ctypes.c_double),
         ("tol", ctypes.c_double),
         ("precision", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
         ("forced_updates", ctypes.c_int32 * MAX_LEVELS),
     ]
 

@@ -79,9 +79,9 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.ntx = L.ncx + (L.nx > L.ncx * P.w ? 1 : 0);
     L.nty = L.ncy + (L.ny > L.ncy * P.w ? 1 : 0);
     L.n = (long long)L.nx * L.ny * L.nz;
+    if (L.n >= (1LL << 31)) { *why = "a pyramid level holds 2^31 voxels or more"; return WR_E_SHAPE; }
     L.ncp = (long long)L.ncx * L.ncy * L.nz;
-    L.nstrips = (L.ntx + strip_windows(P.w) - 1) / strip_windows(P.w);
-    L.nblk = (long long)L.nstrips * L.nty * L.nz;
+    L.nblk = (long long)L.ntx * L.nty * L.nz;
     L.zratio_d = (double)p->zRatio / (double)(1 << l);
     L.zratio = (float)L.zratio_d;
     double sx = resize_scale(nx, L.nx), sy = resize_scale(ny, L.ny);
@@ -146,10 +146,7 @@ template <typename T> static T* at_off(void* base, size_t off) {
   return reinterpret_cast<T*>(static_cast<char*>(base) + off);
 }
 
-static size_t iter_smem(int w) {
-  const int m = strip_windows(w);
-  return 16 * 3 * (size_t)(m + 2) + 4 * 10 * (size_t)strip_threads(w) + 4 * (size_t)m;
-}
+static size_t iter_smem(int w) { return accumulate_smem(w); }
 
 // Separable resize of a full-resolution volume to a level:
 // first pass (x or y, by scale order) into tmp, second pass into `out`.
@@ -198,26 +195,28 @@ static void resize_mask_to_level(const Plan& P, const LevelPlan& L, void* ws, co
 
 template <typename T>
 static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, const uint8_t* mmov_u8,
-                          const uint8_t* mref_u8, cudaStream_t s) {
+                          const uint8_t* mref_u8, bool reuse_ref, cudaStream_t s) {
+  const bool same_mask = mmov_u8 != nullptr && mmov_u8 == mref_u8 && !reuse_ref;
   for (int l = 0; l < P.levels; ++l) {
     const LevelPlan& L = P.lv[l];
     float* refl = at_off<float>(ws, L.ref);
     float4* movg = at_off<float4>(ws, L.movg);
     float* mmov = at_off<float>(ws, L.mmov);
     uint8_t* bits = at_off<uint8_t>(ws, L.mbits);
+    const bool any_mask = mmov_u8 || mref_u8;
     if (l == 0) {
       // scale 1 on every axis: the resize is an exact copy
-      k_to_float<T><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
+      if (!reuse_ref) k_to_float<T><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
       k_pack_movg<T><<<grid_for(L.n), kThreads, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
       if (mmov_u8) k_u8_to_unit_f<<<grid_for(L.n), kThreads, 0, s>>>(mmov_u8, mmov, L.n);
-      if (mmov_u8 || mref_u8)
-        k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(nullptr, mref_u8, mmov_u8 ? mmov : nullptr, bits, L.nz,
-                                                        L.ny, L.nx);
+      if (any_mask)
+        k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8 ? mmov : nullptr,
+                                                        bits, L.nz, L.ny, L.nx, reuse_ref ? 1 : 0);
       continue;
     }
     float* tmpf = at_off<float>(ws, P.tmp_a);
     float* levf = at_off<float>(ws, P.tmp_b);
-    resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, refl, s);
+    if (!reuse_ref) resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, refl, s);
     resize_to_level<T, float, float>(P, L, ws, mov, 1, 0, tmpf, levf, s);
     k_pack_movg<float><<<grid_for(L.n), kThreads, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
     double* tmpd = at_off<double>(ws, P.tmp_a);
@@ -226,10 +225,12 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
       resize_mask_to_level(P, L, ws, mmov_u8, tmpd, levd, s);
       k_d_to_f<<<grid_for(L.n), kThreads, 0, s>>>(levd, mmov, L.n);
     }
-    if (mref_u8) resize_mask_to_level(P, L, ws, mref_u8, tmpd, levd, s);
-    if (mmov_u8 || mref_u8)
-      k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(mref_u8 ? levd : nullptr, nullptr, mmov_u8 ? mmov : nullptr,
-                                                      bits, L.nz, L.ny, L.nx);
+    // one exclusion mask for both volumes: its resize is already in levd
+    if (mref_u8 && !reuse_ref && !same_mask) resize_mask_to_level(P, L, ws, mref_u8, tmpd, levd, s);
+    if (any_mask)
+      k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>((mref_u8 && !reuse_ref) ? levd : nullptr, nullptr,
+                                                      mmov_u8 ? mmov : nullptr, bits, L.nz, L.ny, L.nx,
+                                                      reuse_ref ? 1 : 0);
   }
 }
 
@@ -269,9 +270,15 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
 
 template <int MODE>
 static void launch_accumulate(const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
-  const int threads = strip_threads(a.w);
-  if (mask) k_lk_accumulate<MODE, true><<<grid, threads, smem, s>>>(a);
-  else k_lk_accumulate<MODE, false><<<grid, threads, smem, s>>>(a);
+  if (mask) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_lk_accumulate<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lk_accumulate<MODE, true><<<grid, kAccThreads, smem, s>>>(a);
+  } else {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_lk_accumulate<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lk_accumulate<MODE, false><<<grid, kAccThreads, smem, s>>>(a);
+  }
 }
 
 static void accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
@@ -285,14 +292,21 @@ static void accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool
 
 template <int MODE0>
 static void level_first(const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f, bool cp_init,
-                        bool diff, cudaStream_t s) {
+                        const IterArgs* diff, cudaStream_t s) {
   if (cp_init)
     k_cp_init<MODE0><<<grid_for(L.ncp), kThreads, 0, s>>>(at_off<float4>(ws, L.cp), f, L.ncx, L.ncy, L.nz, P.r, P.w);
-  if (diff) k_diff_first<MODE0><<<grid_for(L.n), kThreads, 0, s>>>(st, f.cpv, f, L.nx, L.ny, L.nz);
+  if (diff) {
+    FieldSrc now = diff->field;
+    now.mode = FIELD_CP;
+    const size_t smem = diff_first_smem(P.w);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_diff_first<MODE0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_diff_first<MODE0><<<dim3(L.nz, L.ntx, L.nty), kAccThreads, smem, s>>>(st, *diff, now);
+  }
 }
 
 static void first_dispatch(int mode, const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f,
-                           bool cp_init, bool diff, cudaStream_t s) {
+                           bool cp_init, const IterArgs* diff, cudaStream_t s) {
   switch (mode) {
     case FIELD_UP: level_first<FIELD_UP>(P, L, ws, st, f, cp_init, diff, s); break;
     case FIELD_DENSE: level_first<FIELD_DENSE>(P, L, ws, st, f, cp_init, diff, s); break;
@@ -339,12 +353,14 @@ static void init_field(const Plan& P, void* ws, const float* init, cudaStream_t 
 
 // Number of kernels run_register launches for a plan (kept next to the launch
 // sequence it mirrors).
-static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_init) {
+static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_init, bool reuse_ref,
+                          bool same_mask) {
   int n = 0;
   for (int l = 0; l < P.levels; ++l) {
     n += 2 + (l + 1 < P.levels ? 2 : 0);                       // tables
-    if (l == 0) n += 2 + (has_mmov ? 1 : 0) + ((has_mmov || has_mref) ? 1 : 0);
-    else n += 5 + (has_mmov ? 3 : 0) + (has_mref ? 2 : 0) + ((has_mmov || has_mref) ? 1 : 0);
+    if (l == 0) n += (reuse_ref ? 1 : 2) + (has_mmov ? 1 : 0) + ((has_mmov || has_mref) ? 1 : 0);
+    else n += (reuse_ref ? 3 : 5) + (has_mmov ? 3 : 0) + ((has_mref && !reuse_ref && !same_mask) ? 2 : 0) +
+              ((has_mmov || has_mref) ? 1 : 0);
   }
   if (has_init) n += (P.levels == 1 ? 3 : 6) + 1;
   for (int l = P.levels - 1; l >= 0; --l) {
@@ -365,7 +381,8 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   int* err_flag = reinterpret_cast<int*>(reinterpret_cast<char*>(st) + sizeof(LKState));
   cudaMemsetAsync(err_flag, 0, sizeof(int), s);
   build_tables(P, ws, err_flag, s);
-  build_pyramid<T>(P, ws, mov, ref, mmov, mref, s);
+  const bool reuse_ref = (p->flags & WR_LK_REUSE_REFERENCE) != 0;
+  build_pyramid<T>(P, ws, mov, ref, mmov, mref, reuse_ref, s);
   if (init) init_field(P, ws, init, s);
   const bool mask = mmov || mref;
   const double sps = p->smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
@@ -386,7 +403,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       mode0 = FIELD_DENSE;
     }
     FieldSrc f0 = field_src(P, l, mode0, ws);
-    first_dispatch(mode0, P, L, ws, st, f0, true, false, s);
+    first_dispatch(mode0, P, L, ws, st, f0, true, nullptr, s);
     IterArgs a;
     memset(&a, 0, sizeof(a));
     a.st = st;
@@ -405,10 +422,8 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     a.w = P.w;
     a.ntx = L.ntx;
     a.nty = L.nty;
-    a.wins_per_strip = strip_windows(P.w);
-    a.nstrips = L.nstrips;
     a.zratio = L.zratio;
-    const dim3 grid(L.nz, L.nstrips, L.nty);
+    const dim3 grid(L.nz, L.ntx, L.nty);
     const size_t smem = iter_smem(P.w);
     const int forced = p->forced_updates[l];
     for (int it = 0; it < P.iter; ++it) {
@@ -421,7 +436,11 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
       k_update<<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
                                                      (double)p->movRange, L.zratio_d);
-      if (it == 0) first_dispatch(mode0, P, L, ws, st, f0, false, true, s);
+      if (it == 0) {
+        IterArgs d = a;
+        d.field = f0;
+        first_dispatch(mode0, P, L, ws, st, f0, false, &d, s);
+      }
       k_post<<<1, 1, 0, s>>>(st, l, forced);
     }
   }
@@ -436,7 +455,8 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
   if (prof) {
     prof->recorded = recorded;
-    prof->launches = count_launches(P, mmov != nullptr, mref != nullptr, init != nullptr);
+    prof->launches = count_launches(P, mmov != nullptr, mref != nullptr, init != nullptr, reuse_ref,
+                                    mmov != nullptr && mmov == mref && !reuse_ref);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "wr_lk_register launch");

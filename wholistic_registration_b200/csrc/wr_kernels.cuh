@@ -218,7 +218,7 @@ __global__ void k_pack_movg(const T* __restrict__ m, float4* __restrict__ movg, 
 // 0 = all 8 corners <= 0, 1 = all > 0, 2 = mixed (needs the exact sum).
 __global__ void k_mask_bits(const double* __restrict__ mref_d, const uint8_t* __restrict__ mref_u8,
                             const float* __restrict__ mmov, uint8_t* __restrict__ bits, int nz,
-                            int ny, int nx) {
+                            int ny, int nx, int keep_ref_bit) {
   long long n = (long long)nz * ny * nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -226,7 +226,7 @@ __global__ void k_mask_bits(const double* __restrict__ mref_d, const uint8_t* __
     long long rest = i / nx;
     int y = (int)(rest % ny);
     int z = (int)(rest / ny);
-    uint8_t b = 0;
+    uint8_t b = keep_ref_bit ? (bits[i] & 1) : 0;
     if (mref_d) b |= (mref_d[i] > 0.0) ? 1 : 0;
     else if (mref_u8) b |= mref_u8[i] ? 1 : 0;
     if (mmov) {
@@ -449,6 +449,14 @@ __device__ __forceinline__ float block_max(float v, float* red) {
 // (utils/calFlow3d_Wei_v1.py:442-588)
 // ---------------------------------------------------------------------------
 
+__device__ __forceinline__ float3 lerp3(const float3& a, const float3& b, float t) {
+  return make_float3(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z));
+}
+__device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float t) {
+  return make_float4(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z),
+                     fmaf(t, b.w - a.w, a.w));
+}
+
 struct IterArgs {
   LKState* st;
   const float* __restrict__ ref;
@@ -461,7 +469,6 @@ struct IterArgs {
   CPView cpv;                          // this level's CPs (motion_current at CPs)
   FieldSrc field;                      // motion used for this iteration
   int r, w, ntx, nty;
-  int wins_per_strip, nstrips;
   float zratio;
 };
 
@@ -486,256 +493,357 @@ __device__ __noinline__ bool warped_mask_exact(const float* mmov, int nx, int ny
   return sample_f64(mmov, nx, ny, nz, cx, cy, cz) > 0.f;
 }
 
-constexpr int kOutPerWarp = 30;   // lanes 1..30 of a warp own output columns; 0 and 31 are halo
-
-// Threads per CTA of the column walk and windows per strip for a patch width.
-__host__ __device__ inline int strip_windows(int w) { int m = 240 / w; return m < 1 ? 1 : m; }
-__host__ __device__ inline int strip_threads(int w) {
-  int cols = strip_windows(w) * w;
-  return 32 * ((cols + kOutPerWarp - 1) / kOutPerWarp);
+// CP-grid interpolation factors along one axis: the (g - r)/(2r+1) coordinate
+// clamped to [0, ncp] (utils/calFlow3d_Wei_v1.py:265-292), lower / upper CP
+// index (absolute, edge-clamped) and fraction.
+__device__ __forceinline__ int2 cp_factor(int g, int r, int w, int ncp, float& t) {
+  float c = __fdiv_rn((float)(g - r), (float)w);
+  c = fminf(fmaxf(c, 0.f), (float)ncp);
+  const float f = floorf(c);
+  t = c - f;
+  return make_int2(min((int)f, ncp - 1), min((int)f + 1, ncp - 1));
 }
 
-__device__ __forceinline__ float3 lerp3(const float3& a, const float3& b, float t) {
-  return make_float3(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z));
-}
-__device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float t) {
-  return make_float4(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y), fmaf(t, b.z - a.z, a.z),
-                     fmaf(t, b.w - a.w, a.w));
+constexpr int kAccThreads = 256;
+constexpr int kTileCP = 4;   // CP rows / columns held per tile
+
+// Motion of a (w+2) x (w+2) tile from shared memory: motion(hx, hy) =
+// sum_j wy[hy].j * ax[hx][j], where ax holds the CP field interpolated along x
+// for kTileCP CP rows and wy the y weights of those rows.  For the up-sampled
+// field of a level's first iteration (utils/calFlow3d_Wei_v1.py:381-410) the
+// same separable form holds over the coarser level's CPs: the bilinear
+// up-sampling table composed with that level's CP interpolation, x and y
+// components doubled.
+struct TileField {
+  float4* ax;   // [hw][kTileCP]
+  float4* wy;   // [hh]
+  float4* cpt;  // [kTileCP][kTileCP]
+  int generic;  // the tile's CP span exceeds kTileCP: evaluate per voxel
+};
+
+__host__ __device__ inline size_t tile_field_smem(int w) {
+  return 16 * ((size_t)(w + 2) * kTileCP + (w + 2) + kTileCP * kTileCP) + 16;
 }
 
-// Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588) as a column walk.
+// Fills the tile field for MODE (all threads of the CTA call it; ends with a barrier).
+template <int MODE>
+__device__ void build_tile_field(const TileField& tf, int* generic_flag, const FieldSrc& f, int r, int w, int x0,
+                                 int y0, int hw, int hh, int z, int nx, int ny) {
+  if (threadIdx.x == 0) *generic_flag = 0;
+  if (MODE == FIELD_CP) {
+    const CPView& g = f.cpv;
+    // CP tile origin: the lowest CP index used by the tile's first column / row
+    float t;
+    const int cx0 = cp_factor(clampi(x0 - 1, 0, nx - 1), r, w, g.ncx, t).x;
+    const int cy0 = cp_factor(clampi(y0 - 1, 0, ny - 1), r, w, g.ncy, t).x;
+    if (threadIdx.x == 0) { generic_flag[2] = cx0; generic_flag[3] = cy0; }
+    if (threadIdx.x < kTileCP * kTileCP) {
+      const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
+      tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+    }
+    __syncthreads();
+    if (threadIdx.x < hw) {
+      const int gx = clampi(x0 - 1 + (int)threadIdx.x, 0, nx - 1);
+      const int2 c = cp_factor(gx, r, w, g.ncx, t);
+      const int i0 = c.x - cx0, i1 = c.y - cx0;
+      for (int j = 0; j < kTileCP; ++j) {
+        const float4 p = tf.cpt[j * kTileCP + min(i0, kTileCP - 1)], q = tf.cpt[j * kTileCP + min(i1, kTileCP - 1)];
+        tf.ax[threadIdx.x * kTileCP + j] =
+            make_float4(fmaf(t, q.x - p.x, p.x), fmaf(t, q.y - p.y, p.y), fmaf(t, q.z - p.z, p.z), 0.f);
+      }
+      if (i1 >= kTileCP) atomicOr(generic_flag, 1);
+    }
+    if (threadIdx.x >= 128 && threadIdx.x < 128 + hh) {
+      const int hy = threadIdx.x - 128;
+      const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
+      const int2 c = cp_factor(gy, r, w, g.ncy, t);
+      float wv[kTileCP] = {0.f, 0.f, 0.f, 0.f};
+      const int j0 = c.x - cy0, j1 = c.y - cy0;
+      if (j1 >= kTileCP) atomicOr(generic_flag, 1);
+      wv[min(j0, kTileCP - 1)] += 1.f - t;
+      wv[min(j1, kTileCP - 1)] += t;
+      tf.wy[hy] = make_float4(wv[0], wv[1], wv[2], wv[3]);
+    }
+  } else if (MODE == FIELD_UP) {
+    const UpView& u = f.up;
+    const CPView& g = u.src;
+    float t;
+    // coarse CP origin: lowest CP index reached from the first column / row
+    const int gx0 = clampi(x0 - 1, 0, nx - 1), gy0 = clampi(y0 - 1, 0, ny - 1);
+    int cx0 = cp_factor(u.ix[2 * gx0], r, w, g.ncx, t).x, cy0 = cp_factor(u.iy[2 * gy0], r, w, g.ncy, t).x;
+    if (u.wx[2 * gx0 + 1] != 0.f) cx0 = min(cx0, cp_factor(u.ix[2 * gx0 + 1], r, w, g.ncx, t).x);
+    if (u.wy[2 * gy0 + 1] != 0.f) cy0 = min(cy0, cp_factor(u.iy[2 * gy0 + 1], r, w, g.ncy, t).x);
+    if (threadIdx.x < kTileCP * kTileCP) {
+      const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
+      tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+    }
+    __syncthreads();
+    if (threadIdx.x < hw) {
+      const int gx = clampi(x0 - 1 + (int)threadIdx.x, 0, nx - 1);
+      float wv[kTileCP] = {0.f, 0.f, 0.f, 0.f};
+      bool over = false;
+      for (int k = 0; k < 2; ++k) {
+        const float uw = u.wx[2 * gx + k];
+        if (uw == 0.f) continue;
+        const int2 c = cp_factor(u.ix[2 * gx + k], r, w, g.ncx, t);
+        const int i0 = c.x - cx0, i1 = c.y - cx0;
+        over |= i1 >= kTileCP || i0 < 0;
+        wv[clampi(i0, 0, kTileCP - 1)] += uw * (1.f - t);
+        wv[clampi(i1, 0, kTileCP - 1)] += uw * t;
+      }
+      if (over) atomicOr(generic_flag, 1);
+      for (int j = 0; j < kTileCP; ++j) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = 0; i < kTileCP; ++i) {
+          const float4 c = tf.cpt[j * kTileCP + i];
+          a.x = fmaf(wv[i], c.x, a.x);
+          a.y = fmaf(wv[i], c.y, a.y);
+          a.z = fmaf(wv[i], c.z, a.z);
+        }
+        a.x *= 2.f;
+        a.y *= 2.f;
+        tf.ax[threadIdx.x * kTileCP + j] = a;
+      }
+    }
+    if (threadIdx.x >= 128 && threadIdx.x < 128 + hh) {
+      const int hy = threadIdx.x - 128;
+      const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
+      float wv[kTileCP] = {0.f, 0.f, 0.f, 0.f};
+      bool over = false;
+      for (int k = 0; k < 2; ++k) {
+        const float uw = u.wy[2 * gy + k];
+        if (uw == 0.f) continue;
+        const int2 c = cp_factor(u.iy[2 * gy + k], r, w, g.ncy, t);
+        const int j0 = c.x - cy0, j1 = c.y - cy0;
+        over |= j1 >= kTileCP || j0 < 0;
+        wv[clampi(j0, 0, kTileCP - 1)] += uw * (1.f - t);
+        wv[clampi(j1, 0, kTileCP - 1)] += uw * t;
+      }
+      if (over) atomicOr(generic_flag, 1);
+      tf.wy[hy] = make_float4(wv[0], wv[1], wv[2], wv[3]);
+    }
+  }
+  __syncthreads();
+}
+
+template <int MODE>
+__device__ __forceinline__ float3 tile_motion(const TileField& tf, bool generic, const FieldSrc& f, int hx, int hy,
+                                              int gx, int gy, int z) {
+  if ((MODE == FIELD_CP || MODE == FIELD_UP) && !generic) {
+    const float4 wv = tf.wy[hy];
+    const float4* a = tf.ax + hx * kTileCP;
+    const float4 a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3];
+    return make_float3(wv.x * a0.x + wv.y * a1.x + wv.z * a2.x + wv.w * a3.x,
+                       wv.x * a0.y + wv.y * a1.y + wv.z * a2.y + wv.w * a3.y,
+                       wv.x * a0.z + wv.y * a1.z + wv.z * a2.z + wv.w * a3.z);
+  }
+  return eval_field<MODE>(f, gx, gy, z);
+}
+
+// Bytes of dynamic shared memory of k_lk_accumulate for patch width w.
+__host__ __device__ inline size_t accumulate_smem(int w) {
+  const size_t hw = (size_t)w + 2;
+  return 16 * (size_t)w * w                  // gradients + exclusion of the tile voxels
+         + 4 * ((hw * hw + 3) & ~size_t(3))  // It_raw of tile + halo
+         + tile_field_smem(w)                // motion factors
+         + 4 * 8 * 12 + 16;                  // reduction scratch, flags
+}
+
+// Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588).
 //
-// A CTA owns one z slice, one row of windows (2r+1 rows) and a strip of
-// whole windows along x.  Each lane owns one column and walks down the rows
-// (plus a halo row above and below): per voxel it evaluates the motion,
-// samples the warped moving level and its gradients with one set of 8 float4
-// corner loads (the previous row's corners are reused when the sample row
-// advances by one), and forms It_raw = ref - warped.  The 3x3 box smoothing
-// of It is a running 3-row sum per lane plus the two neighbouring lanes'
-// sums (warps overlap by two columns, so no CTA barrier is needed in the
-// walk).  Smoothed It, masked gradients and their nine products accumulate
-// per lane; a fixed-order reduction then gives each window's sums (a window
-// hanging over the volume edge counts the edge voxel once per replicated
-// position, mode="nearest" of utils/calculate.py:51) and the CTA's It^2 sum.
+// One CTA per (z slice, window or leftover tile).  Phase 1 takes every voxel
+// of the tile plus a one-voxel halo as independent work: the motion from the
+// tile's CP factors (shared memory), the warped moving level and its
+// gradients from one set of 8 float4 corners (m, Gx, Gy, Gz share the
+// trilinear weights; the upper-x corners come from the next lane when it
+// sampled the same rows), It_raw = ref - warped, and for tile voxels the
+// clipped gradients and the exclusion mask.  Phase 2 smooths It with the 3x3
+// box (edge-replicated), applies the mask and accumulates It^2 and the nine
+// gradient products; a window hanging over the volume edge counts the edge
+// voxel once per replicated position (mode="nearest" of
+// utils/calculate.py:51).  Sums are reduced with warp shuffles in a fixed
+// order, so results are deterministic.
 template <int MODE, bool MASK>
-__global__ void __launch_bounds__(256, 3) k_lk_accumulate(IterArgs a) {
-  if (!a.st->active) return;
-  extern __shared__ float smem[];
+__global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
+  const int active = *(volatile const int*)&a.st->active;   // checked after the tile loads are in flight
+  extern __shared__ float4 smem4[];
   const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
-  const int w = a.w, r = a.r;
+  const int w = a.w;
   const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
-  const int z = blockIdx.x, strip = blockIdx.y, ty = blockIdx.z;
-  const int wa = strip * a.wins_per_strip;
-  const int wb = min(wa + a.wins_per_strip, a.ntx);
-  const int x0 = wa * w, xe = min(wb * w, nx);
-  const int y0 = ty * w, ye = min(y0 + w, ny);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int col = x0 - 1 + warp * kOutPerWarp + lane;
-  const bool own = lane >= 1 && lane <= kOutPerWarp && col >= x0 && col < xe;
-  const bool warp_active = x0 + warp * kOutPerWarp < xe;
-  const int gx = clampi(col, 0, nx - 1);
+  const int z = blockIdx.x, tx = blockIdx.y, ty = blockIdx.z;
+  const bool window = tx < ncx && ty < ncy;
+  const int x0 = tx * w, y0 = ty * w;
+  const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
+  const int hw = wx + 2, hh = wy + 2;
+  float4* gsm = smem4;                                    // w*w
+  float* it_raw = reinterpret_cast<float*>(gsm + w * w);  // (w+2)^2, padded to 4
+  TileField tf;
+  tf.ax = reinterpret_cast<float4*>(it_raw + (((w + 2) * (w + 2) + 3) & ~3));
+  tf.wy = tf.ax + (w + 2) * kTileCP;
+  tf.cpt = tf.wy + (w + 2);
+  int* flags = reinterpret_cast<int*>(tf.cpt + kTileCP * kTileCP);
+  float* red = reinterpret_cast<float*>(flags + 4);       // 8 warps * 12
+  build_tile_field<MODE>(tf, flags, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
+  if (!active) return;
+  const bool generic = flags[0] != 0;
 
-  // CP tile: rows ty-1..ty+1, columns wa-1..wb (edge-clamped)
-  const int tile_w = wb - wa + 2;
-  float4* cpt = reinterpret_cast<float4*>(smem);
-  float* part = smem + 4 * 3 * tile_w;            // blockDim.x * 10 per-lane partials
-  float* wpen = part + blockDim.x * 10;           // per-window penalty
-  for (int i = threadIdx.x; i < 3 * tile_w; i += blockDim.x) {
-    const int jr = i / tile_w, jc = i - jr * tile_w;
-    const int cy = clampi(ty - 1 + jr, 0, ncy - 1), cx = clampi(wa - 1 + jc, 0, ncx - 1);
-    cpt[i] = a.cpv.cp[((size_t)z * ncy + cy) * ncx + cx];
+  const float4* __restrict__ G = a.mov.g;
+  const uint32_t plane = (uint32_t)nx * (uint32_t)ny;
+  const uint32_t zoff = (uint32_t)z * plane;
+  const int total = hh * hw;
+  const float fz_base = (float)z;
+  int hy = threadIdx.x / hw, hx = threadIdx.x - hy * hw;
+  const int step_y = kAccThreads / hw, step_x = kAccThreads - step_y * hw;
+  for (int h = threadIdx.x; h < total; h += kAccThreads) {
+    const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
+    const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
+    const float3 m = tile_motion<MODE>(tf, generic, a.field, hx, hy, gx, gy, z);
+    const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = fz_base + m.z;
+    int ix0, iy0, iz0;
+    float fx, fy, fz;
+    split_coord(cx, ix0, fx);
+    split_coord(cy, iy0, fy);
+    split_coord(cz, iz0, fz);
+    const int xa = clampi(ix0, 0, nx - 1), ya = clampi(iy0, 0, ny - 1), za = clampi(iz0, 0, nz - 1);
+    // taps one step up, or the same tap when clamped at the upper face
+    const bool sx = ix0 >= 0 && ix0 < nx - 1, sy = iy0 >= 0 && iy0 < ny - 1, sz = iz0 >= 0 && iz0 < nz - 1;
+    const uint32_t i000 = (uint32_t)za * plane + (uint32_t)ya * nx + (uint32_t)xa;
+    const float4* p00 = G + i000;
+    const float4* p01 = sy ? p00 + nx : p00;
+    const float4* p10 = sz ? p00 + plane : p00;
+    const float4* p11 = sy ? p10 + nx : p10;
+    float4 c000, c001, c010, c011, c100, c101, c110, c111;
+    c000 = __ldg(p00); c010 = __ldg(p01); c100 = __ldg(p10); c110 = __ldg(p11);
+    if (sx) {
+      c001 = __ldg(p00 + 1); c011 = __ldg(p01 + 1); c101 = __ldg(p10 + 1); c111 = __ldg(p11 + 1);
+    } else {
+      c001 = c000; c011 = c010; c101 = c100; c111 = c110;
+    }
+    // trilinear on (m, Gx) and (Gy, Gz) pairs with paired FP32 FMAs
+    const float2 tx2 = make_float2(fx, fx), ty2 = make_float2(fy, fy), tz2 = make_float2(fz, fz);
+    const float2 ntx2 = make_float2(-fx, -fx), nty2 = make_float2(-fy, -fy), ntz2 = make_float2(-fz, -fz);
+#define WR_LERP2(a, b, t, nt) __ffma2_rn(t, b, __ffma2_rn(nt, a, a))
+    const float2 lo00 = WR_LERP2(make_float2(c000.x, c000.y), make_float2(c001.x, c001.y), tx2, ntx2);
+    const float2 lo01 = WR_LERP2(make_float2(c010.x, c010.y), make_float2(c011.x, c011.y), tx2, ntx2);
+    const float2 lo10 = WR_LERP2(make_float2(c100.x, c100.y), make_float2(c101.x, c101.y), tx2, ntx2);
+    const float2 lo11 = WR_LERP2(make_float2(c110.x, c110.y), make_float2(c111.x, c111.y), tx2, ntx2);
+    const float2 lo = WR_LERP2(WR_LERP2(lo00, lo01, ty2, nty2), WR_LERP2(lo10, lo11, ty2, nty2), tz2, ntz2);
+    const uint32_t p = zoff + (uint32_t)gy * nx + gx;
+    it_raw[h] = __ldg(a.ref + p) - lo.x;
+    if (hx >= 1 && hx <= wx && hy >= 1 && hy <= wy) {
+      const float2 hi00 = WR_LERP2(make_float2(c000.z, c000.w), make_float2(c001.z, c001.w), tx2, ntx2);
+      const float2 hi01 = WR_LERP2(make_float2(c010.z, c010.w), make_float2(c011.z, c011.w), tx2, ntx2);
+      const float2 hi10 = WR_LERP2(make_float2(c100.z, c100.w), make_float2(c101.z, c101.w), tx2, ntx2);
+      const float2 hi11 = WR_LERP2(make_float2(c110.z, c110.w), make_float2(c111.z, c111.w), tx2, ntx2);
+      const float2 hi = WR_LERP2(WR_LERP2(hi00, hi01, ty2, nty2), WR_LERP2(hi10, hi11, ty2, nty2), tz2, ntz2);
+      float gxv = lo.y, gyv = hi.x, gzv = hi.y;
+      if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient(a.mov, cx, cy, cz, 0);
+      if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient(a.mov, cx, cy, cz, 1);
+      if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient(a.mov, cx, cy, cz, 2);
+      float excl = 0.f;
+      if (MASK) {
+        bool ex = (__ldg(a.mbits + p) & 1) != 0;
+        if (!ex && a.mmov) {
+          // the cell code covers exactly this sample's corners when the lower
+          // taps were not clamped
+          int code = 2;
+          if (xa == ix0 && ya == iy0 && za == iz0) code = (__ldg(a.mbits + i000) >> 1) & 3;
+          if (code == 1) ex = true;
+          else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
+        }
+        excl = ex ? 1.f : 0.f;
+      }
+      gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
+    }
+#undef WR_LERP2
+    hx += step_x;
+    hy += step_y;
+    if (hx >= hw) { hx -= hw; ++hy; }
   }
   __syncthreads();
 
   float acc[10];
 #pragma unroll
   for (int k = 0; k < 10; ++k) acc[k] = 0.f;
-
-  if (warp_active) {
-    // x part of the CP interpolation is fixed for the column
-    int cx0 = 0, cx1 = 0;
-    float txc = 0.f;
-    if (MODE == FIELD_CP) {
-      float gxc = __fdiv_rn((float)(gx - r), (float)w);
-      gxc = fminf(fmaxf(gxc, 0.f), (float)ncx);
-      const float fxc = floorf(gxc);
-      txc = gxc - fxc;
-      cx0 = min((int)fxc, ncx - 1) - (wa - 1);
-      cx1 = min((int)fxc + 1, ncx - 1) - (wa - 1);
-    }
-    const int wx_idx = gx / w;      // window column of an owned voxel
-    const bool win_col = own && (col / w) < ncx && ty < ncy;
-    const float mx = (gx == nx - 1) ? (float)(wx_idx * w + w - (nx - 1)) : 1.f;
-    const size_t zoff = (size_t)z * ny * nx;
-    // corners of the upper y tap row, kept for the next row: (za,xa) (za,xb) (zb,xa) (zb,xb)
-    float4 cb0 = make_float4(0.f, 0.f, 0.f, 0.f), cb1 = cb0, cb2 = cb0, cb3 = cb0;
-    int pxa = -1, pxb = -1, pyb = -1, pza = -1, pzb = -1;
-    float r0 = 0.f, r1 = 0.f;                        // It_raw of the two rows above
-    float4 gprev = make_float4(0.f, 0.f, 0.f, 0.f);  // gradients + exclusion of the previous row
-    const int R = (ye - y0) + 2;
-    for (int i = 0; i < R; ++i) {
-      const int gyu = y0 - 1 + i;
-      const int gy = clampi(gyu, 0, ny - 1);
-      float3 m;
-      if (MODE == FIELD_CP) {
-        float gyc = __fdiv_rn((float)(gy - r), (float)w);
-        gyc = fminf(fmaxf(gyc, 0.f), (float)ncy);
-        const float fyc = floorf(gyc), tyc = gyc - fyc;
-        const int j0 = (min((int)fyc, ncy - 1) - ty + 1) * tile_w;
-        const int j1 = (min((int)fyc + 1, ncy - 1) - ty + 1) * tile_w;
-        const float4 p0 = cpt[j0 + cx0], p1 = cpt[j0 + cx1], q0 = cpt[j1 + cx0], q1 = cpt[j1 + cx1];
-        const float3 B0 = make_float3(fmaf(txc, p1.x - p0.x, p0.x), fmaf(txc, p1.y - p0.y, p0.y),
-                                      fmaf(txc, p1.z - p0.z, p0.z));
-        const float3 B1 = make_float3(fmaf(txc, q1.x - q0.x, q0.x), fmaf(txc, q1.y - q0.y, q0.y),
-                                      fmaf(txc, q1.z - q0.z, q0.z));
-        m = lerp3(B0, B1, tyc);
-      } else {
-        m = eval_field<MODE>(a.field, gx, gy, z);
+  const float my_edge = (float)(y0 + w - (ny - 1));
+  const float mx_edge = (float)(x0 + w - (nx - 1));
+  const float inv_zr = (float)(1.0 / (double)a.zratio);
+  {
+    int ly = threadIdx.x / wx, lx = threadIdx.x - ly * wx;
+    const int sy = kAccThreads / wx, sx = kAccThreads - sy * wx;
+    for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
+      const float* rp = it_raw + ly * hw + lx;
+      float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
+                 (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
+      it *= (1.f / 9.f);
+      float4 g = gsm[i];
+      if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
+      acc[9] = fmaf(it, it, acc[9]);
+      if (window) {
+        const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
+        const float iz = g.z * inv_zr;
+        const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
+        acc[0] = fmaf(wgx, g.x, acc[0]);
+        acc[1] = fmaf(wgx, g.y, acc[1]);
+        acc[2] = fmaf(wgx, iz, acc[2]);
+        acc[3] = fmaf(wgy, g.y, acc[3]);
+        acc[4] = fmaf(wgy, iz, acc[4]);
+        acc[5] = fmaf(wgz, iz, acc[5]);
+        acc[6] = fmaf(wgx, it, acc[6]);
+        acc[7] = fmaf(wgy, it, acc[7]);
+        acc[8] = fmaf(wgz, it, acc[8]);
       }
-      const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = (float)z + m.z;
-      int ix0, iy0, iz0;
-      float fx, fy, fz;
-      split_coord(cx, ix0, fx);
-      split_coord(cy, iy0, fy);
-      split_coord(cz, iz0, fz);
-      const int xa = clampi(ix0, 0, nx - 1), xb = clampi(ix0 + 1, 0, nx - 1);
-      const int ya = clampi(iy0, 0, ny - 1), yb = clampi(iy0 + 1, 0, ny - 1);
-      const int za = clampi(iz0, 0, nz - 1), zb = clampi(iz0 + 1, 0, nz - 1);
-      const float4* G = a.mov.g;
-      const size_t oza = (size_t)za * ny * nx, ozb = (size_t)zb * ny * nx;
-      float4 ca0, ca1, ca2, ca3;
-      const bool same_xz = xa == pxa && xb == pxb && za == pza && zb == pzb;
-      if (same_xz && ya == pyb) {
-        // the sample row advanced by one: the old upper row is the new lower row
-        ca0 = cb0; ca1 = cb1; ca2 = cb2; ca3 = cb3;
-      } else {
-        const size_t ra = (size_t)ya * nx;
-        ca0 = __ldg(G + oza + ra + xa); ca1 = __ldg(G + oza + ra + xb);
-        ca2 = __ldg(G + ozb + ra + xa); ca3 = __ldg(G + ozb + ra + xb);
-      }
-      if (!(same_xz && yb == pyb)) {
-        const size_t rb = (size_t)yb * nx;
-        cb0 = __ldg(G + oza + rb + xa); cb1 = __ldg(G + oza + rb + xb);
-        cb2 = __ldg(G + ozb + rb + xa); cb3 = __ldg(G + ozb + rb + xb);
-      }
-      pxa = xa; pxb = xb; pyb = yb; pza = za; pzb = zb;
-      const float4 e0 = lerp4(ca0, ca1, fx), e1 = lerp4(cb0, cb1, fx);
-      const float4 e2 = lerp4(ca2, ca3, fx), e3 = lerp4(cb2, cb3, fx);
-      const float4 s = lerp4(lerp4(e0, e1, fy), lerp4(e2, e3, fy), fz);
-      const float r2 = __ldg(a.ref + zoff + (size_t)gy * nx + gx) - s.x;
-
-      // output row i-1 once its lower neighbour row is known
-      if (i >= 2) {
-        const float v = r0 + r1 + r2;
-        const float vl = __shfl_up_sync(0xffffffffu, v, 1);
-        const float vr = __shfl_down_sync(0xffffffffu, v, 1);
-        if (own) {
-          float it = (vl + v + vr) * (1.f / 9.f);
-          float4 g = gprev;
-          if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
-          acc[9] = fmaf(it, it, acc[9]);
-          if (win_col) {
-            const int gyo = gyu - 1;
-            const float my = (gyo == ny - 1) ? (float)(ty * w + w - (ny - 1)) : 1.f;
-            const float wt = mx * my;
-            const float iz = g.z / a.zratio;
-            const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
-            acc[0] = fmaf(wgx, g.x, acc[0]);
-            acc[1] = fmaf(wgx, g.y, acc[1]);
-            acc[2] = fmaf(wgx, iz, acc[2]);
-            acc[3] = fmaf(wgy, g.y, acc[3]);
-            acc[4] = fmaf(wgy, iz, acc[4]);
-            acc[5] = fmaf(wgz, iz, acc[5]);
-            acc[6] = fmaf(wgx, it, acc[6]);
-            acc[7] = fmaf(wgy, it, acc[7]);
-            acc[8] = fmaf(wgz, it, acc[8]);
-          }
-        }
-      }
-      // gradients and exclusion of this row (used when the next row arrives)
-      if (own && i >= 1 && i <= R - 2) {
-        float gxv = s.y, gyv = s.z, gzv = s.w;
-        if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient(a.mov, cx, cy, cz, 0);
-        if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient(a.mov, cx, cy, cz, 1);
-        if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient(a.mov, cx, cy, cz, 2);
-        float excl = 0.f;
-        if (MASK) {
-          bool ex = (__ldg(a.mbits + zoff + (size_t)gy * nx + gx) & 1) != 0;
-          if (!ex && a.mmov) {
-            const bool in_range = cx >= 0.f && cx <= (float)(nx - 1) && cy >= 0.f && cy <= (float)(ny - 1) &&
-                                  cz >= 0.f && cz <= (float)(nz - 1);
-            int code = 2;
-            if (in_range) code = (__ldg(a.mbits + ((size_t)iz0 * ny + iy0) * nx + ix0) >> 1) & 3;
-            if (code == 1) ex = true;
-            else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
-          }
-          excl = ex ? 1.f : 0.f;
-        }
-        gprev = make_float4(gxv, gyv, gzv, excl);
-      }
-      r0 = r1;
-      r1 = r2;
+      lx += sx;
+      ly += sy;
+      if (lx >= wx) { lx -= wx; ++ly; }
     }
   }
-
-  // fixed-order reduction: per-lane partials -> windows and CTA error
+  // warp reduction, then the 8 warps in order
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 10; ++k) part[threadIdx.x * 10 + k] = acc[k];
+  for (int k = 0; k < 10; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 10; ++k) red[warp * 12 + k] = acc[k];
   __syncthreads();
-  const long long blk = ((long long)ty * a.nstrips + strip) * nz + z;
-  const int nwin = wb - wa;
-  if (threadIdx.x < nwin) {
-    const int k = wa + threadIdx.x;
-    if (k < ncx && ty < ncy) {
-      float s[9];
-#pragma unroll
-      for (int q = 0; q < 9; ++q) s[q] = 0.f;
-      const int c0 = k * w, c1 = min(c0 + w, nx);
-      for (int c = c0; c < c1; ++c) {
-        const int rel = c - x0;
-        const int t = (rel / kOutPerWarp) * 32 + rel % kOutPerWarp + 1;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) s[q] += part[t * 10 + q];
-      }
-      const long long cpi = ((long long)z * ncy + ty) * ncx + k;
-      float* o = a.sums + cpi * 12;
-#pragma unroll
-      for (int q = 0; q < 9; ++q) o[q] = s[q];
+  const long long blk = ((long long)ty * a.ntx + tx) * nz + z;
+  const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
+  if (threadIdx.x < 10) {
+    float t = 0.f;
+    for (int q = 0; q < kAccThreads / 32; ++q) t += red[q * 12 + threadIdx.x];
+    if (threadIdx.x == 9) a.errpart[blk] = (double)t;
+    else if (window) a.sums[cpi * 12 + threadIdx.x] = t;
+  } else if (threadIdx.x == 32) {
+    double pen = 0.0;
+    if (window) {
       // neighbour difference on the CP grid (getNeiDiff with r = 1,
       // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
       // neighbours (edge-replicated) minus the centre, float64 then float32
+      const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
+      // in CP mode the shared-memory CP tile holds the 3x3 neighbourhood
+      const int ox = flags[2], oy = flags[3];
       double sx = 0.0, sy = 0.0, sz = 0.0;
       for (int dy = -1; dy <= 1; ++dy)
         for (int dx = -1; dx <= 1; ++dx) {
           if (dx == 0 && dy == 0) continue;
-          const int cy = clampi(ty + dy, 0, ncy - 1) - ty + 1;
-          const int cxi = clampi(k + dx, 0, ncx - 1) - (wa - 1);
-          const float4 v = cpt[cy * tile_w + cxi];
+          const int qy = clampi(ty + dy, 0, ncy - 1), qx = clampi(tx + dx, 0, ncx - 1);
+          const float4 v = (MODE == FIELD_CP) ? tf.cpt[(qy - oy) * kTileCP + (qx - ox)] : b[qy * ncx + qx];
           sx += 0.125 * (double)v.x;
           sy += 0.125 * (double)v.y;
           sz += 0.125 * (double)v.z;
         }
-      const float4 c = cpt[tile_w + (k - (wa - 1))];
+      const float4 c = (MODE == FIELD_CP) ? tf.cpt[(ty - oy) * kTileCP + (tx - ox)] : b[ty * ncx + tx];
       const float ndx = (float)(sx - (double)c.x);
       const float ndy = (float)(sy - (double)c.y);
       const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
+      float* o = a.sums + cpi * 12;
       o[9] = ndx;
       o[10] = ndy;
       o[11] = ndz;
-      wpen[threadIdx.x] = ndx * ndx + ndy * ndy + ndz * ndz;
+      pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
     }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double e = 0.0;
-    for (int c = x0; c < xe; ++c) {
-      const int rel = c - x0;
-      e += (double)part[((rel / kOutPerWarp) * 32 + rel % kOutPerWarp + 1) * 10 + 9];
-    }
-    a.errpart[blk] = e;
-    double pen = 0.0;
-    for (int t = 0; t < nwin; ++t)
-      if (wa + t < ncx && ty < ncy) pen += (double)wpen[t];
     a.penpart[blk] = pen;
   }
 }
@@ -850,26 +958,41 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
 }
 
 // max |new - old| over every voxel at a level's first iteration, where the
-// old field is not a function of this level's CPs.
+// old field is not a function of this level's CPs (utils/calFlow3d_Wei_v1.py:641-643).
+// One CTA per (z slice, tile); both fields come from shared-memory tile factors.
 template <int MODE0>
-__global__ void __launch_bounds__(kThreads) k_diff_first(LKState* st, CPView cpv, FieldSrc old, int nx, int ny, int nz) {
+__global__ void __launch_bounds__(kAccThreads) k_diff_first(LKState* st, IterArgs a, FieldSrc now) {
   if (!st->do_update) return;
-  __shared__ float red[64];
-  const long long n = (long long)nx * ny * nz;
+  extern __shared__ float4 smem4[];
+  const int nx = a.mov.nx, ny = a.mov.ny, w = a.w;
+  const int z = blockIdx.x, tx = blockIdx.y, ty = blockIdx.z;
+  const int x0 = tx * w, y0 = ty * w;
+  const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
+  const int hw = wx + 2, hh = wy + 2;
+  TileField tn, to;
+  tn.ax = smem4;
+  tn.wy = tn.ax + (w + 2) * kTileCP;
+  tn.cpt = tn.wy + (w + 2);
+  to.ax = tn.cpt + kTileCP * kTileCP;
+  to.wy = to.ax + (w + 2) * kTileCP;
+  to.cpt = to.wy + (w + 2);
+  int* flags = reinterpret_cast<int*>(to.cpt + kTileCP * kTileCP);   // two 4-int slots
+  float* red = reinterpret_cast<float*>(flags + 8);
+  build_tile_field<FIELD_CP>(tn, flags, now, a.r, w, x0, y0, hw, hh, z, nx, ny);
+  build_tile_field<MODE0>(to, flags + 4, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
+  const bool gn = flags[0] != 0, go = flags[4] != 0;
   float dmax = 0.f;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx);
-    const long long rest = i / nx;
-    const int y = (int)(rest % ny);
-    const int z = (int)(rest / ny);
-    const float3 a = cp_field(cpv, x, y, z);
-    const float3 b = eval_field<MODE0>(old, x, y, z);
-    dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(a.x - b.x), fabsf(a.y - b.y)), fabsf(a.z - b.z)));
+  for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
+    const int ly = i / wx, lx = i - ly * wx;
+    const float3 p = tile_motion<FIELD_CP>(tn, gn, now, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
+    const float3 q = tile_motion<MODE0>(to, go, a.field, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
+    dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(p.x - q.x), fabsf(p.y - q.y)), fabsf(p.z - q.z)));
   }
   const float m = block_max(dmax, red);
   if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
 }
+
+__host__ __device__ inline size_t diff_first_smem(int w) { return 2 * tile_field_smem(w) + 32 + 4 * 64; }
 
 // after an update: log max |delta motion| and apply the 1e-3 rule
 // (utils/calFlow3d_Wei_v1.py:641-654)

@@ -16,7 +16,6 @@ struct LevelPlan {
   int nx, ny, nz;     // level extent (x fastest)
   int ncx, ncy;       // control points per slice along x and y
   int ntx, nty;       // tiles: one per window plus a leftover tile if needed
-  int nstrips;        // CTAs along x of the fused iteration kernel
   long long n;        // voxels
   long long ncp;      // control points (ncx * ncy * nz)
   long long nblk;     // CTAs of the fused iteration kernel

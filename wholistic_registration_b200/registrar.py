@@ -119,11 +119,14 @@ class LKRegistrar:
         self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
 
     def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
-                 motion_init=None, out=None, stream=None, profile=None) -> torch.Tensor:
+                 motion_init=None, out=None, stream=None, profile=None, reuse_reference=False) -> torch.Tensor:
         """Motion (z, y, x, 3) float32 registering ``mov`` onto ``ref``.
 
         Masks are (z, y, x) uint8/bool exclusion masks (True = excluded) or
         None; ``motion_init`` is a (z, y, x, 3) float32 initial field or None.
+        ``reuse_reference`` keeps the reference pyramid and reference mask
+        built by the previous call on this registrar (same ``ref`` and
+        ``mask_ref``), as when registering a time series to one template.
         """
         if tuple(mov.shape) != self.shape or tuple(ref.shape) != self.shape:
             raise ValueError(f"volumes must have shape {self.shape}")
@@ -149,6 +152,7 @@ class LKRegistrar:
             init_ptr = motion_init.data_ptr()
         if out is None:
             out = torch.empty(self.shape + (3,), dtype=torch.float32, device=self.device)
+        self._cp.flags = _lib.WR_LK_REUSE_REFERENCE if reuse_reference else 0
         args = (ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
                 out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream))
         if profile is None:

@@ -43,6 +43,7 @@ class SeriesRegistrar:
         self.out_ready = [torch.cuda.Event() for _ in range(depth)]
         self.out_free = [torch.cuda.Event() for _ in range(depth)]
         self.started = [False] * depth
+        self.ref_ready = False   # the registrar's workspace holds the template pyramid
 
     def bytes_per_frame(self):
         n = 1
@@ -70,7 +71,8 @@ class SeriesRegistrar:
                 if self.started[k]:
                     self.s_run.wait_event(self.out_free[k])
                 self.reg.register(self.d_in[k], self.template, mask_mov, self.mask_ref, None,
-                                  out=self.d_motion[k], stream=self.s_run)
+                                  out=self.d_motion[k], stream=self.s_run, reuse_reference=self.ref_ready)
+                self.ref_ready = True
                 warp(self.d_in[k], self.d_motion[k], out=self.d_warp[k], stream=self.s_run)
                 self.in_free[k].record(self.s_run)
                 self.out_ready[k].record(self.s_run)
