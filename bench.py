@@ -202,8 +202,9 @@ def run_ours(args, wl, rank, world, local_rank):
     device = torch.device("cuda", local_rank)
     n_frames = min(wl["frames"], max(args.frames, 1))
     template, excl, frames, factor = make_workload(wl, device, n_frames, seed0=1000 + 97 * rank)
+    prec = {"f32": 0, "f16": 1, "bf16": 2}[args.precision]
     params = LKParams(layer=wl["layer"], iter=wl["iter"], r=wl["r"], zRatio=1.0, movRange=5.0,
-                      smoothPenalty=0.08 * factor, tol=1e-3)
+                      smoothPenalty=0.08 * factor, tol=1e-3, precision=prec)
     reg = LKRegistrar(wl["shape"], params, device)
     motion = torch.empty(wl["shape"] + (3,), dtype=torch.float32, device=device)
     warped = torch.empty(wl["shape"], dtype=torch.float32, device=device)
@@ -249,6 +250,7 @@ def run_ours(args, wl, rank, world, local_rank):
     from wholistic_registration_b200 import _lib
 
     durs = prof.durations_ms()
+    bpv = 10.0 if args.precision == "f32" else 6.0
     st_bytes = stats_hist.cpu().numpy()
     z, y, x = wl["shape"]
     levels = wl["layer"] + 1
@@ -269,7 +271,7 @@ def run_ours(args, wl, rank, world, local_rank):
                 d = durs[k][i]
                 i += 1
                 if it < st.evals[l]:
-                    alg_bytes += n_l * 10.0   # ref + moving level (float32) + two 1-byte masks
+                    alg_bytes += n_l * bpv   # ref + moving level (storage precision) + two 1-byte masks
                     act_ms += d
                     active_launches += 1
                 else:
@@ -285,10 +287,11 @@ def run_ours(args, wl, rank, world, local_rank):
     res = {
         "metric": METRIC, "value": round(vps, 3), "unit": "volumes/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
         "config": {
             "workload": args.workload, "shape_zyx": list(wl["shape"]), "frames_resident": n_frames,
-            "layer": wl["layer"], "r": wl["r"], "iter": wl["iter"], "path": "plain-fp32",
+            "layer": wl["layer"], "r": wl["r"], "iter": wl["iter"],
+            "path": {"f32": "plain-fp32", "f16": "plain, levels in float16", "bf16": "plain, levels in bfloat16"}[args.precision],
             "mask": f"ellipsoid inclusion {wl['coverage']}" if wl["coverage"] else "none",
             "l2": "inputs larger than L2 (each frame 268 MB > 126 MB)",
             "parallelism": f"frames sharded over {world} rank(s), no collective",
@@ -304,7 +307,7 @@ def run_ours(args, wl, rank, world, local_rank):
             "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
             "peak_kind": pk_kind, "traffic": None, "active_launches": active_launches,
             "active_ms_per_step": round(act_ms / args.steps, 4), "idle_launch_ms_per_step": round(idle_ms / args.steps, 4),
-            "bytes_per_voxel": 10,
+            "bytes_per_voxel": bpv,
         },
         "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
         "clocks": clocks.summary() if clocks else None,
@@ -400,6 +403,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="series-128x1024x1024")
     ap.add_argument("--frames", type=int, default=32)
+    ap.add_argument("--precision", choices=["f32", "f16", "bf16"], default="f32")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -111,8 +111,8 @@ typedef struct {
   int32_t levels;                         /* layer + 1 */
   int32_t evals[WR_MAX_LEVELS];           /* error evaluations per level, index = layer */
   int32_t updates[WR_MAX_LEVELS];         /* motion updates per level */
-  int32_t nan_solves;                     /* CP solves whose result was NaN (set to 0) */
-  int32_t pad;
+  int32_t nan_solves;                     /* CP solve components that were NaN (set to 0) */
+  int32_t fp64_solves;                    /* mixed precision: CP solves redone in float64 */
   double current_error;                   /* last evaluated error (returned by getMotion) */
   double diff_error[WR_MAX_LEVELS][WR_MAX_ITERS];
   double penalty_error[WR_MAX_LEVELS][WR_MAX_ITERS];

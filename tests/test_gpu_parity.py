@@ -186,3 +186,45 @@ def test_reuse_reference_matches_fresh_registration():
     b = LKRegistrar(shape, p)
     fresh = b.register(m2, t, e, e)
     torch.testing.assert_close(kept, fresh, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("precision,rms_tol", [(1, 0.02), (2, 0.1)])
+def test_mixed_precision_error_against_fp64_oracle(precision, rms_tol):
+    """Levels and gradients stored in float16 (1) or bfloat16 (2), sums and
+    solves in float32: flow error against the float64 oracle of the method."""
+    cf3 = _cf3()
+    from oracle import lk_oracle as O
+
+    t, m, option = _oracle_case((16, 128, 128), 11, 8, 2, 1.0, True)
+    om, _, _, olog = O.get_motion(m, t, dict(option))
+    opt = dict(option)
+    opt["precision"] = precision
+    opt["forced_updates"] = {l: len(olog[f"layer_{l}"]["max_diff_motion"]) for l in range(3)}
+    gm, _, _, _ = cf3.getMotion(m, t, opt)
+    err = gm - om
+    rms = float(np.sqrt(np.mean(err ** 2)))
+    print(f"precision {precision}: flow RMS {rms:.3e} vox, max {np.abs(err).max():.3e} vox")
+    assert rms <= rms_tol
+    w_o = O.correct_motion(m.astype(np.float32), om)
+    w_g = cf3.correctMotion(m.astype(np.float32), gm)
+    assert rel_l2(w_g, w_o) <= 10 * rms_tol
+
+
+def test_fp64_fallback_for_ill_conditioned_patches():
+    """Without smoothness penalty a near-uniform slab makes the structure
+    tensor singular: the mixed path re-solves those patches in float64."""
+    _cf3()
+    from wholistic_registration_b200 import LKParams, LKRegistrar, synthetic
+
+    shape = (8, 96, 96)
+    tmpl, mov, _ = synthetic.make_pair(shape, 31, n_blobs=200, max_disp=(2.0, 2.0, 0.5))
+    t, mv = tmpl.cuda().float(), mov.cuda().float()
+    t[:, 40:60, :] = 100.0
+    mv[:, 40:60, :] = 100.0
+    p = LKParams(layer=1, iter=6, r=4, zRatio=1.0, movRange=5.0, smoothPenalty=0.0, tol=1e-3,
+                 precision=1, forced_updates={0: 5, 1: 5})
+    reg = LKRegistrar(shape, p)
+    out = reg.register(mv.contiguous(), t.contiguous())
+    st = reg.stats()
+    assert st.fp64_solves > 0
+    assert bool(torch.isfinite(out).all())

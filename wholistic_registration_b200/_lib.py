@@ -75,7 +75,7 @@ class WrLKStats(ctypes.Structure):
         ("evals", ctypes.c_int32 * MAX_LEVELS),
         ("updates", ctypes.c_int32 * MAX_LEVELS),
         ("nan_solves", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("fp64_solves", ctypes.c_int32),
         ("current_error", ctypes.c_double),
         ("diff_error", (ctypes.c_double * MAX_ITERS) * MAX_LEVELS),
         ("penalty_error", (ctypes.c_double * MAX_ITERS) * MAX_LEVELS),

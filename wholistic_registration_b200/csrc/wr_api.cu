@@ -56,7 +56,10 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
   if (p->r < 1 || p->r > 48) { *why = "r out of range [1, 48]"; return WR_E_PARAM; }
   if (!(p->zRatio > 0.f) || !(p->movRange > 0.f)) { *why = "zRatio and movRange must be positive"; return WR_E_PARAM; }
   if (!(p->smoothPenalty >= 0.0) || !(p->tol >= 0.0)) { *why = "smoothPenalty and tol must be >= 0"; return WR_E_PARAM; }
-  if (p->precision != WR_PREC_F32) { *why = "only WR_PREC_F32 is available in this build"; return WR_E_PARAM; }
+  if (p->precision != WR_PREC_F32 && p->precision != WR_PREC_F16 && p->precision != WR_PREC_BF16) {
+    *why = "precision must be WR_PREC_F32, WR_PREC_F16 or WR_PREC_BF16";
+    return WR_E_PARAM;
+  }
   Plan& P = *plan;
   memset(&P, 0, sizeof(P));
   P.nz = nz; P.ny = ny; P.nx = nx;
@@ -88,8 +91,9 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.x_first = sx <= sy;
     L.tx_taps = resize_taps(nx, L.nx);
     L.ty_taps = resize_taps(ny, L.ny);
-    L.ref = A.take((size_t)L.n * 4);
-    L.movg = A.take((size_t)L.n * 16);
+    const size_t vbytes = p->precision == WR_PREC_F32 ? 4 : 2;   // per stored channel value
+    L.ref = A.take((size_t)L.n * vbytes);
+    L.movg = A.take((size_t)L.n * 4 * vbytes);
     L.mbits = A.take((size_t)L.n);
     L.mmov = A.take((size_t)L.n * 4);
     L.cp = A.take((size_t)L.ncp * 16);
@@ -193,21 +197,22 @@ static void resize_mask_to_level(const Plan& P, const LevelPlan& L, void* ws, co
   }
 }
 
-template <typename T>
+template <typename T, int PREC>
 static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, const uint8_t* mmov_u8,
                           const uint8_t* mref_u8, bool reuse_ref, cudaStream_t s) {
+  typedef Store<PREC> S;
   const bool same_mask = mmov_u8 != nullptr && mmov_u8 == mref_u8 && !reuse_ref;
   for (int l = 0; l < P.levels; ++l) {
     const LevelPlan& L = P.lv[l];
-    float* refl = at_off<float>(ws, L.ref);
-    float4* movg = at_off<float4>(ws, L.movg);
+    typename S::V1* refl = at_off<typename S::V1>(ws, L.ref);
+    typename S::V4* movg = at_off<typename S::V4>(ws, L.movg);
     float* mmov = at_off<float>(ws, L.mmov);
     uint8_t* bits = at_off<uint8_t>(ws, L.mbits);
     const bool any_mask = mmov_u8 || mref_u8;
     if (l == 0) {
       // scale 1 on every axis: the resize is an exact copy
-      if (!reuse_ref) k_to_float<T><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
-      k_pack_movg<T><<<grid_for(L.n), kThreads, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
+      if (!reuse_ref) k_to_level<T, PREC><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
+      k_pack_movg<T, PREC><<<grid_for(L.n), kThreads, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
       if (mmov_u8) k_u8_to_unit_f<<<grid_for(L.n), kThreads, 0, s>>>(mmov_u8, mmov, L.n);
       if (any_mask)
         k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8 ? mmov : nullptr,
@@ -216,9 +221,16 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
     }
     float* tmpf = at_off<float>(ws, P.tmp_a);
     float* levf = at_off<float>(ws, P.tmp_b);
-    if (!reuse_ref) resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, refl, s);
+    if (!reuse_ref) {
+      if (PREC == WR_PREC_F32) {
+        resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, reinterpret_cast<float*>(refl), s);
+      } else {
+        resize_to_level<T, float, float>(P, L, ws, ref, 1, 0, tmpf, levf, s);
+        k_store_level<PREC><<<grid_for(L.n), kThreads, 0, s>>>(levf, refl, L.n);
+      }
+    }
     resize_to_level<T, float, float>(P, L, ws, mov, 1, 0, tmpf, levf, s);
-    k_pack_movg<float><<<grid_for(L.n), kThreads, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
+    k_pack_movg<float, PREC><<<grid_for(L.n), kThreads, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
     double* tmpd = at_off<double>(ws, P.tmp_a);
     double* levd = at_off<double>(ws, P.tmp_b);
     if (mmov_u8) {
@@ -268,25 +280,27 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
   return f;
 }
 
-template <int MODE>
-static void launch_accumulate(const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
-  if (mask) {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_lk_accumulate<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lk_accumulate<MODE, true><<<grid, kAccThreads, smem, s>>>(a);
-  } else {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_lk_accumulate<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lk_accumulate<MODE, false><<<grid, kAccThreads, smem, s>>>(a);
-  }
+template <int MODE, bool MASK, int PREC>
+static void launch_accumulate1(const IterArgs& a, dim3 grid, size_t smem, cudaStream_t s) {
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_lk_accumulate<MODE, MASK, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_lk_accumulate<MODE, MASK, PREC><<<grid, kAccThreads, smem, s>>>(a);
 }
 
-static void accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
+template <int PREC>
+static void launch_accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
   switch (mode) {
-    case FIELD_CP: launch_accumulate<FIELD_CP>(a, grid, smem, mask, s); break;
-    case FIELD_UP: launch_accumulate<FIELD_UP>(a, grid, smem, mask, s); break;
-    case FIELD_DENSE: launch_accumulate<FIELD_DENSE>(a, grid, smem, mask, s); break;
-    default: launch_accumulate<FIELD_ZERO>(a, grid, smem, mask, s); break;
+    case FIELD_CP:
+      mask ? launch_accumulate1<FIELD_CP, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_CP, false, PREC>(a, grid, smem, s);
+      break;
+    case FIELD_UP:
+      mask ? launch_accumulate1<FIELD_UP, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_UP, false, PREC>(a, grid, smem, s);
+      break;
+    case FIELD_DENSE:
+      mask ? launch_accumulate1<FIELD_DENSE, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_DENSE, false, PREC>(a, grid, smem, s);
+      break;
+    default:
+      mask ? launch_accumulate1<FIELD_ZERO, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_ZERO, false, PREC>(a, grid, smem, s);
   }
 }
 
@@ -356,11 +370,12 @@ static void init_field(const Plan& P, void* ws, const float* init, cudaStream_t 
 static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_init, bool reuse_ref,
                           bool same_mask) {
   int n = 0;
+  const bool stored = P.precision != WR_PREC_F32;   // reduced-precision reference levels need a store pass
   for (int l = 0; l < P.levels; ++l) {
     n += 2 + (l + 1 < P.levels ? 2 : 0);                       // tables
     if (l == 0) n += (reuse_ref ? 1 : 2) + (has_mmov ? 1 : 0) + ((has_mmov || has_mref) ? 1 : 0);
-    else n += (reuse_ref ? 3 : 5) + (has_mmov ? 3 : 0) + ((has_mref && !reuse_ref && !same_mask) ? 2 : 0) +
-              ((has_mmov || has_mref) ? 1 : 0);
+    else n += (reuse_ref ? 3 : (stored ? 6 : 5)) + (has_mmov ? 3 : 0) +
+              ((has_mref && !reuse_ref && !same_mask) ? 2 : 0) + ((has_mmov || has_mref) ? 1 : 0);
   }
   if (has_init) n += (P.levels == 1 ? 3 : 6) + 1;
   for (int l = P.levels - 1; l >= 0; --l) {
@@ -372,7 +387,7 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
   return n + 1;                                                // final motion
 }
 
-template <typename T>
+template <typename T, int PREC>
 static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
                         const uint8_t* mref, const float* init, float* out, WrLKStats* stats, void* ws,
                         cudaStream_t s, WrProfile* prof) {
@@ -382,7 +397,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   cudaMemsetAsync(err_flag, 0, sizeof(int), s);
   build_tables(P, ws, err_flag, s);
   const bool reuse_ref = (p->flags & WR_LK_REUSE_REFERENCE) != 0;
-  build_pyramid<T>(P, ws, mov, ref, mmov, mref, reuse_ref, s);
+  build_pyramid<T, PREC>(P, ws, mov, ref, mmov, mref, reuse_ref, s);
   if (init) init_field(P, ws, init, s);
   const bool mask = mmov || mref;
   const double sps = p->smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
@@ -407,8 +422,8 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     IterArgs a;
     memset(&a, 0, sizeof(a));
     a.st = st;
-    a.ref = at_off<float>(ws, L.ref);
-    a.mov.g = at_off<float4>(ws, L.movg);
+    a.ref = at_off<void>(ws, L.ref);
+    a.mov.g = at_off<void>(ws, L.movg);
     a.mov.nx = L.nx;
     a.mov.ny = L.ny;
     a.mov.nz = L.nz;
@@ -431,11 +446,15 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
       const bool rec = prof && recorded < prof->capacity;
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
-      accumulate(mode, a, grid, smem, mask, s);
+      launch_accumulate<PREC>(mode, a, grid, smem, mask, s);
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
-      k_update<<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
-                                                     (double)p->movRange, L.zratio_d);
+      if (PREC == WR_PREC_F32)
+        k_update<false><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
+                                                              (double)p->movRange, L.zratio_d);
+      else
+        k_update<true><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
+                                                             (double)p->movRange, L.zratio_d);
       if (it == 0) {
         IterArgs d = a;
         d.field = f0;
@@ -497,6 +516,23 @@ static int noalloc_partials(double** out) {
   return WR_OK;
 }
 
+template <int PREC>
+static int dispatch_dtype(const Plan& P, const WrLKParams* p, const WrVolume* mov, const WrVolume* ref,
+                          const uint8_t* mmov, const uint8_t* mref, const float* init, float* out, WrLKStats* stats,
+                          void* ws, cudaStream_t s, WrProfile* prof) {
+  switch (mov->dtype) {
+    case WR_U16:
+      return run_register<uint16_t, PREC>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, mmov, mref,
+                                          init, out, stats, ws, s, prof);
+    case WR_U8:
+      return run_register<uint8_t, PREC>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, mmov, mref, init,
+                                         out, stats, ws, s, prof);
+    default:
+      return run_register<float, PREC>(P, p, (const float*)mov->data, (const float*)ref->data, mmov, mref, init, out,
+                                       stats, ws, s, prof);
+  }
+}
+
 static int check_volume(const WrVolume* v, const char* name) {
   if (!v || !v->data) return fail(WR_E_NULL, (std::string(name) + " is NULL").c_str());
   if (v->dtype != WR_U8 && v->dtype != WR_U16 && v->dtype != WR_F32)
@@ -552,16 +588,16 @@ int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint
   if (rc) return fail(rc, why);
   if (workspace_bytes < P.total) return fail(WR_E_WORKSPACE, "workspace smaller than wr_lk_workspace_size");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  switch (mov->dtype) {
-    case WR_U16:
-      return run_register<uint16_t>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, excl_mask_mov,
-                                    excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
-    case WR_U8:
-      return run_register<uint8_t>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, excl_mask_mov,
-                                   excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
+  switch (p->precision) {
+    case WR_PREC_F16:
+      return dispatch_dtype<WR_PREC_F16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
+                                         workspace, s, prof);
+    case WR_PREC_BF16:
+      return dispatch_dtype<WR_PREC_BF16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
+                                          workspace, s, prof);
     default:
-      return run_register<float>(P, p, (const float*)mov->data, (const float*)ref->data, excl_mask_mov,
-                                 excl_mask_ref, motion_init, motion_out, stats, workspace, s, prof);
+      return dispatch_dtype<WR_PREC_F32>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
+                                         workspace, s, prof);
   }
 }
 

@@ -7,6 +7,8 @@
 // (see lk_accumulate).  Control points (CP) are float4 (dx, dy, dz, 0).
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -43,6 +45,59 @@ __device__ __forceinline__ void split_coord(float c, int& i0, float& t) {
   t = c - f;
   i0 = (int)f;
 }
+
+// Storage of a level's (m, Gx, Gy, Gz) and of the reference level.
+// WR_PREC_F32: float4 / float.  WR_PREC_F16: 4 x half / half holding half
+// the value (so that uint16 data, up to 65535, stays inside the float16
+// range), scaled back by 2 on load.  WR_PREC_BF16: 4 x bfloat16 / bfloat16.
+template <int PREC> struct Store;
+template <> struct Store<WR_PREC_F32> {
+  typedef float4 V4;
+  typedef float V1;
+  static __device__ __forceinline__ float4 load4(const V4* p) { return __ldg(p); }
+  static __device__ __forceinline__ float load_m(const V4* p) { return __ldg(reinterpret_cast<const float*>(p)); }
+  static __device__ __forceinline__ float load1(const V1* p) { return __ldg(p); }
+  static __device__ __forceinline__ V4 pack4(float4 v) { return v; }
+  static __device__ __forceinline__ V1 pack1(float v) { return v; }
+};
+template <> struct Store<WR_PREC_F16> {
+  typedef uint2 V4;
+  typedef __half V1;
+  static __device__ __forceinline__ float4 load4(const V4* p) {
+    const uint2 u = __ldg(p);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    return make_float4(2.f * a.x, 2.f * a.y, 2.f * b.x, 2.f * b.y);
+  }
+  static __device__ __forceinline__ float load_m(const V4* p) {
+    return 2.f * __half2float(__ldg(reinterpret_cast<const __half*>(p)));
+  }
+  static __device__ __forceinline__ float load1(const V1* p) { return 2.f * __half2float(__ldg(p)); }
+  static __device__ __forceinline__ V4 pack4(float4 v) {
+    __half2 a = __floats2half2_rn(0.5f * v.x, 0.5f * v.y), b = __floats2half2_rn(0.5f * v.z, 0.5f * v.w);
+    return make_uint2(*reinterpret_cast<unsigned*>(&a), *reinterpret_cast<unsigned*>(&b));
+  }
+  static __device__ __forceinline__ V1 pack1(float v) { return __float2half_rn(0.5f * v); }
+};
+template <> struct Store<WR_PREC_BF16> {
+  typedef uint2 V4;
+  typedef __nv_bfloat16 V1;
+  static __device__ __forceinline__ float4 load4(const V4* p) {
+    const uint2 u = __ldg(p);
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+  }
+  static __device__ __forceinline__ float load_m(const V4* p) {
+    return __bfloat162float(__ldg(reinterpret_cast<const __nv_bfloat16*>(p)));
+  }
+  static __device__ __forceinline__ float load1(const V1* p) { return __bfloat162float(__ldg(p)); }
+  static __device__ __forceinline__ V4 pack4(float4 v) {
+    __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+    return make_uint2(*reinterpret_cast<unsigned*>(&a), *reinterpret_cast<unsigned*>(&b));
+  }
+  static __device__ __forceinline__ V1 pack1(float v) { return __float2bfloat16_rn(v); }
+};
 
 // ---------------------------------------------------------------------------
 // resize tables (utils/imresize.py:60-82)
@@ -184,16 +239,32 @@ __global__ void k_mask_to_d(const uint8_t* __restrict__ m, double* __restrict__ 
 // level packing
 // ---------------------------------------------------------------------------
 
-template <typename T>
-__global__ void k_to_float(const T* __restrict__ in, float* __restrict__ out, long long n) {
+template <typename T, typename O>
+__global__ void k_to_float(const T* __restrict__ in, O* __restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    out[i] = load_f<T>(in, i);
+    out[i] = (O)load_f<T>(in, i);
+}
+
+// input volume -> stored reference level (level 0: the resize is a copy)
+template <typename T, int PREC>
+__global__ void k_to_level(const T* __restrict__ in, typename Store<PREC>::V1* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = Store<PREC>::pack1(load_f<T>(in, i));
+}
+
+// float level -> stored reference level
+template <int PREC>
+__global__ void k_store_level(const float* __restrict__ in, typename Store<PREC>::V1* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = Store<PREC>::pack1(in[i]);
 }
 
 // movg[p] = (m, Gx, Gy, Gz) with G = half the clamped central difference.
-template <typename T>
-__global__ void k_pack_movg(const T* __restrict__ m, float4* __restrict__ movg, int nz, int ny, int nx) {
+template <typename T, int PREC>
+__global__ void k_pack_movg(const T* __restrict__ m, typename Store<PREC>::V4* __restrict__ movg, int nz, int ny, int nx) {
   long long n = (long long)nz * ny * nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -209,7 +280,7 @@ __global__ void k_pack_movg(const T* __restrict__ m, float4* __restrict__ movg, 
     float ym = load_f<T>(m, i - (size_t)(y - max(y - 1, 0)) * sy);
     float zp = load_f<T>(m, i + (size_t)(min(z + 1, nz - 1) - z) * sz);
     float zm = load_f<T>(m, i - (size_t)(z - max(z - 1, 0)) * sz);
-    movg[i] = make_float4(c, 0.5f * (xp - xm), 0.5f * (yp - ym), 0.5f * (zp - zm));
+    movg[i] = Store<PREC>::pack4(make_float4(c, 0.5f * (xp - xm), 0.5f * (yp - ym), 0.5f * (zp - zm)));
   }
 }
 
@@ -354,16 +425,18 @@ __device__ __forceinline__ float3 eval_field(const FieldSrc& f, int x, int y, in
 // ---------------------------------------------------------------------------
 
 struct VolView {
-  const float4* g;   // (m, Gx, Gy, Gz)
+  const void* g;     // (m, Gx, Gy, Gz) in the storage of the call's precision
   int nx, ny, nz;
 };
 
-__device__ __forceinline__ const float4& at(const VolView& v, int x, int y, int z) {
-  return v.g[((size_t)z * v.ny + y) * v.nx + x];
+template <int PREC>
+__device__ __forceinline__ float m_at(const VolView& v, int x, int y, int z) {
+  return Store<PREC>::load_m(static_cast<const typename Store<PREC>::V4*>(v.g) + ((size_t)z * v.ny + y) * v.nx + x);
 }
 
 // Trilinear sample of the m channel at an arbitrary coordinate (map_coordinates
 // order=1, mode="nearest").
+template <int PREC>
 __device__ __forceinline__ float sample_m(const VolView& v, float cx, float cy, float cz) {
   int x0, y0, z0;
   float tx, ty, tz;
@@ -373,10 +446,10 @@ __device__ __forceinline__ float sample_m(const VolView& v, float cx, float cy, 
   int xa = clampi(x0, 0, v.nx - 1), xb = clampi(x0 + 1, 0, v.nx - 1);
   int ya = clampi(y0, 0, v.ny - 1), yb = clampi(y0 + 1, 0, v.ny - 1);
   int za = clampi(z0, 0, v.nz - 1), zb = clampi(z0 + 1, 0, v.nz - 1);
-  float c000 = at(v, xa, ya, za).x, c001 = at(v, xb, ya, za).x;
-  float c010 = at(v, xa, yb, za).x, c011 = at(v, xb, yb, za).x;
-  float c100 = at(v, xa, ya, zb).x, c101 = at(v, xb, ya, zb).x;
-  float c110 = at(v, xa, yb, zb).x, c111 = at(v, xb, yb, zb).x;
+  float c000 = m_at<PREC>(v, xa, ya, za), c001 = m_at<PREC>(v, xb, ya, za);
+  float c010 = m_at<PREC>(v, xa, yb, za), c011 = m_at<PREC>(v, xb, yb, za);
+  float c100 = m_at<PREC>(v, xa, ya, zb), c101 = m_at<PREC>(v, xb, ya, zb);
+  float c110 = m_at<PREC>(v, xa, yb, zb), c111 = m_at<PREC>(v, xb, yb, zb);
   float e00 = fmaf(tx, c001 - c000, c000), e01 = fmaf(tx, c011 - c010, c010);
   float e10 = fmaf(tx, c101 - c100, c100), e11 = fmaf(tx, c111 - c110, c110);
   float f0 = fmaf(ty, e01 - e00, e00), f1 = fmaf(ty, e11 - e10, e10);
@@ -459,7 +532,7 @@ __device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float 
 
 struct IterArgs {
   LKState* st;
-  const float* __restrict__ ref;
+  const void* __restrict__ ref;        // reference level in the call's storage
   VolView mov;
   const uint8_t* __restrict__ mbits;   // null: no masks
   const float* __restrict__ mmov;      // null: no moving mask
@@ -475,17 +548,18 @@ struct IterArgs {
 // Central difference of two trilinear samples at c +- e_axis with the shifted
 // coordinate clipped to the volume (utils/calFlow3d_Wei_v1.py:134-206); the
 // general form, used within one voxel of the volume faces.
+template <int PREC>
 __device__ __noinline__ float clipped_gradient(VolView v, float cx, float cy, float cz, int axis) {
   if (axis == 0) {
     const float hi = fminf(fmaxf(cx + 1.f, 0.f), (float)(v.nx - 1)), lo = fminf(fmaxf(cx - 1.f, 0.f), (float)(v.nx - 1));
-    return 0.5f * (sample_m(v, hi, cy, cz) - sample_m(v, lo, cy, cz));
+    return 0.5f * (sample_m<PREC>(v, hi, cy, cz) - sample_m<PREC>(v, lo, cy, cz));
   }
   if (axis == 1) {
     const float hi = fminf(fmaxf(cy + 1.f, 0.f), (float)(v.ny - 1)), lo = fminf(fmaxf(cy - 1.f, 0.f), (float)(v.ny - 1));
-    return 0.5f * (sample_m(v, cx, hi, cz) - sample_m(v, cx, lo, cz));
+    return 0.5f * (sample_m<PREC>(v, cx, hi, cz) - sample_m<PREC>(v, cx, lo, cz));
   }
   const float hi = fminf(fmaxf(cz + 1.f, 0.f), (float)(v.nz - 1)), lo = fminf(fmaxf(cz - 1.f, 0.f), (float)(v.nz - 1));
-  return 0.5f * (sample_m(v, cx, cy, hi) - sample_m(v, cx, cy, lo));
+  return 0.5f * (sample_m<PREC>(v, cx, cy, hi) - sample_m<PREC>(v, cx, cy, lo));
 }
 
 // warped moving exclusion mask > 0, evaluated exactly (float64 sum, float32 result)
@@ -663,8 +737,9 @@ __host__ __device__ inline size_t accumulate_smem(int w) {
 // voxel once per replicated position (mode="nearest" of
 // utils/calculate.py:51).  Sums are reduced with warp shuffles in a fixed
 // order, so results are deterministic.
-template <int MODE, bool MASK>
+template <int MODE, bool MASK, int PREC>
 __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
+  typedef Store<PREC> S;
   const int active = *(volatile const int*)&a.st->active;   // checked after the tile loads are in flight
   extern __shared__ float4 smem4[];
   const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
@@ -687,7 +762,8 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
   if (!active) return;
   const bool generic = flags[0] != 0;
 
-  const float4* __restrict__ G = a.mov.g;
+  const typename S::V4* __restrict__ G = static_cast<const typename S::V4*>(a.mov.g);
+  const typename S::V1* __restrict__ R = static_cast<const typename S::V1*>(a.ref);
   const uint32_t plane = (uint32_t)nx * (uint32_t)ny;
   const uint32_t zoff = (uint32_t)z * plane;
   const int total = hh * hw;
@@ -708,14 +784,14 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
     // taps one step up, or the same tap when clamped at the upper face
     const bool sx = ix0 >= 0 && ix0 < nx - 1, sy = iy0 >= 0 && iy0 < ny - 1, sz = iz0 >= 0 && iz0 < nz - 1;
     const uint32_t i000 = (uint32_t)za * plane + (uint32_t)ya * nx + (uint32_t)xa;
-    const float4* p00 = G + i000;
-    const float4* p01 = sy ? p00 + nx : p00;
-    const float4* p10 = sz ? p00 + plane : p00;
-    const float4* p11 = sy ? p10 + nx : p10;
+    const typename S::V4* p00 = G + i000;
+    const typename S::V4* p01 = sy ? p00 + nx : p00;
+    const typename S::V4* p10 = sz ? p00 + plane : p00;
+    const typename S::V4* p11 = sy ? p10 + nx : p10;
     float4 c000, c001, c010, c011, c100, c101, c110, c111;
-    c000 = __ldg(p00); c010 = __ldg(p01); c100 = __ldg(p10); c110 = __ldg(p11);
+    c000 = S::load4(p00); c010 = S::load4(p01); c100 = S::load4(p10); c110 = S::load4(p11);
     if (sx) {
-      c001 = __ldg(p00 + 1); c011 = __ldg(p01 + 1); c101 = __ldg(p10 + 1); c111 = __ldg(p11 + 1);
+      c001 = S::load4(p00 + 1); c011 = S::load4(p01 + 1); c101 = S::load4(p10 + 1); c111 = S::load4(p11 + 1);
     } else {
       c001 = c000; c011 = c010; c101 = c100; c111 = c110;
     }
@@ -729,7 +805,7 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
     const float2 lo11 = WR_LERP2(make_float2(c110.x, c110.y), make_float2(c111.x, c111.y), tx2, ntx2);
     const float2 lo = WR_LERP2(WR_LERP2(lo00, lo01, ty2, nty2), WR_LERP2(lo10, lo11, ty2, nty2), tz2, ntz2);
     const uint32_t p = zoff + (uint32_t)gy * nx + gx;
-    it_raw[h] = __ldg(a.ref + p) - lo.x;
+    it_raw[h] = S::load1(R + p) - lo.x;
     if (hx >= 1 && hx <= wx && hy >= 1 && hy <= wy) {
       const float2 hi00 = WR_LERP2(make_float2(c000.z, c000.w), make_float2(c001.z, c001.w), tx2, ntx2);
       const float2 hi01 = WR_LERP2(make_float2(c010.z, c010.w), make_float2(c011.z, c011.w), tx2, ntx2);
@@ -737,9 +813,9 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
       const float2 hi11 = WR_LERP2(make_float2(c110.z, c110.w), make_float2(c111.z, c111.w), tx2, ntx2);
       const float2 hi = WR_LERP2(WR_LERP2(hi00, hi01, ty2, nty2), WR_LERP2(hi10, hi11, ty2, nty2), tz2, ntz2);
       float gxv = lo.y, gyv = hi.x, gzv = hi.y;
-      if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient(a.mov, cx, cy, cz, 0);
-      if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient(a.mov, cx, cy, cz, 1);
-      if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient(a.mov, cx, cy, cz, 2);
+      if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 0);
+      if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 1);
+      if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 2);
       float excl = 0.f;
       if (MASK) {
         bool ex = (__ldg(a.mbits + p) & 1) != 0;
@@ -912,6 +988,28 @@ __global__ void k_decide(LKState* st, const double* __restrict__ errpart, const 
 // CP solve and update (utils/calFlow3d_Wei_v1.py:209-262,591-624)
 // ---------------------------------------------------------------------------
 
+// Regularised 3x3 solve by adjugate / determinant: float64 (the reference's
+// arithmetic) or float32 re-solved in float64 when the Frobenius condition
+// estimate |A| |adj A| / |det A| exceeds 1e6 or the float32 result is not finite.
+template <typename R>
+__device__ __forceinline__ void solve3(R ixx, R ixy, R ixz, R iyy, R iyz, R izz, R ixt, R iyt, R izt, R& vx, R& vy,
+                                       R& vz, R& cond) {
+  const R det = ixx * (iyy * izz - iyz * iyz) - ixy * (ixy * izz - iyz * ixz) + ixz * (ixy * iyz - iyy * ixz);
+  const R m11 = iyy * izz - iyz * iyz;
+  const R m12 = -(ixy * izz - iyz * ixz);
+  const R m13 = ixy * iyz - iyy * ixz;
+  const R m22 = ixx * izz - ixz * ixz;
+  const R m23 = -(ixx * iyz - ixy * ixz);
+  const R m33 = ixx * iyy - ixy * ixy;
+  vx = (m11 * ixt + m12 * iyt + m13 * izt) / det;
+  vy = (m12 * ixt + m22 * iyt + m23 * izt) / det;
+  vz = (m13 * ixt + m23 * iyt + m33 * izt) / det;
+  const R na = ixx * ixx + iyy * iyy + izz * izz + R(2) * (ixy * ixy + ixz * ixz + iyz * iyz);
+  const R nb = m11 * m11 + m22 * m22 + m33 * m33 + R(2) * (m12 * m12 + m13 * m13 + m23 * m23);
+  cond = sqrt(na * nb) / fabs(det);
+}
+
+template <bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, const float* __restrict__ sums,
                                                     long long ncp, double sps, float sps_f, double mov_range,
                                                     double zratio_d) {
@@ -919,24 +1017,28 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
   __shared__ float red[64];
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   float dmax = 0.f;
-  int nan_count = 0;
+  int nan_count = 0, fp64_count = 0;
   if (i < ncp) {
     const float* s = sums + i * 12;
-    const double ixx = (double)s[0] + sps, ixy = s[1], ixz = s[2];
-    const double iyy = (double)s[3] + sps, iyz = s[4], izz = (double)s[5] + sps;
-    const double ixt = (double)s[6] + (double)__fmul_rn(sps_f, s[9]);
-    const double iyt = (double)s[7] + (double)__fmul_rn(sps_f, s[10]);
-    const double izt = (double)s[8] + (double)__fmul_rn(sps_f, s[11]);
-    const double det = ixx * (iyy * izz - iyz * iyz) - ixy * (ixy * izz - iyz * ixz) + ixz * (ixy * iyz - iyy * ixz);
-    const double m11 = iyy * izz - iyz * iyz;
-    const double m12 = -(ixy * izz - iyz * ixz);
-    const double m13 = ixy * iyz - iyy * ixz;
-    const double m22 = ixx * izz - ixz * ixz;
-    const double m23 = -(ixx * iyz - ixy * ixz);
-    const double m33 = ixx * iyy - ixy * ixy;
-    double vx = (m11 * ixt + m12 * iyt + m13 * izt) / det;
-    double vy = (m12 * ixt + m22 * iyt + m23 * izt) / det;
-    double vz = (m13 * ixt + m23 * iyt + m33 * izt) / det;
+    const float ntx = __fmul_rn(sps_f, s[9]), nty = __fmul_rn(sps_f, s[10]), ntz = __fmul_rn(sps_f, s[11]);
+    double vx, vy, vz;
+    bool done = false;
+    if (MIXED) {
+      const float fs = (float)sps;
+      float fx, fy, fz, fc;
+      solve3<float>(s[0] + fs, s[1], s[2], s[3] + fs, s[4], s[5] + fs, s[6] + ntx, s[7] + nty, s[8] + ntz, fx, fy, fz, fc);
+      if (isfinite(fx) && isfinite(fy) && isfinite(fz) && fc <= 1e6f) {
+        vx = fx; vy = fy; vz = fz;
+        done = true;
+      } else {
+        ++fp64_count;
+      }
+    }
+    if (!done) {
+      double dc;
+      solve3<double>((double)s[0] + sps, s[1], s[2], (double)s[3] + sps, s[4], (double)s[5] + sps,
+                     (double)s[6] + (double)ntx, (double)s[7] + (double)nty, (double)s[8] + (double)ntz, vx, vy, vz, dc);
+    }
     if (isnan(vx)) { vx = 0.0; ++nan_count; }
     if (isnan(vy)) { vy = 0.0; ++nan_count; }
     if (isnan(vz)) { vz = 0.0; ++nan_count; }
@@ -953,6 +1055,7 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
     dmax = fmaxf(fmaxf(fabsf(nx - old.x), fabsf(ny - old.y)), fabsf(nz - old.z));
   }
   if (nan_count) atomicAdd(&st->stats.nan_solves, nan_count);
+  if (fp64_count) atomicAdd(&st->stats.fp64_solves, fp64_count);
   const float m = block_max(dmax, red);
   if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
 }
