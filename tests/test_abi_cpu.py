@@ -22,8 +22,12 @@ def lib():
 
 
 def test_exports_match_header(lib):
-    with open(os.path.join(ROOT, "include", "wr_b200.h")) as fh:
-        header = fh.read()
+    import glob
+
+    header = ""
+    for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))):
+        with open(h) as fh:
+            header += fh.read()
     declared = set(re.findall(r"WR_API\s+[\w\s\*]*?\b(wr_\w+)\s*\(", header))
     assert declared == set(_lib.EXPORTS)
     for name in declared:

@@ -41,6 +41,15 @@ EXPORTS = (
     "wr_penalty_factor_noalloc",
     "wr_penalty_factor_scratch",
     "wr_resize_table",
+    "wr_net_last_error",
+    "wr_net_conv3d_fwd",
+    "wr_net_conv3d_dgrad",
+    "wr_net_conv3d_wgrad",
+    "wr_net_act_backward",
+    "wr_net_split_grad",
+    "wr_net_adam",
+    "wr_net_weights_to_bf16",
+    "wr_net_flow_loss",
 )
 
 
@@ -94,6 +103,11 @@ class WrProfile(ctypes.Structure):
     ]
 
 
+class WrConvGeom(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in
+                ("n", "oz", "oy", "ox", "iz", "iy", "ix", "stride", "c1", "c2", "up1", "cout", "act")]
+
+
 class WrError(RuntimeError):
     """A C-ABI call returned a nonzero status."""
 
@@ -134,8 +148,20 @@ def load():
         lib.wr_penalty_factor_noalloc.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_penalty_factor_scratch.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
         lib.wr_resize_table.argtypes = [i32, i32, i32, vp, vp, ctypes.POINTER(i32)]
+        G = ctypes.POINTER(WrConvGeom)
+        f32, i64, fl = ctypes.c_float, ctypes.c_longlong, ctypes.c_float
+        lib.wr_net_conv3d_fwd.argtypes = [G, vp, vp, vp, vp, vp, vp, vp]
+        lib.wr_net_conv3d_dgrad.argtypes = [G, vp, vp, vp, vp]
+        lib.wr_net_conv3d_wgrad.argtypes = [G, vp, vp, vp, vp, vp, vp]
+        lib.wr_net_act_backward.argtypes = [vp, vp, ctypes.c_int, vp, i64, ctypes.c_int, vp]
+        lib.wr_net_split_grad.argtypes = [G, vp, vp, vp, vp]
+        lib.wr_net_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, ctypes.c_int, f32, vp]
+        lib.wr_net_weights_to_bf16.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
+        lib.wr_net_flow_loss.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, fl, fl, fl, vp]
         for name in EXPORTS:
-            getattr(lib, name).restype = ctypes.c_int if name != "wr_last_error" else ctypes.c_char_p
+            getattr(lib, name).restype = (ctypes.c_char_p if name in ("wr_last_error", "wr_net_last_error")
+                                          else ctypes.c_int)
         if lib.wr_abi_version() != 1:
             raise ImportError("wr_b200 ABI version mismatch")
         _lib = lib
@@ -144,7 +170,8 @@ def load():
 
 def check(fn, code):
     if code != 0:
-        msg = load().wr_last_error().decode(errors="replace")
+        lib = load()
+        msg = (lib.wr_net_last_error() if fn.startswith("wr_net") else lib.wr_last_error()).decode(errors="replace")
         if code > 0:
             raise ArgumentError(fn, code, msg)
         raise WrError(fn, code, msg)

@@ -20,8 +20,8 @@ ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "_wr_b200.so")
-SOURCES = ["wr_api.cu"]
-DEPS = ["wr_api.cu", "wr_kernels.cuh", "wr_plan.h", "wr_resize_table.cuh"]
+SOURCES = ["wr_api.cu", "wr_net.cu"]
+DEPS = ["wr_api.cu", "wr_net.cu", "wr_kernels.cuh", "wr_plan.h", "wr_resize_table.cuh"]
 
 
 def nvcc_path() -> str:
@@ -46,7 +46,7 @@ def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, d) for d in DEPS] + [os.path.join(INCLUDE, "wr_b200.h")]
+    deps = [os.path.join(SRC, d) for d in DEPS] + [os.path.join(INCLUDE, h) for h in ("wr_b200.h", "wr_net.h")]
     return all(os.path.getmtime(d) <= t for d in deps)
 
 

@@ -1,0 +1,626 @@
+// Kernels of the learned warm-start network: a small 3-D convolutional
+// encoder-decoder that predicts a coarse displacement field (1/4 resolution in
+// x and y) from a template / moving pair.  No counterpart exists in the
+// reference; its output enters the registration through the reference's own
+// warm-start channel, option["motion"] (utils/calFlow3d_Wei_v1.py:362-377).
+//
+// Tensors are channels-last bfloat16: [n][z][y][x][c], channel counts padded
+// to multiples of 16.  A convolution is an implicit GEMM on BF16 tensor cores
+// (mma.sync m16n8k16, float32 accumulate):
+//   forward  y[q][co] = act(b[co] + sum_{tap,ci} x[p(q,tap)][ci] w[tap][co][ci])
+//   data     dx[p][ci] = sum_{tap,co} dy[q(p,tap)][co] w[tap][co][ci]
+//   weights  dw[tap][co][ci] = sum_q dy[q][co] x[p(q,tap)][ci]
+// with p = stride*q + tap - 1 per axis (3x3x3 kernel, padding 1).  The input
+// of a decoder convolution is the virtual concatenation of a coarser tensor
+// (nearest-upsampled by 2: its voxel is p/2) and a skip tensor; the gather
+// reads either directly, so no upsampled or concatenated copy is formed.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "wr_b200.h"
+#include "wr_net.h"
+
+namespace wrnet {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* m) {
+  g_err = m;
+  return code;
+}
+
+static int cuda_status(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return WR_OK;
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return -(int)e;
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Geometry of one convolution (all extents of the output / input grids).
+struct Conv {
+  int n;                // batch
+  int oz, oy, ox;       // output grid
+  int iz, iy, ix;       // input grid (of the skip / direct source)
+  int stride;           // 1 or 2
+  int c1, c2;           // channels from source 1 and source 2 (c2 = 0: single source)
+  int up1;              // source 1 is half resolution, read at p / 2
+  int cin;              // c1 + c2 (multiple of 16)
+  int cout;             // real output channels
+  int cout_p;           // padded to a multiple of 16 (weight rows)
+  int act;              // 1: LeakyReLU(0.1)
+};
+
+__device__ __forceinline__ long long vox(int n, int z, int y, int x, int Z, int Y, int X) {
+  return (((long long)n * Z + z) * Y + y) * X + x;
+}
+
+// ---------------------------------------------------------------------------
+// forward: CTA = 4 warps x 32 output voxels, all output channels (<= 64)
+// ---------------------------------------------------------------------------
+
+constexpr int kWarps = 4;
+constexpr int kMT = 2;     // m16 tiles per warp
+constexpr int kMaxNT = 8;  // n8 tiles (64 output channels)
+
+template <int NT>
+__global__ void __launch_bounds__(kWarps * 32) k_conv_fwd(Conv c, const __nv_bfloat16* __restrict__ x1,
+                                                          const __nv_bfloat16* __restrict__ x2,
+                                                          const __nv_bfloat16* __restrict__ w,
+                                                          const float* __restrict__ bias,
+                                                          __nv_bfloat16* __restrict__ y, float* __restrict__ y32) {
+  extern __shared__ __nv_bfloat16 wsm[];   // [cout_p][cin] of the current tap
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
+  const long long base = ((long long)blockIdx.x * kWarps + warp) * (16 * kMT);
+  // the four output rows this thread feeds into A fragments
+  long long row[kMT][2];
+  int rz[kMT][2], ry[kMT][2], rx[kMT][2], rn[kMT][2];
+  bool rv[kMT][2];
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int h = 0; h < 2; ++h) {
+      long long q = base + mt * 16 + g + 8 * h;
+      rv[mt][h] = q < nvox;
+      row[mt][h] = q;
+      long long qq = rv[mt][h] ? q : 0;
+      rx[mt][h] = (int)(qq % c.ox); qq /= c.ox;
+      ry[mt][h] = (int)(qq % c.oy); qq /= c.oy;
+      rz[mt][h] = (int)(qq % c.oz); rn[mt][h] = (int)(qq / c.oz);
+    }
+  float acc[kMT][NT][4];
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int nt = 0; nt < NT; ++nt)
+      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
+  const int chunks = c.cin / 16;
+  for (int tap = 0; tap < 27; ++tap) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < c.cout_p * c.cin / 2; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(wsm)[i] = reinterpret_cast<const uint32_t*>(w + (size_t)tap * c.cout_p * c.cin)[i];
+    __syncthreads();
+    const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
+    // source voxel of each row for this tap (fine grid) and validity
+    long long p2[kMT][2], p1[kMT][2];
+    bool pv[kMT][2];
+    for (int mt = 0; mt < kMT; ++mt)
+      for (int h = 0; h < 2; ++h) {
+        const int z = c.stride * rz[mt][h] + kz, yy = c.stride * ry[mt][h] + ky, xx = c.stride * rx[mt][h] + kx;
+        pv[mt][h] = rv[mt][h] && z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix;
+        p2[mt][h] = pv[mt][h] ? vox(rn[mt][h], z, yy, xx, c.iz, c.iy, c.ix) : 0;
+        const int hz = (c.iz + 1) / 2, hy = (c.iy + 1) / 2, hx = (c.ix + 1) / 2;
+        p1[mt][h] = pv[mt][h] ? (c.up1 ? vox(rn[mt][h], z >> 1, yy >> 1, xx >> 1, hz, hy, hx) : p2[mt][h]) : 0;
+      }
+    for (int ch = 0; ch < chunks; ++ch) {
+      const int c0 = ch * 16;
+      const bool from1 = c0 < c.c1;
+      const __nv_bfloat16* src = from1 ? x1 : x2;
+      const int cs = from1 ? c.c1 : c.c2;
+      const int cc = from1 ? c0 : c0 - c.c1;
+      uint32_t a[kMT][4];
+      for (int mt = 0; mt < kMT; ++mt)
+        for (int h = 0; h < 2; ++h) {
+          uint32_t lo = 0u, hi = 0u;
+          if (pv[mt][h]) {
+            const long long pix = from1 ? p1[mt][h] : p2[mt][h];
+            const uint32_t* sp = reinterpret_cast<const uint32_t*>(src + pix * cs + cc);
+            lo = __ldg(sp + t);
+            hi = __ldg(sp + 4 + t);
+          }
+          a[mt][h] = lo;       // a0 (row g) / a1 (row g+8)
+          a[mt][2 + h] = hi;   // a2 / a3 (channels +8)
+        }
+      for (int nt = 0; nt < NT; ++nt) {
+        const uint32_t* wp = reinterpret_cast<const uint32_t*>(wsm + (size_t)(nt * 8 + g) * c.cin + c0);
+        const uint32_t b0 = wp[t], b1 = wp[4 + t];
+        for (int mt = 0; mt < kMT; ++mt) mma_bf16(acc[mt][nt], a[mt], b0, b1);
+      }
+    }
+  }
+  // epilogue: bias, activation, store
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int h = 0; h < 2; ++h) {
+      if (!rv[mt][h]) continue;
+      const long long q = row[mt][h];
+      for (int nt = 0; nt < NT; ++nt) {
+        const int co = nt * 8 + 2 * t;
+        float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
+        if (co < c.cout) v0 += bias[co];
+        if (co + 1 < c.cout) v1 += bias[co + 1];
+        if (c.act) {
+          v0 = v0 > 0.f ? v0 : 0.1f * v0;
+          v1 = v1 > 0.f ? v1 : 0.1f * v1;
+        }
+        if (y32) {
+          if (co < c.cout) y32[q * c.cout + co] = v0;
+          if (co + 1 < c.cout) y32[q * c.cout + co + 1] = v1;
+        } else if (co < c.cout) {
+          *reinterpret_cast<__nv_bfloat162*>(y + q * c.cout + co) = __floats2bfloat162_rn(v0, v1);
+        }
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// data gradient: GEMM over input voxels p (fine grid of the virtual input),
+// k = (tap, co); weights transposed to wt[tap][ci][co_p]
+// ---------------------------------------------------------------------------
+
+template <int NT>
+__global__ void __launch_bounds__(kWarps * 32) k_conv_dgrad(Conv c, const __nv_bfloat16* __restrict__ dy,
+                                                            const __nv_bfloat16* __restrict__ wt,
+                                                            float* __restrict__ dx) {
+  extern __shared__ __nv_bfloat16 wsm[];   // [cin][cout_p] of the current tap
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
+  const long long base = ((long long)blockIdx.x * kWarps + warp) * (16 * kMT);
+  const int ncol = c.cin;   // output columns of this GEMM
+  const int col0 = blockIdx.y * NT * 8;
+  long long row[kMT][2];
+  int rz[kMT][2], ry[kMT][2], rx[kMT][2], rn[kMT][2];
+  bool rv[kMT][2];
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int h = 0; h < 2; ++h) {
+      long long p = base + mt * 16 + g + 8 * h;
+      rv[mt][h] = p < nvox;
+      row[mt][h] = p;
+      long long pp = rv[mt][h] ? p : 0;
+      rx[mt][h] = (int)(pp % c.ix); pp /= c.ix;
+      ry[mt][h] = (int)(pp % c.iy); pp /= c.iy;
+      rz[mt][h] = (int)(pp % c.iz); rn[mt][h] = (int)(pp / c.iz);
+    }
+  float acc[kMT][NT][4];
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int nt = 0; nt < NT; ++nt)
+      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
+  const int chunks = c.cout_p / 16;
+  for (int tap = 0; tap < 27; ++tap) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < c.cin * c.cout_p / 2; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(wsm)[i] = reinterpret_cast<const uint32_t*>(wt + (size_t)tap * c.cin * c.cout_p)[i];
+    __syncthreads();
+    const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
+    long long q[kMT][2];
+    bool qv[kMT][2];
+    for (int mt = 0; mt < kMT; ++mt)
+      for (int h = 0; h < 2; ++h) {
+        // output voxel reading this input voxel through the tap: p = s*q + k
+        const int az = rz[mt][h] - kz, ay = ry[mt][h] - ky, ax = rx[mt][h] - kx;
+        bool ok = rv[mt][h] && az >= 0 && ay >= 0 && ax >= 0;
+        int oz = az, oy = ay, ox = ax;
+        if (c.stride == 2) {
+          ok = ok && !(az & 1) && !(ay & 1) && !(ax & 1);
+          oz = az >> 1; oy = ay >> 1; ox = ax >> 1;
+        }
+        ok = ok && oz < c.oz && oy < c.oy && ox < c.ox;
+        qv[mt][h] = ok;
+        q[mt][h] = ok ? vox(rn[mt][h], oz, oy, ox, c.oz, c.oy, c.ox) : 0;
+      }
+    for (int ch = 0; ch < chunks; ++ch) {
+      const int c0 = ch * 16;
+      uint32_t a[kMT][4];
+      for (int mt = 0; mt < kMT; ++mt)
+        for (int h = 0; h < 2; ++h) {
+          uint32_t lo = 0u, hi = 0u;
+          if (qv[mt][h]) {
+            const uint32_t* sp = reinterpret_cast<const uint32_t*>(dy + q[mt][h] * c.cout_p + c0);
+            lo = __ldg(sp + t);
+            hi = __ldg(sp + 4 + t);
+          }
+          a[mt][h] = lo;
+          a[mt][2 + h] = hi;
+        }
+      for (int nt = 0; nt < NT; ++nt) {
+        const int ci = col0 + nt * 8 + g;
+        uint32_t b0 = 0u, b1 = 0u;
+        if (ci < ncol) {
+          const uint32_t* wp = reinterpret_cast<const uint32_t*>(wsm + (size_t)ci * c.cout_p + c0);
+          b0 = wp[t];
+          b1 = wp[4 + t];
+        }
+        for (int mt = 0; mt < kMT; ++mt) mma_bf16(acc[mt][nt], a[mt], b0, b1);
+      }
+    }
+  }
+  for (int mt = 0; mt < kMT; ++mt)
+    for (int h = 0; h < 2; ++h) {
+      if (!rv[mt][h]) continue;
+      const long long p = row[mt][h];
+      for (int nt = 0; nt < NT; ++nt) {
+        const int ci = col0 + nt * 8 + 2 * t;
+        if (ci < ncol) dx[p * ncol + ci] = acc[mt][nt][2 * h];
+        if (ci + 1 < ncol) dx[p * ncol + ci + 1] = acc[mt][nt][2 * h + 1];
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient: per (tap, chunk of output voxels) a [cout_p x cin] partial,
+// accumulated into float32 dw with atomics.  Operands are staged in shared
+// memory transposed so that the reduction index (voxel) is contiguous.
+// ---------------------------------------------------------------------------
+
+constexpr int kWgVox = 32;        // voxels per staged chunk (two k16 steps)
+constexpr int kWgChunks = 16;     // chunks per CTA
+
+__global__ void __launch_bounds__(kWarps * 32) k_conv_wgrad(Conv c, const __nv_bfloat16* __restrict__ x1,
+                                                            const __nv_bfloat16* __restrict__ x2,
+                                                            const __nv_bfloat16* __restrict__ dy,
+                                                            float* __restrict__ dw, float* __restrict__ db) {
+  extern __shared__ __nv_bfloat16 sm[];
+  const int cop = c.cout_p, cin = c.cin;
+  __nv_bfloat16* sdy = sm;                          // [cop][kWgVox]
+  __nv_bfloat16* sx = sm + cop * kWgVox;            // [cin][kWgVox]
+  const int tap = blockIdx.y;
+  const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
+  // output tiles: (cop/16) m-tiles x (cin/8) n-tiles, distributed over warps
+  const int mtiles = cop / 16, ntiles = cin / 8, tiles = mtiles * ntiles;
+  constexpr int kMaxTiles = 4 * 14 / kWarps + 1;   // cop <= 64, cin <= 112
+  float acc[kMaxTiles][4];
+  for (int i = 0; i < kMaxTiles; ++i)
+    for (int k = 0; k < 4; ++k) acc[i][k] = 0.f;
+  float bsum = 0.f;
+  for (int chunk = 0; chunk < kWgChunks; ++chunk) {
+    const long long q0 = ((long long)blockIdx.x * kWgChunks + chunk) * kWgVox;
+    if (q0 >= nvox) break;
+    __syncthreads();
+    // stage dy (transposed) and the tap-shifted input (transposed)
+    for (int i = threadIdx.x; i < kWgVox * cop; i += blockDim.x) {
+      const int v = i / cop, co = i - v * cop;
+      const long long q = q0 + v;
+      sdy[co * kWgVox + v] = q < nvox ? dy[q * cop + co] : __float2bfloat16(0.f);
+    }
+    for (int i = threadIdx.x; i < kWgVox * cin; i += blockDim.x) {
+      const int v = i / cin, ci = i - v * cin;
+      const long long q = q0 + v;
+      __nv_bfloat16 val = __float2bfloat16(0.f);
+      if (q < nvox) {
+        long long qq = q;
+        const int ox = (int)(qq % c.ox); qq /= c.ox;
+        const int oy = (int)(qq % c.oy); qq /= c.oy;
+        const int oz = (int)(qq % c.oz); const int n = (int)(qq / c.oz);
+        const int z = c.stride * oz + kz, yy = c.stride * oy + ky, xx = c.stride * ox + kx;
+        if (z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix) {
+          if (ci < c.c1) {
+            const long long p = c.up1 ? vox(n, z >> 1, yy >> 1, xx >> 1, (c.iz + 1) / 2, (c.iy + 1) / 2, (c.ix + 1) / 2)
+                                      : vox(n, z, yy, xx, c.iz, c.iy, c.ix);
+            val = x1[p * c.c1 + ci];
+          } else {
+            val = x2[vox(n, z, yy, xx, c.iz, c.iy, c.ix) * c.c2 + (ci - c.c1)];
+          }
+        }
+      }
+      sx[ci * kWgVox + v] = val;
+    }
+    __syncthreads();
+    if (tap == 13 && db != nullptr)
+      for (int co = threadIdx.x; co < c.cout; co += blockDim.x)
+        for (int v = 0; v < kWgVox; ++v) bsum += __bfloat162float(sdy[co * kWgVox + v]);
+    int slot = 0;
+    for (int tile = warp; tile < tiles; tile += kWarps, ++slot) {
+      const int mt = tile / ntiles, nt = tile - mt * ntiles;
+      for (int ks = 0; ks < kWgVox / 16; ++ks) {
+        uint32_t a[4];
+        const __nv_bfloat16* ap = sdy + (mt * 16) * kWgVox + ks * 16;
+        a[0] = *reinterpret_cast<const uint32_t*>(ap + g * kWgVox + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(ap + (g + 8) * kWgVox + 2 * t);
+        a[2] = *reinterpret_cast<const uint32_t*>(ap + g * kWgVox + 2 * t + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(ap + (g + 8) * kWgVox + 2 * t + 8);
+        const __nv_bfloat16* bp = sx + (nt * 8 + g) * kWgVox + ks * 16;
+        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(bp + 2 * t);
+        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(bp + 2 * t + 8);
+        mma_bf16(acc[slot], a, b0, b1);
+      }
+    }
+  }
+  int slot = 0;
+  for (int tile = warp; tile < tiles; tile += kWarps, ++slot) {
+    const int mt = tile / ntiles, nt = tile - mt * ntiles;
+    for (int h = 0; h < 2; ++h) {
+      const int co = mt * 16 + g + 8 * h;
+      const int ci = nt * 8 + 2 * t;
+      float* o = dw + ((size_t)tap * cop + co) * cin + ci;
+      atomicAdd(o, acc[slot][2 * h]);
+      atomicAdd(o + 1, acc[slot][2 * h + 1]);
+    }
+  }
+  if (tap == 13 && db != nullptr)
+    for (int co = threadIdx.x; co < c.cout; co += blockDim.x) atomicAdd(db + co, bsum);
+}
+
+// ---------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------
+
+// dpre = grad * LeakyReLU'(y) (y is the activation output, whose sign equals
+// the pre-activation's), bf16, channels padded to cout_p with zeros
+__global__ void k_act_backward(const float* __restrict__ grad, const __nv_bfloat16* __restrict__ y, int act,
+                               __nv_bfloat16* __restrict__ dpre, long long nvox, int cout, int cout_p) {
+  const long long total = nvox * cout_p;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long v = i / cout_p;
+    const int co = (int)(i - v * cout_p);
+    float d = 0.f;
+    if (co < cout) {
+      d = grad[v * cout + co];
+      if (act && y != nullptr && __bfloat162float(y[v * cout + co]) <= 0.f) d *= 0.1f;
+    }
+    dpre[i] = __float2bfloat16(d);
+  }
+}
+
+// scatter the virtual input's gradient: channels [0, c1) go to source 1
+// (summed over the 2x2x2 fine voxels of each coarse voxel when upsampled),
+// channels [c1, cin) to source 2; both accumulate (+=)
+__global__ void k_split_grad(Conv c, const float* __restrict__ dxv, float* __restrict__ g1, float* __restrict__ g2) {
+  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
+  const long long total = nvox * c.cin;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long p = i / c.cin;
+    const int ch = (int)(i - p * c.cin);
+    const float v = dxv[i];
+    if (ch >= c.c1) {
+      if (g2) g2[p * c.c2 + (ch - c.c1)] += v;
+    } else if (g1) {
+      if (c.up1) {
+        long long pp = p;
+        const int x = (int)(pp % c.ix); pp /= c.ix;
+        const int y = (int)(pp % c.iy); pp /= c.iy;
+        const int z = (int)(pp % c.iz); const int n = (int)(pp / c.iz);
+        const long long q = vox(n, z >> 1, y >> 1, x >> 1, (c.iz + 1) / 2, (c.iy + 1) / 2, (c.ix + 1) / 2);
+        atomicAdd(g1 + q * c.c1 + ch, v);
+      } else {
+        g1[p * c.c1 + ch] += v;
+      }
+    }
+  }
+}
+
+// Adam on float32 master weights; also writes the bf16 forward weights and,
+// for layers with a data-gradient pass, the transposed bf16 weights
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ gw, float* __restrict__ m, float* __restrict__ v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2, float decay) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = gw[i] + decay * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// float32 [tap][cout_p][cin] -> bf16 forward weights and bf16 [tap][cin][cout_p]
+__global__ void k_weights_to_bf16(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
+                                  __nv_bfloat16* __restrict__ wt, int cout_p, int cin) {
+  const long long n = 27LL * cout_p * cin;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long tap = i / ((long long)cout_p * cin);
+    const int rem = (int)(i - tap * cout_p * cin);
+    const int co = rem / cin, ci = rem - co * cin;
+    const __nv_bfloat16 b = __float2bfloat16(w[i]);
+    wf[i] = b;
+    if (wt) wt[(tap * cin + ci) * cout_p + co] = b;
+  }
+}
+
+// flow loss: l2 * mean |pred - target|^2 plus a warped-residual term
+// res * mean (mov(p + f(p)) - tmpl(p))^2 on the network's grid (flow in
+// full-resolution voxels; x and y are divided by `scale` on that grid)
+__global__ void k_flow_loss(const float* __restrict__ pred, const float* __restrict__ target,
+                            const float* __restrict__ tmpl, const float* __restrict__ mov, float* __restrict__ grad,
+                            double* __restrict__ loss, int n, int Z, int Y, int X, float scale, float l2, float res) {
+  const long long nvox = (long long)n * Z * Y * X;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvox;
+       i += (long long)gridDim.x * blockDim.x) {
+    float g[3] = {0.f, 0.f, 0.f};
+    double li = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const float d = pred[3 * i + k] - target[3 * i + k];
+      li += (double)l2 * d * d;
+      g[k] = 2.f * l2 * d;
+    }
+    if (res > 0.f) {
+      long long ii = i;
+      const int x = (int)(ii % X); ii /= X;
+      const int y = (int)(ii % Y); ii /= Y;
+      const int z = (int)(ii % Z); const int b = (int)(ii / Z);
+      const float cx = x + pred[3 * i] / scale, cy = y + pred[3 * i + 1] / scale, cz = z + pred[3 * i + 2];
+      const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+      const float tx = cx - fx, ty = cy - fy, tz = cz - fz;
+      int xs[2], ys[2], zs[2];
+      xs[0] = min(max((int)fx, 0), X - 1); xs[1] = min(max((int)fx + 1, 0), X - 1);
+      ys[0] = min(max((int)fy, 0), Y - 1); ys[1] = min(max((int)fy + 1, 0), Y - 1);
+      zs[0] = min(max((int)fz, 0), Z - 1); zs[1] = min(max((int)fz + 1, 0), Z - 1);
+      float v = 0.f, dvx = 0.f, dvy = 0.f, dvz = 0.f;
+      for (int a = 0; a < 2; ++a)
+        for (int bb = 0; bb < 2; ++bb)
+          for (int cc = 0; cc < 2; ++cc) {
+            const float m = mov[(((long long)b * Z + zs[a]) * Y + ys[bb]) * X + xs[cc]];
+            const float wz = a ? tz : 1.f - tz, wy = bb ? ty : 1.f - ty, wx = cc ? tx : 1.f - tx;
+            v += wz * wy * wx * m;
+            dvx += wz * wy * (cc ? 1.f : -1.f) * m;
+            dvy += wz * wx * (bb ? 1.f : -1.f) * m;
+            dvz += wy * wx * (a ? 1.f : -1.f) * m;
+          }
+      const float r = v - tmpl[i];
+      li += (double)res * r * r;
+      g[0] += 2.f * res * r * dvx / scale;
+      g[1] += 2.f * res * r * dvy / scale;
+      g[2] += 2.f * res * r * dvz;
+    }
+    for (int k = 0; k < 3; ++k) grad[3 * i + k] = g[k] / (float)nvox;
+    acc += li;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, red[0] / (double)nvox);
+}
+
+static int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b < 1) b = 1;
+  return (int)(b < 148LL * 16 ? b : 148LL * 16);
+}
+
+static int check(const WrConvGeom* g, Conv* c) {
+  if (!g) return fail(WR_E_NULL, "geometry is NULL");
+  c->n = g->n; c->oz = g->oz; c->oy = g->oy; c->ox = g->ox;
+  c->iz = g->iz; c->iy = g->iy; c->ix = g->ix;
+  c->stride = g->stride; c->c1 = g->c1; c->c2 = g->c2; c->up1 = g->up1;
+  c->cin = g->c1 + g->c2; c->cout = g->cout; c->cout_p = (g->cout + 15) / 16 * 16; c->act = g->act;
+  if (c->n < 1 || c->oz < 1 || c->oy < 1 || c->ox < 1 || c->iz < 1 || c->iy < 1 || c->ix < 1)
+    return fail(WR_E_SHAPE, "empty grid");
+  if (c->stride != 1 && c->stride != 2) return fail(WR_E_PARAM, "stride must be 1 or 2");
+  if (c->c1 % 16 || c->c2 % 16 || c->cin < 16 || c->cin > 112) return fail(WR_E_PARAM, "channels must be multiples of 16, total <= 112");
+  if (c->cout < 1 || c->cout_p > 64) return fail(WR_E_PARAM, "cout must be in [1, 64]");
+  const int ez = (c->iz - 1) / c->stride + 1, ey = (c->iy - 1) / c->stride + 1, ex = (c->ix - 1) / c->stride + 1;
+  if (c->oz != ez || c->oy != ey || c->ox != ex) return fail(WR_E_SHAPE, "output grid does not match input and stride");
+  return WR_OK;
+}
+
+template <int NT>
+static void launch_fwd(const Conv& c, const void* x1, const void* x2, const void* w, const float* b, void* y, float* y32,
+                       cudaStream_t s) {
+  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
+  const int blocks = (int)((nvox + kWarps * 16 * kMT - 1) / (kWarps * 16 * kMT));
+  k_conv_fwd<NT><<<blocks, kWarps * 32, (size_t)c.cout_p * c.cin * 2, s>>>(
+      c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2, (const __nv_bfloat16*)w, b, (__nv_bfloat16*)y, y32);
+}
+
+}  // namespace wrnet
+
+using namespace wrnet;
+
+extern "C" {
+
+const char* wr_net_last_error(void) { return g_err.c_str(); }
+
+int wr_net_conv3d_fwd(const WrConvGeom* geom, const void* x1, const void* x2, const void* w, const float* bias,
+                      void* y, float* y32, void* stream) {
+  Conv c;
+  int rc = check(geom, &c);
+  if (rc) return rc;
+  if (!x1 || !w || !bias || (!y && !y32) || (c.c2 && !x2)) return fail(WR_E_NULL, "a required pointer is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (c.cout_p / 8) {
+    case 2: launch_fwd<2>(c, x1, x2, w, bias, y, y32, s); break;
+    case 4: launch_fwd<4>(c, x1, x2, w, bias, y, y32, s); break;
+    case 6: launch_fwd<6>(c, x1, x2, w, bias, y, y32, s); break;
+    default: launch_fwd<8>(c, x1, x2, w, bias, y, y32, s); break;
+  }
+  return cuda_status("wr_net_conv3d_fwd");
+}
+
+int wr_net_conv3d_dgrad(const WrConvGeom* geom, const void* dy, const void* wt, float* dxv, void* stream) {
+  Conv c;
+  int rc = check(geom, &c);
+  if (rc) return rc;
+  if (!dy || !wt || !dxv) return fail(WR_E_NULL, "a required pointer is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
+  constexpr int NT = 4;   // 32 input channels per CTA column
+  dim3 grid((unsigned)((nvox + kWarps * 16 * kMT - 1) / (kWarps * 16 * kMT)), (unsigned)((c.cin + NT * 8 - 1) / (NT * 8)));
+  k_conv_dgrad<NT><<<grid, kWarps * 32, (size_t)c.cin * c.cout_p * 2, s>>>(c, (const __nv_bfloat16*)dy,
+                                                                           (const __nv_bfloat16*)wt, dxv);
+  return cuda_status("wr_net_conv3d_dgrad");
+}
+
+int wr_net_conv3d_wgrad(const WrConvGeom* geom, const void* x1, const void* x2, const void* dy, float* dw, float* db,
+                        void* stream) {
+  Conv c;
+  int rc = check(geom, &c);
+  if (rc) return rc;
+  if (!x1 || !dy || !dw || (c.c2 && !x2)) return fail(WR_E_NULL, "a required pointer is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
+  dim3 grid((unsigned)((nvox + kWgVox * kWgChunks - 1) / (kWgVox * kWgChunks)), 27);
+  k_conv_wgrad<<<grid, kWarps * 32, (size_t)(c.cout_p + c.cin) * kWgVox * 2, s>>>(
+      c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2, (const __nv_bfloat16*)dy, dw, db);
+  return cuda_status("wr_net_conv3d_wgrad");
+}
+
+int wr_net_act_backward(const float* grad, const void* y, int act, void* dpre, long long nvox, int cout, void* stream) {
+  if (!grad || !dpre) return fail(WR_E_NULL, "a required pointer is NULL");
+  const int cout_p = (cout + 15) / 16 * 16;
+  k_act_backward<<<grid_for(nvox * cout_p), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      grad, (const __nv_bfloat16*)y, act, (__nv_bfloat16*)dpre, nvox, cout, cout_p);
+  return cuda_status("wr_net_act_backward");
+}
+
+int wr_net_split_grad(const WrConvGeom* geom, const float* dxv, float* g1, float* g2, void* stream) {
+  Conv c;
+  int rc = check(geom, &c);
+  if (rc) return rc;
+  if (!dxv) return fail(WR_E_NULL, "dxv is NULL");
+  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
+  k_split_grad<<<grid_for(nvox * c.cin), 256, 0, static_cast<cudaStream_t>(stream)>>>(c, dxv, g1, g2);
+  return cuda_status("wr_net_split_grad");
+}
+
+int wr_net_adam(float* w, const float* gw, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                int step, float decay, void* stream) {
+  if (!w || !gw || !m || !v) return fail(WR_E_NULL, "a required pointer is NULL");
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, gw, m, v, n, lr, b1, b2, eps, c1, c2, decay);
+  return cuda_status("wr_net_adam");
+}
+
+int wr_net_weights_to_bf16(const float* w, void* wf, void* wt, int cout, int cin, void* stream) {
+  if (!w || !wf) return fail(WR_E_NULL, "a required pointer is NULL");
+  const int cout_p = (cout + 15) / 16 * 16;
+  k_weights_to_bf16<<<grid_for(27LL * cout_p * cin), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      w, (__nv_bfloat16*)wf, (__nv_bfloat16*)wt, cout_p, cin);
+  return cuda_status("wr_net_weights_to_bf16");
+}
+
+int wr_net_flow_loss(const float* pred, const float* target, const float* tmpl, const float* mov, float* grad,
+                     double* loss, int n, int nz, int ny, int nx, float scale, float l2, float res, void* stream) {
+  if (!pred || !target || !grad || !loss || (res > 0.f && (!tmpl || !mov))) return fail(WR_E_NULL, "a required pointer is NULL");
+  k_flow_loss<<<grid_for((long long)n * nz * ny * nx), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      pred, target, tmpl, mov, grad, loss, n, nz, ny, nx, scale, l2, res);
+  return cuda_status("wr_net_flow_loss");
+}
+
+}  // extern "C"
