@@ -74,6 +74,25 @@ WR_API int wr_net_flow_loss(const float* pred, const float* target, const float*
                             float* grad, double* loss, int n, int nz, int ny, int nx, float scale, float l2,
                             float res, void* stream);
 
+/* Network input from a (z, y, x) template / moving pair (uint16 or float32):
+   factor x factor mean pooling in x and y, divided by the template's mean
+   (computed into *mean_scratch, one device double); x0 bf16 [z][y/f][x/f][16]
+   with channels 0 / 1 = template / moving; t4, m4 (nullable) float32 copies. */
+WR_API int wr_net_prepare_input(const WrVolume* tmpl, const WrVolume* mov, int factor, double* mean_scratch,
+                                void* x0, float* t4, float* m4, void* stream);
+
+/* Adds sum((a - b)^2) and the voxel count over voxels with excl == 0 (or all
+   when excl is NULL) to out2[0], out2[1]; a float32, b uint16 or float32.
+   Used to compare a warm-started registration's residual with the plain
+   method's. */
+WR_API int wr_net_masked_sse(const float* a, const WrVolume* b, const uint8_t* excl, double* out2, void* stream);
+
+/* Flow (z, y, x, 3) -> factor x factor mean pooling in x and y. */
+WR_API int wr_net_pool_flow(const float* flow, int nz, int ny, int nx, int factor, float* out, void* stream);
+
+/* Coarse flow (z, y/f, x/f, 3) -> (z, y, x, 3), bilinear in x and y. */
+WR_API int wr_net_upsample_flow(const float* fq, int nz, int ny, int nx, int factor, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

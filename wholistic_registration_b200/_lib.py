@@ -50,6 +50,10 @@ EXPORTS = (
     "wr_net_adam",
     "wr_net_weights_to_bf16",
     "wr_net_flow_loss",
+    "wr_net_prepare_input",
+    "wr_net_masked_sse",
+    "wr_net_pool_flow",
+    "wr_net_upsample_flow",
 )
 
 
@@ -159,6 +163,11 @@ def load():
         lib.wr_net_weights_to_bf16.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
         lib.wr_net_flow_loss.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, fl, fl, fl, vp]
+        ci = ctypes.c_int
+        lib.wr_net_prepare_input.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), ci, vp, vp, vp, vp, vp]
+        lib.wr_net_masked_sse.argtypes = [vp, ctypes.POINTER(WrVolume), vp, vp, vp]
+        lib.wr_net_pool_flow.argtypes = [vp, ci, ci, ci, ci, vp, vp]
+        lib.wr_net_upsample_flow.argtypes = [vp, ci, ci, ci, ci, vp, vp]
         for name in EXPORTS:
             getattr(lib, name).restype = (ctypes.c_char_p if name in ("wr_last_error", "wr_net_last_error")
                                           else ctypes.c_int)

@@ -498,6 +498,123 @@ __global__ void k_flow_loss(const float* __restrict__ pred, const float* __restr
   if (threadIdx.x == 0) atomicAdd(loss, red[0] / (double)nvox);
 }
 
+// mean of a (z, y, x) volume (float64), one value to device memory
+template <typename T>
+__global__ void k_mean(const T* __restrict__ v, long long n, double* __restrict__ out) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc += (double)v[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(out, red[0] / (double)n);
+}
+
+// network input: f x f mean pooling in x and y of template (channel 0) and
+// moving (channel 1), divided by the template mean; channels 2..15 zero.
+// Float32 copies of both pooled volumes feed the residual loss.
+template <typename T>
+__global__ void k_pool_input(const T* __restrict__ tmpl, const T* __restrict__ mov, const double* __restrict__ mean,
+                             int Z, int Y, int X, int f, __nv_bfloat16* __restrict__ x0, float* __restrict__ t4,
+                             float* __restrict__ m4) {
+  const int Yq = Y / f, Xq = X / f;
+  const long long n = (long long)Z * Yq * Xq;
+  const float inv = (float)(1.0 / fmax(*mean, 1e-12));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % Xq);
+    const long long r = i / Xq;
+    const int y = (int)(r % Yq), z = (int)(r / Yq);
+    float st = 0.f, sm = 0.f;
+    for (int dy = 0; dy < f; ++dy)
+      for (int dx = 0; dx < f; ++dx) {
+        const long long p = ((long long)z * Y + y * f + dy) * X + x * f + dx;
+        st += (float)tmpl[p];
+        sm += (float)mov[p];
+      }
+    st *= inv / (f * f);
+    sm *= inv / (f * f);
+    if (t4) t4[i] = st;
+    if (m4) m4[i] = sm;
+    __nv_bfloat16* o = x0 + i * 16;
+    o[0] = __float2bfloat16(st);
+    o[1] = __float2bfloat16(sm);
+    for (int c = 2; c < 16; ++c) o[c] = __float2bfloat16(0.f);
+  }
+}
+
+// flow (z, y, x, 3) -> mean over f x f blocks in x and y
+__global__ void k_pool_flow(const float* __restrict__ flow, int Z, int Y, int X, int f, float* __restrict__ out) {
+  const int Yq = Y / f, Xq = X / f;
+  const long long n = (long long)Z * Yq * Xq;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % Xq);
+    const long long r = i / Xq;
+    const int y = (int)(r % Yq), z = (int)(r / Yq);
+    float a[3] = {0.f, 0.f, 0.f};
+    for (int dy = 0; dy < f; ++dy)
+      for (int dx = 0; dx < f; ++dx) {
+        const long long p = ((long long)z * Y + y * f + dy) * X + x * f + dx;
+        for (int c = 0; c < 3; ++c) a[c] += flow[3 * p + c];
+      }
+    for (int c = 0; c < 3; ++c) out[3 * i + c] = a[c] / (f * f);
+  }
+}
+
+// coarse flow (z, Y/f, X/f, 3) -> full-resolution (z, Y, X, 3), bilinear in x
+// and y on pixel centres, edge-clamped
+__global__ void k_upsample_flow(const float* __restrict__ fq, int Z, int Y, int X, int f, float* __restrict__ out) {
+  const int Yq = Y / f, Xq = X / f;
+  const long long n = (long long)Z * Y * X;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % X);
+    const long long r = i / X;
+    const int y = (int)(r % Y), z = (int)(r / Y);
+    const float cx = fminf(fmaxf((x + 0.5f) / f - 0.5f, 0.f), (float)(Xq - 1));
+    const float cy = fminf(fmaxf((y + 0.5f) / f - 0.5f, 0.f), (float)(Yq - 1));
+    const int x0 = (int)cx, y0 = (int)cy;
+    const int x1 = min(x0 + 1, Xq - 1), y1 = min(y0 + 1, Yq - 1);
+    const float tx = cx - x0, ty = cy - y0;
+    const float* b = fq + (long long)z * Yq * Xq * 3;
+    for (int c = 0; c < 3; ++c) {
+      const float v00 = b[(y0 * Xq + x0) * 3 + c], v01 = b[(y0 * Xq + x1) * 3 + c];
+      const float v10 = b[(y1 * Xq + x0) * 3 + c], v11 = b[(y1 * Xq + x1) * 3 + c];
+      out[3 * i + c] = (1.f - ty) * ((1.f - tx) * v00 + tx * v01) + ty * ((1.f - tx) * v10 + tx * v11);
+    }
+  }
+}
+
+// mean of (a - b)^2 over voxels not excluded (mask == 0 or no mask)
+template <typename T>
+__global__ void k_masked_mse(const float* __restrict__ a, const T* __restrict__ b, const uint8_t* __restrict__ excl,
+                             long long n, double* __restrict__ out) {
+  __shared__ double red[2][256];
+  double s = 0.0, c = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (excl && excl[i]) continue;
+    const double d = (double)a[i] - (double)b[i];
+    s += d * d;
+    c += 1.0;
+  }
+  red[0][threadIdx.x] = s;
+  red[1][threadIdx.x] = c;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + k];
+      red[1][threadIdx.x] += red[1][threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(out, red[0][0]);
+    atomicAdd(out + 1, red[1][0]);
+  }
+}
+
 static int grid_for(long long n) {
   long long b = (n + 255) / 256;
   if (b < 1) b = 1;
@@ -621,6 +738,55 @@ int wr_net_flow_loss(const float* pred, const float* target, const float* tmpl, 
   k_flow_loss<<<grid_for((long long)n * nz * ny * nx), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       pred, target, tmpl, mov, grad, loss, n, nz, ny, nx, scale, l2, res);
   return cuda_status("wr_net_flow_loss");
+}
+
+int wr_net_prepare_input(const WrVolume* tmpl, const WrVolume* mov, int factor, double* mean_scratch, void* x0,
+                         float* t4, float* m4, void* stream) {
+  if (!tmpl || !mov || !tmpl->data || !mov->data || !mean_scratch || !x0) return fail(WR_E_NULL, "a required pointer is NULL");
+  if (tmpl->dtype != mov->dtype || (tmpl->dtype != WR_U16 && tmpl->dtype != WR_F32)) return fail(WR_E_DTYPE, "uint16 or float32 volumes of one type");
+  if (tmpl->nz != mov->nz || tmpl->ny != mov->ny || tmpl->nx != mov->nx) return fail(WR_E_SHAPE, "shapes differ");
+  if (factor < 1 || tmpl->ny % factor || tmpl->nx % factor) return fail(WR_E_SHAPE, "x and y extents must be multiples of factor");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long n = (long long)tmpl->nz * tmpl->ny * tmpl->nx;
+  const long long nq = n / (factor * factor);
+  cudaMemsetAsync(mean_scratch, 0, sizeof(double), s);
+  if (tmpl->dtype == WR_U16) {
+    k_mean<uint16_t><<<grid_for(n), 256, 0, s>>>((const uint16_t*)tmpl->data, n, mean_scratch);
+    k_pool_input<uint16_t><<<grid_for(nq), 256, 0, s>>>((const uint16_t*)tmpl->data, (const uint16_t*)mov->data,
+                                                        mean_scratch, tmpl->nz, tmpl->ny, tmpl->nx, factor,
+                                                        (__nv_bfloat16*)x0, t4, m4);
+  } else {
+    k_mean<float><<<grid_for(n), 256, 0, s>>>((const float*)tmpl->data, n, mean_scratch);
+    k_pool_input<float><<<grid_for(nq), 256, 0, s>>>((const float*)tmpl->data, (const float*)mov->data, mean_scratch,
+                                                     tmpl->nz, tmpl->ny, tmpl->nx, factor, (__nv_bfloat16*)x0, t4, m4);
+  }
+  return cuda_status("wr_net_prepare_input");
+}
+
+int wr_net_masked_sse(const float* a, const WrVolume* b, const uint8_t* excl, double* out2, void* stream) {
+  if (!a || !b || !b->data || !out2) return fail(WR_E_NULL, "a required pointer is NULL");
+  const long long n = (long long)b->nz * b->ny * b->nx;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->dtype == WR_U16) k_masked_mse<uint16_t><<<grid_for(n), 256, 0, s>>>(a, (const uint16_t*)b->data, excl, n, out2);
+  else if (b->dtype == WR_F32) k_masked_mse<float><<<grid_for(n), 256, 0, s>>>(a, (const float*)b->data, excl, n, out2);
+  else return fail(WR_E_DTYPE, "uint16 or float32 volume");
+  return cuda_status("wr_net_masked_sse");
+}
+
+int wr_net_pool_flow(const float* flow, int nz, int ny, int nx, int factor, float* out, void* stream) {
+  if (!flow || !out) return fail(WR_E_NULL, "a required pointer is NULL");
+  if (factor < 1 || ny % factor || nx % factor) return fail(WR_E_SHAPE, "x and y extents must be multiples of factor");
+  const long long nq = (long long)nz * (ny / factor) * (nx / factor);
+  k_pool_flow<<<grid_for(nq), 256, 0, static_cast<cudaStream_t>(stream)>>>(flow, nz, ny, nx, factor, out);
+  return cuda_status("wr_net_pool_flow");
+}
+
+int wr_net_upsample_flow(const float* fq, int nz, int ny, int nx, int factor, float* out, void* stream) {
+  if (!fq || !out) return fail(WR_E_NULL, "a required pointer is NULL");
+  if (factor < 1 || ny % factor || nx % factor) return fail(WR_E_SHAPE, "x and y extents must be multiples of factor");
+  k_upsample_flow<<<grid_for((long long)nz * ny * nx), 256, 0, static_cast<cudaStream_t>(stream)>>>(fq, nz, ny, nx,
+                                                                                                     factor, out);
+  return cuda_status("wr_net_upsample_flow");
 }
 
 }  // extern "C"
