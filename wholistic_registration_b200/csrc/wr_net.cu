@@ -171,6 +171,129 @@ __global__ void __launch_bounds__(kWarps * 32) k_conv_fwd(Conv c, const __nv_bfl
 }
 
 // ---------------------------------------------------------------------------
+// forward, stride 1, shared-memory tiled: the CTA's 4x4x8 output voxels read
+// a 6x6x10 input tile staged once in shared memory (both sources, source 1
+// replicated onto the fine grid when it is upsampled); A and B fragments come
+// from ldmatrix.  Voxel rows are padded to an odd number of 16-byte chunks so
+// the 8 rows of each ldmatrix land in distinct banks.
+// ---------------------------------------------------------------------------
+
+constexpr int kTZ = 4, kTY = 4, kTX = 8;                 // output tile (128 voxels, one z plane per warp)
+constexpr int kHZ = kTZ + 2, kHY = kTY + 2, kHX = kTX + 2;
+constexpr int kHalo = kHZ * kHY * kHX;                   // 360 input voxels
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+
+__host__ __device__ inline int tile_row_elems(int cin) { return cin + 8; }
+
+template <int NT>
+__global__ void __launch_bounds__(kWarps * 32) k_conv_fwd_tiled(Conv c, const __nv_bfloat16* __restrict__ x1,
+                                                                const __nv_bfloat16* __restrict__ x2,
+                                                                const __nv_bfloat16* __restrict__ w,
+                                                                const float* __restrict__ bias,
+                                                                __nv_bfloat16* __restrict__ y, float* __restrict__ y32) {
+  extern __shared__ __align__(16) __nv_bfloat16 sm[];
+  const int rs = tile_row_elems(c.cin);               // elements per voxel row
+  __nv_bfloat16* tile = sm;                            // [kHalo][rs]
+  __nv_bfloat16* wsm = sm + kHalo * rs;                // [cout_p][rs]
+  const int tiles_x = (c.ox + kTX - 1) / kTX, tiles_y = (c.oy + kTY - 1) / kTY, tiles_z = (c.oz + kTZ - 1) / kTZ;
+  int b = blockIdx.x;
+  const int bx = b % tiles_x; b /= tiles_x;
+  const int by = b % tiles_y; b /= tiles_y;
+  const int bz = b % tiles_z;
+  const int n = b / tiles_z;
+  const int ox0 = bx * kTX, oy0 = by * kTY, oz0 = bz * kTZ;
+  const int hz = (c.iz + 1) / 2, hy = (c.iy + 1) / 2, hx = (c.ix + 1) / 2;
+  // stage the input tile: 16-byte chunks of every halo voxel
+  const int cpr = c.cin / 8;
+  for (int i = threadIdx.x; i < kHalo * cpr; i += blockDim.x) {
+    const int v = i / cpr, ch = i - v * cpr;
+    const int lx = v % kHX, ly = (v / kHX) % kHY, lz = v / (kHX * kHY);
+    const int z = oz0 - 1 + lz, yy = oy0 - 1 + ly, xx = ox0 - 1 + lx;
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+    if (z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix) {
+      const int c0 = ch * 8;
+      if (c0 < c.c1) {
+        const long long p = c.up1 ? vox(n, z >> 1, yy >> 1, xx >> 1, hz, hy, hx) : vox(n, z, yy, xx, c.iz, c.iy, c.ix);
+        val = __ldg(reinterpret_cast<const uint4*>(x1 + p * c.c1 + c0));
+      } else {
+        val = __ldg(reinterpret_cast<const uint4*>(x2 + vox(n, z, yy, xx, c.iz, c.iy, c.ix) * c.c2 + (c0 - c.c1)));
+      }
+    }
+    *reinterpret_cast<uint4*>(tile + v * rs + ch * 8) = val;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  float acc[2][NT][4];
+  for (int mt = 0; mt < 2; ++mt)
+    for (int nt = 0; nt < NT; ++nt)
+      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
+  // ldmatrix row this lane addresses: matrix j = lane / 8, row r = lane % 8
+  const int j = lane >> 3, r = lane & 7;
+  const int chunks = c.cin / 16;
+  for (int tap = 0; tap < 27; ++tap) {
+    __syncthreads();
+    const int cp = c.cin / 8;
+    for (int i = threadIdx.x; i < c.cout_p * cp; i += blockDim.x) {
+      const int co = i / cp, ch = i - co * cp;
+      *reinterpret_cast<uint4*>(wsm + co * rs + ch * 8) =
+          __ldg(reinterpret_cast<const uint4*>(w + ((size_t)tap * c.cout_p + co) * c.cin + ch * 8));
+    }
+    __syncthreads();
+    const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
+    // output voxel of this lane's ldmatrix row in m-tile mt: (warp, ty, tx)
+    const __nv_bfloat16* arow[2];
+    for (int mt = 0; mt < 2; ++mt) {
+      const int m = mt * 16 + r + 8 * (j & 1);
+      const int ty = m >> 3, tx = m & 7;
+      arow[mt] = tile + (((warp + kz) * kHY + ty + ky) * kHX + tx + kx) * rs + 8 * (j >> 1);
+    }
+    for (int ch = 0; ch < chunks; ++ch) {
+      uint32_t a[2][4];
+      ldsm_x4(a[0], arow[0] + ch * 16);
+      ldsm_x4(a[1], arow[1] + ch * 16);
+#pragma unroll
+      for (int np = 0; np < NT / 2; ++np) {
+        // two n8 tiles: matrices (co 0-7, k lo), (co 0-7, k hi), (co 8-15, k lo), (co 8-15, k hi)
+        uint32_t bm[4];
+        ldsm_x4(bm, wsm + (np * 16 + r + 8 * (j >> 1)) * rs + ch * 16 + 8 * (j & 1));
+        mma_bf16(acc[0][2 * np], a[0], bm[0], bm[1]);
+        mma_bf16(acc[1][2 * np], a[1], bm[0], bm[1]);
+        mma_bf16(acc[0][2 * np + 1], a[0], bm[2], bm[3]);
+        mma_bf16(acc[1][2 * np + 1], a[1], bm[2], bm[3]);
+      }
+    }
+  }
+  for (int mt = 0; mt < 2; ++mt)
+    for (int h = 0; h < 2; ++h) {
+      const int m = mt * 16 + g + 8 * h;
+      const int oz = oz0 + warp, oy = oy0 + (m >> 3), ox = ox0 + (m & 7);
+      if (oz >= c.oz || oy >= c.oy || ox >= c.ox) continue;
+      const long long q = vox(n, oz, oy, ox, c.oz, c.oy, c.ox);
+      for (int nt = 0; nt < NT; ++nt) {
+        const int co = nt * 8 + 2 * t;
+        float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
+        if (co < c.cout) v0 += bias[co];
+        if (co + 1 < c.cout) v1 += bias[co + 1];
+        if (c.act) {
+          v0 = v0 > 0.f ? v0 : 0.1f * v0;
+          v1 = v1 > 0.f ? v1 : 0.1f * v1;
+        }
+        if (y32) {
+          if (co < c.cout) y32[q * c.cout + co] = v0;
+          if (co + 1 < c.cout) y32[q * c.cout + co + 1] = v1;
+        } else if (co < c.cout) {
+          *reinterpret_cast<__nv_bfloat162*>(y + q * c.cout + co) = __floats2bfloat162_rn(v0, v1);
+        }
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // data gradient: GEMM over input voxels p (fine grid of the virtual input),
 // k = (tap, co); weights transposed to wt[tap][ci][co_p]
 // ---------------------------------------------------------------------------
@@ -640,6 +763,14 @@ static int check(const WrConvGeom* g, Conv* c) {
 template <int NT>
 static void launch_fwd(const Conv& c, const void* x1, const void* x2, const void* w, const float* b, void* y, float* y32,
                        cudaStream_t s) {
+  if (c.stride == 1) {
+    const int tiles = ((c.ox + kTX - 1) / kTX) * ((c.oy + kTY - 1) / kTY) * ((c.oz + kTZ - 1) / kTZ) * c.n;
+    const size_t smem = (size_t)(kHalo + c.cout_p) * tile_row_elems(c.cin) * 2;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_conv_fwd_tiled<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_conv_fwd_tiled<NT><<<tiles, kWarps * 32, smem, s>>>(c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2,
+                                                          (const __nv_bfloat16*)w, b, (__nv_bfloat16*)y, y32);
+    return;
+  }
   const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
   const int blocks = (int)((nvox + kWarps * 16 * kMT - 1) / (kWarps * 16 * kMT));
   k_conv_fwd<NT><<<blocks, kWarps * 32, (size_t)c.cout_p * c.cin * 2, s>>>(
