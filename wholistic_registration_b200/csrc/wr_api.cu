@@ -8,6 +8,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "wr_b200.h"
 #include "wr_kernels.cuh"
@@ -37,6 +38,43 @@ struct Alloc {
     return off;
   }
 };
+
+// Shift-invariant interior of the full-res -> level table along one axis:
+// the widest range of outputs around the middle whose tap rows (as
+// resize_row computes them) read in[s*o + c0 + t] with bit-identical weights.
+static SITaps find_si_taps(int in_len, int out_len) {
+  SITaps si;
+  memset(&si, 0, sizeof(si));
+  const int P = resize_taps(in_len, out_len);
+  if (P > kSIMaxTaps || out_len < 1 || in_len % out_len != 0) return si;
+  const int s = in_len / out_len;
+  std::vector<double> w((size_t)out_len * P);
+  std::vector<int32_t> ix((size_t)out_len * P);
+  for (int k = 0; k < out_len; ++k) resize_row(in_len, out_len, RESIZE_BICUBIC, k, &w[(size_t)k * P], &ix[(size_t)k * P]);
+  const int mid = out_len / 2;
+  const int c0 = ix[(size_t)mid * P] - s * mid;
+  auto fits = [&](int k) {
+    for (int t = 0; t < P; ++t) {
+      if (ix[(size_t)k * P + t] != s * k + c0 + t) return false;
+      if (memcmp(&w[(size_t)k * P + t], &w[(size_t)mid * P + t], sizeof(double)) != 0) return false;
+    }
+    return true;
+  };
+  if (!fits(mid)) return si;
+  int lo = mid, hi = mid + 1;
+  while (lo > 0 && fits(lo - 1)) --lo;
+  while (hi < out_len && fits(hi)) ++hi;
+  si.P = P; si.s = s; si.c0 = c0; si.lo = lo; si.hi = hi;
+  si.ls = in_len / s + 1;
+  for (int t = 0; t < P; ++t) {
+    si.w[t] = w[(size_t)mid * P + t];
+    si.wf[t] = (float)si.w[t];
+    const int e = c0 + t;                         // tap position of output 0
+    const int q = e >= 0 ? e / s : -((-e + s - 1) / s);
+    si.off[t] = (e - q * s) * si.ls + q;
+  }
+  return si;
+}
 
 static int level_extent(int n, int layer) { return (int)((double)n / (double)(1 << layer)); }
 
@@ -91,6 +129,10 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.x_first = sx <= sy;
     L.tx_taps = resize_taps(nx, L.nx);
     L.ty_taps = resize_taps(ny, L.ny);
+    if (l > 0) {
+      L.six = find_si_taps(nx, L.nx);
+      L.siy = find_si_taps(ny, L.ny);
+    }
     const size_t vbytes = p->precision == WR_PREC_F32 ? 4 : 2;   // per stored channel value
     L.ref = A.take((size_t)L.n * vbytes);
     L.movg = A.take((size_t)L.n * 4 * vbytes);
@@ -126,6 +168,13 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     tmp_a = first > tmp_a ? first : tmp_a;
     tmp_b = (size_t)C.n * 3 > tmp_b ? (size_t)C.n * 3 : tmp_b;
   }
+  // row-major x tables before their transpose
+  size_t tab = 0;
+  for (int l = 0; l < P.levels; ++l) {
+    const size_t b = (size_t)P.lv[l].nx * P.lv[l].tx_taps * 12;
+    tab = b > tab ? b : tab;
+  }
+  P.tab_scratch = A.take(tab);
   P.tmp_a_bytes = tmp_a * 8;
   P.tmp_b_bytes = tmp_b * 8;
   P.tmp_a = A.take(P.tmp_a_bytes);
@@ -146,14 +195,43 @@ static int grid_for(long long n, int threads = kThreads) {
   return (int)(b < cap ? b : cap);
 }
 
+// Grid of a row-parallel voxel kernel (blocks of 32 x kRowWarps threads).
+static int row_grid(long long nrows) {
+  long long b = (nrows + kRowWarps - 1) / kRowWarps;
+  long long cap = 148LL * 16;
+  if (b < 1) b = 1;
+  return (int)(b < cap ? b : cap);
+}
+static const dim3 kRowBlock(32, kRowWarps);
+
 template <typename T> static T* at_off(void* base, size_t off) {
   return reinterpret_cast<T*>(static_cast<char*>(base) + off);
 }
 
 static size_t iter_smem(int w) { return accumulate_smem(w); }
 
+// x pass of a resize: rows staged in shared memory when the table has a
+// shift-invariant interior and the staged rows fit, else straight from
+// global memory.
+template <typename Tin, typename A, typename Tout>
+static void resample_x(const SITaps& si, const Tin* in, Tout* out, int nrows, int nx_in, int nx_out,
+                       const double* w, const int32_t* idx, int P, int stride, int comp, cudaStream_t s) {
+  const size_t smem = (size_t)kStageWarps * si.s * si.ls * sizeof(A);
+  if (si.hi > si.lo && smem <= 96 * 1024) {
+    auto kern = k_resample_x_staged<Tin, A, Tout>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    long long g = (nrows + kStageWarps - 1) / kStageWarps;
+    if (g > 148LL * 32) g = 148LL * 32;
+    kern<<<(int)g, dim3(32, kStageWarps), smem, s>>>(si, in, out, nrows, nx_in, nx_out, w, idx, P, stride, comp);
+  } else {
+    k_resample_x<Tin, A, Tout><<<row_grid(nrows), kRowBlock, 0, s>>>(si, in, out, 1, nrows, nx_in, nx_out, w, idx, P,
+                                                                     stride, comp);
+  }
+}
+
 // Separable resize of a full-resolution volume to a level:
 // first pass (x or y, by scale order) into tmp, second pass into `out`.
+// A = double with Tin/Tout of any type gives the float64-exact resize.
 template <typename Tin, typename A, typename Tout>
 static void resize_to_level(const Plan& P, const LevelPlan& L, void* ws, const Tin* in, int stride, int comp,
                             A* tmp, Tout* out, cudaStream_t s) {
@@ -162,38 +240,13 @@ static void resize_to_level(const Plan& P, const LevelPlan& L, void* ws, const T
   const double* tyw = at_off<double>(ws, L.ty_w);
   const int32_t* tyi = at_off<int32_t>(ws, L.ty_i);
   if (L.x_first) {
-    long long n1 = (long long)P.nz * P.ny * L.nx;
-    k_resample_x<Tin, A, A><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, P.nx, L.nx, txw, txi, L.tx_taps,
-                                                               stride, comp);
-    k_resample_y<A, A, Tout><<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi,
-                                                                 L.ty_taps, 1, 0);
+    resample_x<Tin, A, A>(L.six, in, tmp, P.nz * P.ny, P.nx, L.nx, txw, txi, L.tx_taps, stride, comp, s);
+    k_resample_y<A, A, Tout><<<row_grid((long long)P.nz * L.ny), kRowBlock, 0, s>>>(
+        L.siy, tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi, L.ty_taps, 1, 0);
   } else {
-    long long n1 = (long long)P.nz * L.ny * P.nx;
-    k_resample_y<Tin, A, A><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, L.ny, P.nx, tyw, tyi, L.ty_taps,
-                                                               stride, comp);
-    k_resample_x<A, A, Tout><<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, L.ny, P.nx, L.nx, txw, txi,
-                                                                 L.tx_taps, 1, 0);
-  }
-}
-
-// the same for a uint8 exclusion mask, float64 throughout (bit-exact with the
-// reference's float64 resize, whose result is thresholded at > 0)
-static void resize_mask_to_level(const Plan& P, const LevelPlan& L, void* ws, const uint8_t* in, double* tmp,
-                                 double* out, cudaStream_t s) {
-  const double* txw = at_off<double>(ws, L.tx_w);
-  const int32_t* txi = at_off<int32_t>(ws, L.tx_i);
-  const double* tyw = at_off<double>(ws, L.ty_w);
-  const int32_t* tyi = at_off<int32_t>(ws, L.ty_i);
-  if (L.x_first) {
-    long long n1 = (long long)P.nz * P.ny * L.nx;
-    k_resample_x<uint8_t, double, double><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, P.nx, L.nx, txw,
-                                                                             txi, L.tx_taps, 1, 0);
-    k_resample_y_d<<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi, L.ty_taps);
-  } else {
-    long long n1 = (long long)P.nz * L.ny * P.nx;
-    k_resample_y<uint8_t, double, double><<<grid_for(n1), kThreads, 0, s>>>(in, tmp, P.nz, P.ny, L.ny, P.nx, tyw,
-                                                                             tyi, L.ty_taps, 1, 0);
-    k_resample_x_d<<<grid_for(L.n), kThreads, 0, s>>>(tmp, out, P.nz, L.ny, P.nx, L.nx, txw, txi, L.tx_taps);
+    k_resample_y<Tin, A, A><<<row_grid((long long)P.nz * L.ny), kRowBlock, 0, s>>>(
+        L.siy, in, tmp, P.nz, P.ny, L.ny, P.nx, tyw, tyi, L.ty_taps, stride, comp);
+    resample_x<A, A, Tout>(L.six, tmp, out, P.nz * L.ny, P.nx, L.nx, txw, txi, L.tx_taps, 1, 0, s);
   }
 }
 
@@ -212,11 +265,12 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
     if (l == 0) {
       // scale 1 on every axis: the resize is an exact copy
       if (!reuse_ref) k_to_level<T, PREC><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
-      k_pack_movg<T, PREC><<<grid_for(L.n), kThreads, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
-      if (mmov_u8) k_u8_to_unit_f<<<grid_for(L.n), kThreads, 0, s>>>(mmov_u8, mmov, L.n);
+      k_pack_movg<T, PREC><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
+      // exclusion bits and the moving mask as float, straight from the uint8 masks
       if (any_mask)
-        k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>(nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8 ? mmov : nullptr,
-                                                        bits, L.nz, L.ny, L.nx, reuse_ref ? 1 : 0);
+        k_mask_bits<uint8_t><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(
+            nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8, mmov_u8 ? mmov : nullptr, bits, L.nz, L.ny, L.nx,
+            reuse_ref ? 1 : 0);
       continue;
     }
     float* tmpf = at_off<float>(ws, P.tmp_a);
@@ -230,19 +284,24 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
       }
     }
     resize_to_level<T, float, float>(P, L, ws, mov, 1, 0, tmpf, levf, s);
-    k_pack_movg<float, PREC><<<grid_for(L.n), kThreads, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
+    k_pack_movg<float, PREC><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(levf, movg, L.nz, L.ny, L.nx);
     double* tmpd = at_off<double>(ws, P.tmp_a);
     double* levd = at_off<double>(ws, P.tmp_b);
     if (mmov_u8) {
-      resize_mask_to_level(P, L, ws, mmov_u8, tmpd, levd, s);
-      k_d_to_f<<<grid_for(L.n), kThreads, 0, s>>>(levd, mmov, L.n);
+      if (same_mask) {
+        resize_to_level<uint8_t, double, double>(P, L, ws, mmov_u8, 1, 0, tmpd, levd, s);
+        k_d_to_f<<<grid_for(L.n), kThreads, 0, s>>>(levd, mmov, L.n);
+      } else {
+        // float64 sums rounded once to float32 on store
+        resize_to_level<uint8_t, double, float>(P, L, ws, mmov_u8, 1, 0, tmpd, mmov, s);
+      }
     }
     // one exclusion mask for both volumes: its resize is already in levd
-    if (mref_u8 && !reuse_ref && !same_mask) resize_mask_to_level(P, L, ws, mref_u8, tmpd, levd, s);
+    if (mref_u8 && !reuse_ref && !same_mask) resize_to_level<uint8_t, double, double>(P, L, ws, mref_u8, 1, 0, tmpd, levd, s);
     if (any_mask)
-      k_mask_bits<<<grid_for(L.n), kThreads, 0, s>>>((mref_u8 && !reuse_ref) ? levd : nullptr, nullptr,
-                                                      mmov_u8 ? mmov : nullptr, bits, L.nz, L.ny, L.nx,
-                                                      reuse_ref ? 1 : 0);
+      k_mask_bits<float><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(
+          (mref_u8 && !reuse_ref) ? levd : nullptr, nullptr, mmov_u8 ? mmov : nullptr, nullptr, bits, L.nz, L.ny, L.nx,
+          reuse_ref ? 1 : 0);
   }
 }
 
@@ -280,27 +339,55 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
   return f;
 }
 
+// Grid of a persistent tile kernel: as many CTAs as stay resident on the
+// device at once (occupancy x SM count), at most one per tile.
+// The resident-CTA count is cached per (kernel, shared memory, device).
+template <typename K>
+static int persistent_grid(K kernel, size_t smem, long long ntiles) {
+  struct Entry { const void* fn; size_t smem; int dev; int ctas; };
+  static std::mutex mu;
+  static std::vector<Entry> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int ctas = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+      if (e.fn == (const void*)kernel && e.smem == smem && e.dev == dev) ctas = e.ctas;
+  }
+  if (ctas == 0) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAccThreads, smem);
+    ctas = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+    std::lock_guard<std::mutex> lock(mu);
+    cache.push_back(Entry{(const void*)kernel, smem, dev, ctas});
+  }
+  return (int)(ntiles < ctas ? (ntiles > 0 ? ntiles : 1) : ctas);
+}
+
 template <int MODE, bool MASK, int PREC>
-static void launch_accumulate1(const IterArgs& a, dim3 grid, size_t smem, cudaStream_t s) {
+static void launch_accumulate1(const IterArgs& a, long long ntiles, size_t smem, cudaStream_t s) {
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_lk_accumulate<MODE, MASK, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = persistent_grid(k_lk_accumulate<MODE, MASK, PREC>, smem, ntiles);
   k_lk_accumulate<MODE, MASK, PREC><<<grid, kAccThreads, smem, s>>>(a);
 }
 
 template <int PREC>
-static void launch_accumulate(int mode, const IterArgs& a, dim3 grid, size_t smem, bool mask, cudaStream_t s) {
+static void launch_accumulate(int mode, const IterArgs& a, long long ntiles, size_t smem, bool mask, cudaStream_t s) {
   switch (mode) {
     case FIELD_CP:
-      mask ? launch_accumulate1<FIELD_CP, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_CP, false, PREC>(a, grid, smem, s);
+      mask ? launch_accumulate1<FIELD_CP, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_CP, false, PREC>(a, ntiles, smem, s);
       break;
     case FIELD_UP:
-      mask ? launch_accumulate1<FIELD_UP, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_UP, false, PREC>(a, grid, smem, s);
+      mask ? launch_accumulate1<FIELD_UP, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_UP, false, PREC>(a, ntiles, smem, s);
       break;
     case FIELD_DENSE:
-      mask ? launch_accumulate1<FIELD_DENSE, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_DENSE, false, PREC>(a, grid, smem, s);
+      mask ? launch_accumulate1<FIELD_DENSE, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_DENSE, false, PREC>(a, ntiles, smem, s);
       break;
     default:
-      mask ? launch_accumulate1<FIELD_ZERO, true, PREC>(a, grid, smem, s) : launch_accumulate1<FIELD_ZERO, false, PREC>(a, grid, smem, s);
+      mask ? launch_accumulate1<FIELD_ZERO, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_ZERO, false, PREC>(a, ntiles, smem, s);
   }
 }
 
@@ -315,7 +402,8 @@ static void level_first(const Plan& P, const LevelPlan& L, void* ws, LKState* st
     const size_t smem = diff_first_smem(P.w);
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_diff_first<MODE0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_diff_first<MODE0><<<dim3(L.nz, L.ntx, L.nty), kAccThreads, smem, s>>>(st, *diff, now);
+    const int grid = persistent_grid(k_diff_first<MODE0>, smem, L.nblk);
+    k_diff_first<MODE0><<<grid, kAccThreads, smem, s>>>(st, *diff, now);
   }
 }
 
@@ -331,8 +419,13 @@ static void first_dispatch(int mode, const Plan& P, const LevelPlan& L, void* ws
 static void build_tables(const Plan& P, void* ws, int* err_flag, cudaStream_t s) {
   for (int l = 0; l < P.levels; ++l) {
     const LevelPlan& L = P.lv[l];
-    k_build_table<<<(L.nx + 127) / 128, 128, 0, s>>>(at_off<double>(ws, L.tx_w), at_off<int32_t>(ws, L.tx_i), P.nx,
-                                                      L.nx, RESIZE_BICUBIC, L.tx_taps);
+    // x tables are stored tap-major ([tap][output]) for the x pass
+    double* rw = at_off<double>(ws, P.tab_scratch);
+    int32_t* ri = reinterpret_cast<int32_t*>(rw + (size_t)L.nx * L.tx_taps);
+    k_build_table<<<(L.nx + 127) / 128, 128, 0, s>>>(rw, ri, P.nx, L.nx, RESIZE_BICUBIC, L.tx_taps);
+    const long long nt = (long long)L.nx * L.tx_taps;
+    k_transpose_table<<<(int)((nt + 255) / 256), 256, 0, s>>>(rw, ri, at_off<double>(ws, L.tx_w),
+                                                              at_off<int32_t>(ws, L.tx_i), L.nx, L.tx_taps);
     k_build_table<<<(L.ny + 127) / 128, 128, 0, s>>>(at_off<double>(ws, L.ty_w), at_off<int32_t>(ws, L.ty_i), P.ny,
                                                       L.ny, RESIZE_BICUBIC, L.ty_taps);
     if (l + 1 < P.levels) {
@@ -354,8 +447,8 @@ static void init_field(const Plan& P, void* ws, const float* init, cudaStream_t 
   if (P.levels == 1) {
     // scale 1: exact copy
     for (int c = 0; c < 3; ++c)
-      k_resample_x<float, double, float><<<grid_for(C.n), kThreads, 0, s>>>(
-          init, comp + (size_t)c * C.n, P.nz, P.ny, P.nx, C.nx, at_off<double>(ws, C.tx_w),
+      k_resample_x<float, double, float><<<row_grid((long long)C.nz * C.ny), kRowBlock, 0, s>>>(
+          C.six, init, comp + (size_t)c * C.n, P.nz, P.ny, P.nx, C.nx, at_off<double>(ws, C.tx_w),
           at_off<int32_t>(ws, C.tx_i), C.tx_taps, 3, c);
   } else {
     for (int c = 0; c < 3; ++c)
@@ -372,9 +465,9 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
   int n = 0;
   const bool stored = P.precision != WR_PREC_F32;   // reduced-precision reference levels need a store pass
   for (int l = 0; l < P.levels; ++l) {
-    n += 2 + (l + 1 < P.levels ? 2 : 0);                       // tables
-    if (l == 0) n += (reuse_ref ? 1 : 2) + (has_mmov ? 1 : 0) + ((has_mmov || has_mref) ? 1 : 0);
-    else n += (reuse_ref ? 3 : (stored ? 6 : 5)) + (has_mmov ? 3 : 0) +
+    n += 3 + (l + 1 < P.levels ? 2 : 0);                       // tables (x table built, then transposed)
+    if (l == 0) n += (reuse_ref ? 1 : 2) + ((has_mmov || has_mref) ? 1 : 0);
+    else n += (reuse_ref ? 3 : (stored ? 6 : 5)) + (has_mmov ? (same_mask ? 3 : 2) : 0) +
               ((has_mref && !reuse_ref && !same_mask) ? 2 : 0) + ((has_mmov || has_mref) ? 1 : 0);
   }
   if (has_init) n += (P.levels == 1 ? 3 : 6) + 1;
@@ -413,8 +506,8 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       // no update can happen at any level: carry dense fields down the pyramid
       FieldSrc f = field_src(P, l, mode0, ws);
       float4* dense = at_off<float4>(ws, L.dense);
-      if (mode0 == FIELD_UP) k_dense_from<FIELD_UP><<<grid_for(L.n), kThreads, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
-      else if (mode0 == FIELD_ZERO) k_dense_from<FIELD_ZERO><<<grid_for(L.n), kThreads, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+      if (mode0 == FIELD_UP) k_dense_from<FIELD_UP><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+      else if (mode0 == FIELD_ZERO) k_dense_from<FIELD_ZERO><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
       mode0 = FIELD_DENSE;
     }
     FieldSrc f0 = field_src(P, l, mode0, ws);
@@ -438,7 +531,6 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     a.ntx = L.ntx;
     a.nty = L.nty;
     a.zratio = L.zratio;
-    const dim3 grid(L.nz, L.ntx, L.nty);
     const size_t smem = iter_smem(P.w);
     const int forced = p->forced_updates[l];
     for (int it = 0; it < P.iter; ++it) {
@@ -446,7 +538,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
       const bool rec = prof && recorded < prof->capacity;
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
-      launch_accumulate<PREC>(mode, a, grid, smem, mask, s);
+      launch_accumulate<PREC>(mode, a, L.nblk, smem, mask, s);
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
       if (PREC == WR_PREC_F32)
@@ -466,10 +558,10 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   const LevelPlan& L0 = P.lv[0];
   if (P.dense_all) {
     FieldSrc f = field_src(P, 0, FIELD_DENSE, ws);
-    k_write_motion<FIELD_DENSE><<<grid_for(L0.n), kThreads, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+    k_write_motion<FIELD_DENSE><<<row_grid((long long)L0.nz * L0.ny), kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   } else {
     FieldSrc f = field_src(P, 0, FIELD_CP, ws);
-    k_write_motion<FIELD_CP><<<grid_for(L0.n), kThreads, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+    k_write_motion<FIELD_CP><<<row_grid((long long)L0.nz * L0.ny), kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   }
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
   if (prof) {
@@ -606,16 +698,18 @@ int wr_warp_trilinear(const WrVolume* src, const float* motion, float* out, void
   if ((rc = check_volume(src, "src"))) return rc;
   if (!motion || !out) return fail(WR_E_NULL, "motion or out is NULL");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  long long n = (long long)src->nz * src->ny * src->nx;
+  const long long rows = (long long)src->nz * src->ny;
+  if (rows >= (1LL << 31)) return fail(WR_E_SHAPE, "src has 2^31 rows or more");
+  const int g = row_grid(rows);
   switch (src->dtype) {
     case WR_U16:
-      k_warp<uint16_t><<<grid_for(n), kThreads, 0, s>>>((const uint16_t*)src->data, motion, out, src->nz, src->ny, src->nx);
+      k_warp<uint16_t><<<g, kRowBlock, 0, s>>>((const uint16_t*)src->data, motion, out, src->nz, src->ny, src->nx);
       break;
     case WR_U8:
-      k_warp<uint8_t><<<grid_for(n), kThreads, 0, s>>>((const uint8_t*)src->data, motion, out, src->nz, src->ny, src->nx);
+      k_warp<uint8_t><<<g, kRowBlock, 0, s>>>((const uint8_t*)src->data, motion, out, src->nz, src->ny, src->nx);
       break;
     default:
-      k_warp<float><<<grid_for(n), kThreads, 0, s>>>((const float*)src->data, motion, out, src->nz, src->ny, src->nx);
+      k_warp<float><<<g, kRowBlock, 0, s>>>((const float*)src->data, motion, out, src->nz, src->ny, src->nx);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "wr_warp_trilinear launch");

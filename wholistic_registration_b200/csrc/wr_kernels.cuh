@@ -37,6 +37,14 @@ template <> __device__ __forceinline__ float load_f<float>(const float* p, size_
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Row-parallel voxel loops: blocks of 32 x kRowWarps threads; warp
+// threadIdx.y of a block takes rows in turn and its lanes take the columns,
+// so that voxel kernels need no per-voxel integer division.
+constexpr int kRowWarps = 8;
+#define WR_FOR_ROWS(nrows, wr_row_) \
+  for (int wr_row_ = blockIdx.x * kRowWarps + threadIdx.y; wr_row_ < (nrows); wr_row_ += gridDim.x * kRowWarps)
+#define WR_FOR_COLS(ncols, wr_col_) for (int wr_col_ = threadIdx.x; wr_col_ < (ncols); wr_col_ += 32)
+
 // f32 coordinate -> (lower tap, fraction); huge values are pinned so the
 // integer conversion stays defined (the taps are clamped anyway).
 __device__ __forceinline__ void split_coord(float c, int& i0, float& t) {
@@ -110,6 +118,17 @@ __global__ void k_build_table(double* w, int32_t* idx, int in_len, int out_len, 
   resize_row(in_len, out_len, method, k, w + (size_t)k * P, idx + (size_t)k * P);
 }
 
+// [n][P] -> [P][n]: in the x pass the lanes of a warp hold consecutive
+// outputs and then read consecutive weights and indexes.
+__global__ void k_transpose_table(const double* __restrict__ w, const int32_t* __restrict__ idx, double* wt,
+                                  int32_t* it, int n, int P) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)n * P) return;
+  const int k = (int)(i / P), t = (int)(i - (long long)k * P);
+  wt[(size_t)t * n + k] = w[i];
+  it[(size_t)t * n + k] = idx[i];
+}
+
 // Bilinear up-sampling table compacted to the (at most two) taps with nonzero
 // weight.  Dropping exact-zero terms does not change the weighted sum.
 __global__ void k_build_up_table(float* w2, int32_t* i2, int in_len, int out_len, int* err_flag) {
@@ -139,92 +158,120 @@ __global__ void k_build_up_table(float* w2, int32_t* i2, int in_len, int out_len
 // ---------------------------------------------------------------------------
 
 // Float64 accumulation without contraction reproduces the reference's
-// float64 products and tap-order sums exactly; float32 uses FMA.
+// float64 products and tap-order sums exactly; float32 uses FMA with the
+// weight rounded to float32.
 template <typename A> struct Acc;
 template <> struct Acc<double> {
   static __device__ __forceinline__ double madd(double acc, double w, double v) {
     return __dadd_rn(acc, __dmul_rn(w, v));
   }
+  static __device__ __forceinline__ double si_weight(const SITaps& si, int t) { return si.w[t]; }
 };
 template <> struct Acc<float> {
   static __device__ __forceinline__ float madd(float acc, double w, float v) {
     return fmaf((float)w, v, acc);
   }
+  static __device__ __forceinline__ float madd(float acc, float w, float v) { return fmaf(w, v, acc); }
+  static __device__ __forceinline__ float si_weight(const SITaps& si, int t) { return si.wf[t]; }
 };
 
-// out[z][y][xo] = sum_t w[xo][t] * in[z][y][idx[xo][t]]   (stride/comp select
-// one component of an interleaved input)
+// Separable resize passes.  Outputs inside the table's shift-invariant
+// interior (SITaps) read their taps at s*o + c0 + t with the weights held in
+// the kernel parameters; the few outputs near the edges (reflected taps) read
+// the table, x tables tap-major ([tap][output]), y tables output-major.
+// stride/comp select one component of an interleaved input.
+
+// out[z][y][xo] = sum_t w[t][xo] * in[z][y][idx[t][xo]]
 template <typename Tin, typename A, typename Tout>
-__global__ void k_resample_x(const Tin* __restrict__ in, Tout* __restrict__ out, int nz, int ny,
-                             int nx_in, int nx_out, const double* __restrict__ w,
+__global__ void k_resample_x(const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out,
+                             int nz, int ny, int nx_in, int nx_out, const double* __restrict__ w,
                              const int32_t* __restrict__ idx, int P, int stride, int comp) {
-  long long total = (long long)nz * ny * nx_out;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
-       o += (long long)gridDim.x * blockDim.x) {
-    int xo = (int)(o % nx_out);
-    long long row = o / nx_out;
+  WR_FOR_ROWS(nz * ny, row) {
     const Tin* src = in + (size_t)row * nx_in * stride + comp;
-    const double* wr = w + (size_t)xo * P;
-    const int32_t* ir = idx + (size_t)xo * P;
-    A acc = 0;
-    for (int t = 0; t < P; ++t) acc = Acc<A>::madd(acc, wr[t], (A)__ldg(src + (size_t)ir[t] * stride));
-    out[o] = (Tout)acc;
+    Tout* dst = out + (size_t)row * nx_out;
+    WR_FOR_COLS(nx_out, xo) {
+      A acc = 0;
+      if (xo >= si.lo && xo < si.hi) {
+        const Tin* q = src + (size_t)(si.s * xo + si.c0) * stride;
+#pragma unroll 4
+        for (int t = 0; t < si.P; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), (A)__ldg(q + (size_t)t * stride));
+      } else {
+        for (int t = 0; t < P; ++t)
+          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo),
+                             (A)__ldg(src + (size_t)__ldg(idx + (size_t)t * nx_out + xo) * stride));
+      }
+      dst[xo] = (Tout)acc;
+    }
   }
 }
 
+// The x pass with each row staged in shared memory: one warp per row, the
+// row read once with coalesced loads and stored in polyphase order, interior
+// outputs read their taps from shared memory without bank conflicts, edge
+// outputs from the table.  Blocks of 32 x kStageWarps threads; dynamic shared
+// memory kStageWarps * s * ls elements of A.
+constexpr int kStageWarps = 4;
 template <typename Tin, typename A, typename Tout>
-__global__ void k_resample_y(const Tin* __restrict__ in, Tout* __restrict__ out, int nz, int ny_in,
-                             int ny_out, int nx, const double* __restrict__ w,
+__global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_staged(
+    const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out, int nrows, int nx_in,
+    int nx_out, const double* __restrict__ w, const int32_t* __restrict__ idx, int P, int stride, int comp) {
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  A* buf = reinterpret_cast<A*>(stage_raw) + (size_t)threadIdx.y * si.s * si.ls;
+  const int lane = threadIdx.x;
+  for (int row = blockIdx.x * kStageWarps + threadIdx.y; row < nrows; row += gridDim.x * kStageWarps) {
+    const Tin* src = in + (size_t)row * nx_in * stride + comp;
+    for (int q = lane; q < si.ls; q += 32)
+      for (int ph = 0; ph < si.s; ++ph) {
+        const int e = q * si.s + ph;
+        if (e < nx_in) buf[ph * si.ls + q] = (A)__ldg(src + (size_t)e * stride);
+      }
+    __syncwarp();
+    Tout* dst = out + (size_t)row * nx_out;
+    for (int xo = lane; xo < nx_out; xo += 32) {
+      A acc = 0;
+      if (xo >= si.lo && xo < si.hi) {
+#pragma unroll 4
+        for (int t = 0; t < si.P; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), buf[si.off[t] + xo]);
+      } else {
+        for (int t = 0; t < P; ++t)
+          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo),
+                             (A)__ldg(src + (size_t)__ldg(idx + (size_t)t * nx_out + xo) * stride));
+      }
+      dst[xo] = (Tout)acc;
+    }
+    __syncwarp();
+  }
+}
+
+// out[z][yo][x] = sum_t w[yo][t] * in[z][idx[yo][t]][x]
+template <typename Tin, typename A, typename Tout>
+__global__ void k_resample_y(const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out,
+                             int nz, int ny_in, int ny_out, int nx, const double* __restrict__ w,
                              const int32_t* __restrict__ idx, int P, int stride, int comp) {
-  long long total = (long long)nz * ny_out * nx;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
-       o += (long long)gridDim.x * blockDim.x) {
-    int x = (int)(o % nx);
-    long long rest = o / nx;
-    int yo = (int)(rest % ny_out);
-    int z = (int)(rest / ny_out);
-    const Tin* src = in + (size_t)z * ny_in * nx * stride + (size_t)x * stride + comp;
-    const double* wr = w + (size_t)yo * P;
-    const int32_t* ir = idx + (size_t)yo * P;
-    A acc = 0;
-    for (int t = 0; t < P; ++t)
-      acc = Acc<A>::madd(acc, wr[t], (A)__ldg(src + (size_t)ir[t] * nx * stride));
-    out[o] = (Tout)acc;
-  }
-}
-
-// double-exact variant of the y pass reading float64 input
-__global__ void k_resample_y_d(const double* __restrict__ in, double* __restrict__ out, int nz,
-                               int ny_in, int ny_out, int nx, const double* __restrict__ w,
-                               const int32_t* __restrict__ idx, int P) {
-  long long total = (long long)nz * ny_out * nx;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
-       o += (long long)gridDim.x * blockDim.x) {
-    int x = (int)(o % nx);
-    long long rest = o / nx;
-    int yo = (int)(rest % ny_out);
-    int z = (int)(rest / ny_out);
-    const double* src = in + (size_t)z * ny_in * nx + x;
-    double acc = 0.0;
-    for (int t = 0; t < P; ++t)
-      acc = __dadd_rn(acc, __dmul_rn(w[(size_t)yo * P + t], src[(size_t)idx[(size_t)yo * P + t] * nx]));
-    out[o] = acc;
-  }
-}
-
-__global__ void k_resample_x_d(const double* __restrict__ in, double* __restrict__ out, int nz,
-                               int ny, int nx_in, int nx_out, const double* __restrict__ w,
-                               const int32_t* __restrict__ idx, int P) {
-  long long total = (long long)nz * ny * nx_out;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
-       o += (long long)gridDim.x * blockDim.x) {
-    int xo = (int)(o % nx_out);
-    long long row = o / nx_out;
-    const double* src = in + (size_t)row * nx_in;
-    double acc = 0.0;
-    for (int t = 0; t < P; ++t)
-      acc = __dadd_rn(acc, __dmul_rn(w[(size_t)xo * P + t], src[idx[(size_t)xo * P + t]]));
-    out[o] = acc;
+  const size_t rs = (size_t)nx * stride;   // input row stride
+  WR_FOR_ROWS(nz * ny_out, row) {
+    const int z = row / ny_out, yo = row - z * ny_out;
+    const Tin* plane = in + (size_t)z * ny_in * rs + comp;
+    Tout* dst = out + (size_t)row * nx;
+    if (yo >= si.lo && yo < si.hi) {
+      const Tin* r0 = plane + (size_t)(si.s * yo + si.c0) * rs;
+      WR_FOR_COLS(nx, x) {
+        const Tin* q = r0 + (size_t)x * stride;
+        A acc = 0;
+#pragma unroll 4
+        for (int t = 0; t < si.P; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), (A)__ldg(q + (size_t)t * rs));
+        dst[x] = (Tout)acc;
+      }
+    } else {
+      const double* wr = w + (size_t)yo * P;
+      const int32_t* ir = idx + (size_t)yo * P;
+      WR_FOR_COLS(nx, x) {
+        const Tin* q = plane + (size_t)x * stride;
+        A acc = 0;
+        for (int t = 0; t < P; ++t) acc = Acc<A>::madd(acc, __ldg(wr + t), (A)__ldg(q + (size_t)__ldg(ir + t) * rs));
+        dst[x] = (Tout)acc;
+      }
+    }
   }
 }
 
@@ -263,56 +310,88 @@ __global__ void k_store_level(const float* __restrict__ in, typename Store<PREC>
 }
 
 // movg[p] = (m, Gx, Gy, Gz) with G = half the clamped central difference.
+// Each warp takes 32 columns of a row; the x neighbours come from the
+// adjacent lanes.
 template <typename T, int PREC>
 __global__ void k_pack_movg(const T* __restrict__ m, typename Store<PREC>::V4* __restrict__ movg, int nz, int ny, int nx) {
-  long long n = (long long)nz * ny * nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    int x = (int)(i % nx);
-    long long rest = i / nx;
-    int y = (int)(rest % ny);
-    int z = (int)(rest / ny);
-    size_t sy = nx, sz = (size_t)nx * ny;
-    float c = load_f<T>(m, i);
-    float xp = load_f<T>(m, i - x + min(x + 1, nx - 1));
-    float xm = load_f<T>(m, i - x + max(x - 1, 0));
-    float yp = load_f<T>(m, i + (size_t)(min(y + 1, ny - 1) - y) * sy);
-    float ym = load_f<T>(m, i - (size_t)(y - max(y - 1, 0)) * sy);
-    float zp = load_f<T>(m, i + (size_t)(min(z + 1, nz - 1) - z) * sz);
-    float zm = load_f<T>(m, i - (size_t)(z - max(z - 1, 0)) * sz);
-    movg[i] = Store<PREC>::pack4(make_float4(c, 0.5f * (xp - xm), 0.5f * (yp - ym), 0.5f * (zp - zm)));
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const int lane = threadIdx.x;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const size_t base = (size_t)row * nx;
+    const size_t dyp = (size_t)(min(y + 1, ny - 1) - y) * sy, dym = (size_t)(y - max(y - 1, 0)) * sy;
+    const size_t dzp = (size_t)(min(z + 1, nz - 1) - z) * sz, dzm = (size_t)(z - max(z - 1, 0)) * sz;
+    for (int x0 = 0; x0 < nx; x0 += 32) {
+      const int x = x0 + lane, xc = min(x, nx - 1);
+      const size_t i = base + xc;
+      const float c = load_f<T>(m, i);
+      float xm = __shfl_up_sync(0xffffffffu, c, 1), xp = __shfl_down_sync(0xffffffffu, c, 1);
+      if (lane == 0) xm = load_f<T>(m, base + max(xc - 1, 0));
+      if (lane == 31 || x >= nx - 1) xp = load_f<T>(m, base + min(xc + 1, nx - 1));
+      if (x < nx) {
+        const float yp = load_f<T>(m, i + dyp), ym = load_f<T>(m, i - dym);
+        const float zp = load_f<T>(m, i + dzp), zm = load_f<T>(m, i - dzm);
+        movg[i] = Store<PREC>::pack4(make_float4(c, 0.5f * (xp - xm), 0.5f * (yp - ym), 0.5f * (zp - zm)));
+      }
+    }
   }
 }
 
 // mask bits of a level: bit0 = resized mask_ref > 0; bits 1-2 = class of the
 // trilinear cell whose lower corner is this voxel in the resized mask_mov:
 // 0 = all 8 corners <= 0, 1 = all > 0, 2 = mixed (needs the exact sum).
+template <typename TM> __device__ __forceinline__ bool mask_on(const TM* m, size_t i);
+template <> __device__ __forceinline__ bool mask_on<float>(const float* m, size_t i) { return __ldg(m + i) > 0.f; }
+template <> __device__ __forceinline__ bool mask_on<uint8_t>(const uint8_t* m, size_t i) { return __ldg(m + i) != 0; }
+
+// Exclusion bits of a level: bit 0 = reference mask > 0 (from its float64
+// resize, its uint8 values at full resolution, or kept), bits 1-2 = class
+// of the moving mask's trilinear cell at each voxel (corners x..x+1,
+// y..y+1, z..z+1, edge-clamped): 0 no corner > 0, 1 all, 2 mixed.  Each warp
+// takes 32 columns of a row; the x+1 corners come from the next lane's
+// ballot bit.  mmov_f (optional) receives the moving mask as float (the
+// full-resolution level, where TM is uint8).
+template <typename TM>
 __global__ void k_mask_bits(const double* __restrict__ mref_d, const uint8_t* __restrict__ mref_u8,
-                            const float* __restrict__ mmov, uint8_t* __restrict__ bits, int nz,
-                            int ny, int nx, int keep_ref_bit) {
-  long long n = (long long)nz * ny * nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    int x = (int)(i % nx);
-    long long rest = i / nx;
-    int y = (int)(rest % ny);
-    int z = (int)(rest / ny);
-    uint8_t b = keep_ref_bit ? (bits[i] & 1) : 0;
-    if (mref_d) b |= (mref_d[i] > 0.0) ? 1 : 0;
-    else if (mref_u8) b |= mref_u8[i] ? 1 : 0;
-    if (mmov) {
-      int pos = 0, tot = 0;
-      for (int dz = 0; dz < 2; ++dz)
-        for (int dy = 0; dy < 2; ++dy)
-          for (int dx = 0; dx < 2; ++dx) {
-            int xx = min(x + dx, nx - 1), yy = min(y + dy, ny - 1), zz = min(z + dz, nz - 1);
-            pos += mmov[((size_t)zz * ny + yy) * nx + xx] > 0.f;
-            ++tot;
-          }
-      int code = pos == 0 ? 0 : (pos == tot ? 1 : 2);
-      b |= (uint8_t)(code << 1);
+                            const TM* __restrict__ mmov, float* __restrict__ mmov_f, uint8_t* __restrict__ bits,
+                            int nz, int ny, int nx, int keep_ref_bit) {
+  const int lane = threadIdx.x;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const size_t base = (size_t)row * nx;
+    const size_t dy = (size_t)(min(y + 1, ny - 1) - y) * nx, dz = (size_t)(min(z + 1, nz - 1) - z) * nx * ny;
+    for (int x0 = 0; x0 < nx; x0 += 32) {
+      const int x = x0 + lane, xc = min(x, nx - 1);
+      const size_t i = base + xc;
+      uint8_t b = 0;
+      if (x < nx) {
+        b = keep_ref_bit ? (bits[i] & 1) : 0;
+        if (mref_d) b |= (mref_d[i] > 0.0) ? 1 : 0;
+        else if (mref_u8) b |= mref_u8[i] ? 1 : 0;
+      }
+      if (mmov) {
+        const bool f0 = mask_on<TM>(mmov, i), f1 = mask_on<TM>(mmov, i + dy);
+        const bool f2 = mask_on<TM>(mmov, i + dz), f3 = mask_on<TM>(mmov, i + dz + dy);
+        const unsigned b0 = __ballot_sync(0xffffffffu, f0), b1 = __ballot_sync(0xffffffffu, f1);
+        const unsigned b2 = __ballot_sync(0xffffffffu, f2), b3 = __ballot_sync(0xffffffffu, f3);
+        bool n0, n1, n2, n3;   // corners at column min(x + 1, nx - 1)
+        if (x >= nx - 1) {
+          n0 = f0; n1 = f1; n2 = f2; n3 = f3;
+        } else if (lane == 31) {
+          const size_t j = base + x + 1;
+          n0 = mask_on<TM>(mmov, j); n1 = mask_on<TM>(mmov, j + dy);
+          n2 = mask_on<TM>(mmov, j + dz); n3 = mask_on<TM>(mmov, j + dz + dy);
+        } else {
+          n0 = (b0 >> (lane + 1)) & 1u; n1 = (b1 >> (lane + 1)) & 1u;
+          n2 = (b2 >> (lane + 1)) & 1u; n3 = (b3 >> (lane + 1)) & 1u;
+        }
+        const bool any = f0 | f1 | f2 | f3 | n0 | n1 | n2 | n3;
+        const bool all = f0 & f1 & f2 & f3 & n0 & n1 & n2 & n3;
+        b |= (uint8_t)((any ? (all ? 1 : 2) : 0) << 1);
+        if (mmov_f && x < nx) mmov_f[i] = f0 ? 1.f : 0.f;
+      }
+      if (x < nx) bits[i] = b;
     }
-    bits[i] = b;
   }
 }
 
@@ -320,12 +399,6 @@ __global__ void k_d_to_f(const double* __restrict__ in, float* __restrict__ out,
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     out[i] = (float)in[i];
-}
-
-__global__ void k_u8_to_unit_f(const uint8_t* __restrict__ in, float* __restrict__ out, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = in[i] ? 1.f : 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -588,11 +661,17 @@ constexpr int kTileCP = 4;   // CP rows / columns held per tile
 // same separable form holds over the coarser level's CPs: the bilinear
 // up-sampling table composed with that level's CP interpolation, x and y
 // components doubled.
+//
+// ax is stored CP row by CP row ([kTileCP][ld]) so that the lanes of a warp,
+// which hold consecutive columns, read consecutive float4s (no shared-memory
+// bank conflicts).  In CP mode a row of the tile touches at most two CP rows:
+// wy[hy] then holds their weights and row indexes (w0, w1, j0, j1); in UP
+// mode it holds the four row weights.
 struct TileField {
-  float4* ax;   // [hw][kTileCP]
+  float4* ax;   // [kTileCP][ld]
   float4* wy;   // [hh]
   float4* cpt;  // [kTileCP][kTileCP]
-  int generic;  // the tile's CP span exceeds kTileCP: evaluate per voxel
+  int ld;       // row length of ax (w + 2)
 };
 
 __host__ __device__ inline size_t tile_field_smem(int w) {
@@ -622,7 +701,7 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
       const int i0 = c.x - cx0, i1 = c.y - cx0;
       for (int j = 0; j < kTileCP; ++j) {
         const float4 p = tf.cpt[j * kTileCP + min(i0, kTileCP - 1)], q = tf.cpt[j * kTileCP + min(i1, kTileCP - 1)];
-        tf.ax[threadIdx.x * kTileCP + j] =
+        tf.ax[j * tf.ld + threadIdx.x] =
             make_float4(fmaf(t, q.x - p.x, p.x), fmaf(t, q.y - p.y, p.y), fmaf(t, q.z - p.z, p.z), 0.f);
       }
       if (i1 >= kTileCP) atomicOr(generic_flag, 1);
@@ -631,12 +710,11 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
       const int hy = threadIdx.x - 128;
       const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
       const int2 c = cp_factor(gy, r, w, g.ncy, t);
-      float wv[kTileCP] = {0.f, 0.f, 0.f, 0.f};
-      const int j0 = c.x - cy0, j1 = c.y - cy0;
-      if (j1 >= kTileCP) atomicOr(generic_flag, 1);
-      wv[min(j0, kTileCP - 1)] += 1.f - t;
-      wv[min(j1, kTileCP - 1)] += t;
-      tf.wy[hy] = make_float4(wv[0], wv[1], wv[2], wv[3]);
+      const int j0 = min(c.x - cy0, kTileCP - 1), j1 = min(c.y - cy0, kTileCP - 1);
+      if (c.y - cy0 >= kTileCP) atomicOr(generic_flag, 1);
+      float w0 = 1.f - t, w1 = t;
+      if (j0 == j1) { w0 = w0 + w1; w1 = 0.f; }   // both weights on one row (edge clamp)
+      tf.wy[hy] = make_float4(w0, w1, __int_as_float(j0), __int_as_float(j1));
     }
   } else if (MODE == FIELD_UP) {
     const UpView& u = f.up;
@@ -676,7 +754,7 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
         }
         a.x *= 2.f;
         a.y *= 2.f;
-        tf.ax[threadIdx.x * kTileCP + j] = a;
+        tf.ax[j * tf.ld + threadIdx.x] = a;
       }
     }
     if (threadIdx.x >= 128 && threadIdx.x < 128 + hh) {
@@ -703,13 +781,18 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
 template <int MODE>
 __device__ __forceinline__ float3 tile_motion(const TileField& tf, bool generic, const FieldSrc& f, int hx, int hy,
                                               int gx, int gy, int z) {
-  if ((MODE == FIELD_CP || MODE == FIELD_UP) && !generic) {
+  if (MODE == FIELD_CP && !generic) {
     const float4 wv = tf.wy[hy];
-    const float4* a = tf.ax + hx * kTileCP;
-    const float4 a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3];
-    return make_float3(wv.x * a0.x + wv.y * a1.x + wv.z * a2.x + wv.w * a3.x,
-                       wv.x * a0.y + wv.y * a1.y + wv.z * a2.y + wv.w * a3.y,
-                       wv.x * a0.z + wv.y * a1.z + wv.z * a2.z + wv.w * a3.z);
+    const float4 p = tf.ax[__float_as_int(wv.z) * tf.ld + hx], q = tf.ax[__float_as_int(wv.w) * tf.ld + hx];
+    return make_float3(fmaf(wv.y, q.x, __fmul_rn(wv.x, p.x)), fmaf(wv.y, q.y, __fmul_rn(wv.x, p.y)),
+                       fmaf(wv.y, q.z, __fmul_rn(wv.x, p.z)));
+  }
+  if (MODE == FIELD_UP && !generic) {
+    const float4 wv = tf.wy[hy];
+    const float4 a0 = tf.ax[hx], a1 = tf.ax[tf.ld + hx], a2 = tf.ax[2 * tf.ld + hx], a3 = tf.ax[3 * tf.ld + hx];
+    return make_float3(fmaf(wv.w, a3.x, fmaf(wv.z, a2.x, fmaf(wv.y, a1.x, __fmul_rn(wv.x, a0.x)))),
+                       fmaf(wv.w, a3.y, fmaf(wv.z, a2.y, fmaf(wv.y, a1.y, __fmul_rn(wv.x, a0.y)))),
+                       fmaf(wv.w, a3.z, fmaf(wv.z, a2.z, fmaf(wv.y, a1.z, __fmul_rn(wv.x, a0.z)))));
   }
   return eval_field<MODE>(f, gx, gy, z);
 }
@@ -725,13 +808,12 @@ __host__ __device__ inline size_t accumulate_smem(int w) {
 
 // Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588).
 //
-// One CTA per (z slice, window or leftover tile).  Phase 1 takes every voxel
-// of the tile plus a one-voxel halo as independent work: the motion from the
-// tile's CP factors (shared memory), the warped moving level and its
-// gradients from one set of 8 float4 corners (m, Gx, Gy, Gz share the
-// trilinear weights; the upper-x corners come from the next lane when it
-// sampled the same rows), It_raw = ref - warped, and for tile voxels the
-// clipped gradients and the exclusion mask.  Phase 2 smooths It with the 3x3
+// Persistent CTAs take (z slice, window or leftover tile) tiles in turn.  For
+// each tile, phase 1 takes every voxel of the tile plus a one-voxel halo as
+// independent work: the motion from the tile's CP factors (shared memory),
+// the warped moving level and its gradients from one set of 8 float4 corners
+// (m, Gx, Gy, Gz share the trilinear weights), It_raw = ref - warped, and for
+// tile voxels the clipped gradients and the exclusion mask.  Phase 2 smooths It with the 3x3
 // box (edge-replicated), applies the mask and accumulates It^2 and the nine
 // gradient products; a window hanging over the volume edge counts the edge
 // voxel once per replicated position (mode="nearest" of
@@ -740,187 +822,194 @@ __host__ __device__ inline size_t accumulate_smem(int w) {
 template <int MODE, bool MASK, int PREC>
 __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
   typedef Store<PREC> S;
-  const int active = *(volatile const int*)&a.st->active;   // checked after the tile loads are in flight
+  // a level that has stopped leaves its remaining iteration launches empty
+  if (!*(volatile const int*)&a.st->active) return;
   extern __shared__ float4 smem4[];
   const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
   const int w = a.w;
   const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
-  const int z = blockIdx.x, tx = blockIdx.y, ty = blockIdx.z;
-  const bool window = tx < ncx && ty < ncy;
-  const int x0 = tx * w, y0 = ty * w;
-  const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
-  const int hw = wx + 2, hh = wy + 2;
   float4* gsm = smem4;                                    // w*w
   float* it_raw = reinterpret_cast<float*>(gsm + w * w);  // (w+2)^2, padded to 4
   TileField tf;
   tf.ax = reinterpret_cast<float4*>(it_raw + (((w + 2) * (w + 2) + 3) & ~3));
   tf.wy = tf.ax + (w + 2) * kTileCP;
   tf.cpt = tf.wy + (w + 2);
+  tf.ld = w + 2;
   int* flags = reinterpret_cast<int*>(tf.cpt + kTileCP * kTileCP);
   float* red = reinterpret_cast<float*>(flags + 4);       // 8 warps * 12
-  build_tile_field<MODE>(tf, flags, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
-  if (!active) return;
-  const bool generic = flags[0] != 0;
+  const int ntiles = nz * a.ntx * a.nty;
+  // persistent CTAs walk the tiles z fastest: tile = (ty * ntx + tx) * nz + z
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int z = tile % nz, txy = tile / nz;
+    const int ty = txy / a.ntx, tx = txy - ty * a.ntx;
+    const bool window = tx < ncx && ty < ncy;
+    const int x0 = tx * w, y0 = ty * w;
+    const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
+    const int hw = wx + 2, hh = wy + 2;
+    build_tile_field<MODE>(tf, flags, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
+    const bool generic = flags[0] != 0;
 
-  const typename S::V4* __restrict__ G = static_cast<const typename S::V4*>(a.mov.g);
-  const typename S::V1* __restrict__ R = static_cast<const typename S::V1*>(a.ref);
-  const uint32_t plane = (uint32_t)nx * (uint32_t)ny;
-  const uint32_t zoff = (uint32_t)z * plane;
-  const int total = hh * hw;
-  const float fz_base = (float)z;
-  int hy = threadIdx.x / hw, hx = threadIdx.x - hy * hw;
-  const int step_y = kAccThreads / hw, step_x = kAccThreads - step_y * hw;
-  for (int h = threadIdx.x; h < total; h += kAccThreads) {
-    const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
-    const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
-    const float3 m = tile_motion<MODE>(tf, generic, a.field, hx, hy, gx, gy, z);
-    const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = fz_base + m.z;
-    int ix0, iy0, iz0;
-    float fx, fy, fz;
-    split_coord(cx, ix0, fx);
-    split_coord(cy, iy0, fy);
-    split_coord(cz, iz0, fz);
-    const int xa = clampi(ix0, 0, nx - 1), ya = clampi(iy0, 0, ny - 1), za = clampi(iz0, 0, nz - 1);
-    // taps one step up, or the same tap when clamped at the upper face
-    const bool sx = ix0 >= 0 && ix0 < nx - 1, sy = iy0 >= 0 && iy0 < ny - 1, sz = iz0 >= 0 && iz0 < nz - 1;
-    const uint32_t i000 = (uint32_t)za * plane + (uint32_t)ya * nx + (uint32_t)xa;
-    const typename S::V4* p00 = G + i000;
-    const typename S::V4* p01 = sy ? p00 + nx : p00;
-    const typename S::V4* p10 = sz ? p00 + plane : p00;
-    const typename S::V4* p11 = sy ? p10 + nx : p10;
-    float4 c000, c001, c010, c011, c100, c101, c110, c111;
-    c000 = S::load4(p00); c010 = S::load4(p01); c100 = S::load4(p10); c110 = S::load4(p11);
-    if (sx) {
-      c001 = S::load4(p00 + 1); c011 = S::load4(p01 + 1); c101 = S::load4(p10 + 1); c111 = S::load4(p11 + 1);
-    } else {
-      c001 = c000; c011 = c010; c101 = c100; c111 = c110;
-    }
-    // trilinear on (m, Gx) and (Gy, Gz) pairs with paired FP32 FMAs
-    const float2 tx2 = make_float2(fx, fx), ty2 = make_float2(fy, fy), tz2 = make_float2(fz, fz);
-    const float2 ntx2 = make_float2(-fx, -fx), nty2 = make_float2(-fy, -fy), ntz2 = make_float2(-fz, -fz);
-#define WR_LERP2(a, b, t, nt) __ffma2_rn(t, b, __ffma2_rn(nt, a, a))
-    const float2 lo00 = WR_LERP2(make_float2(c000.x, c000.y), make_float2(c001.x, c001.y), tx2, ntx2);
-    const float2 lo01 = WR_LERP2(make_float2(c010.x, c010.y), make_float2(c011.x, c011.y), tx2, ntx2);
-    const float2 lo10 = WR_LERP2(make_float2(c100.x, c100.y), make_float2(c101.x, c101.y), tx2, ntx2);
-    const float2 lo11 = WR_LERP2(make_float2(c110.x, c110.y), make_float2(c111.x, c111.y), tx2, ntx2);
-    const float2 lo = WR_LERP2(WR_LERP2(lo00, lo01, ty2, nty2), WR_LERP2(lo10, lo11, ty2, nty2), tz2, ntz2);
-    const uint32_t p = zoff + (uint32_t)gy * nx + gx;
-    it_raw[h] = S::load1(R + p) - lo.x;
-    if (hx >= 1 && hx <= wx && hy >= 1 && hy <= wy) {
-      const float2 hi00 = WR_LERP2(make_float2(c000.z, c000.w), make_float2(c001.z, c001.w), tx2, ntx2);
-      const float2 hi01 = WR_LERP2(make_float2(c010.z, c010.w), make_float2(c011.z, c011.w), tx2, ntx2);
-      const float2 hi10 = WR_LERP2(make_float2(c100.z, c100.w), make_float2(c101.z, c101.w), tx2, ntx2);
-      const float2 hi11 = WR_LERP2(make_float2(c110.z, c110.w), make_float2(c111.z, c111.w), tx2, ntx2);
-      const float2 hi = WR_LERP2(WR_LERP2(hi00, hi01, ty2, nty2), WR_LERP2(hi10, hi11, ty2, nty2), tz2, ntz2);
-      float gxv = lo.y, gyv = hi.x, gzv = hi.y;
-      if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 0);
-      if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 1);
-      if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 2);
-      float excl = 0.f;
-      if (MASK) {
-        bool ex = (__ldg(a.mbits + p) & 1) != 0;
-        if (!ex && a.mmov) {
-          // the cell code covers exactly this sample's corners when the lower
-          // taps were not clamped
-          int code = 2;
-          if (xa == ix0 && ya == iy0 && za == iz0) code = (__ldg(a.mbits + i000) >> 1) & 3;
-          if (code == 1) ex = true;
-          else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
-        }
-        excl = ex ? 1.f : 0.f;
+    const typename S::V4* __restrict__ G = static_cast<const typename S::V4*>(a.mov.g);
+    const typename S::V1* __restrict__ R = static_cast<const typename S::V1*>(a.ref);
+    const uint32_t plane = (uint32_t)nx * (uint32_t)ny;
+    const uint32_t zoff = (uint32_t)z * plane;
+    const int total = hh * hw;
+    const float fz_base = (float)z;
+    int hy = threadIdx.x / hw, hx = threadIdx.x - hy * hw;
+    const int step_y = kAccThreads / hw, step_x = kAccThreads - step_y * hw;
+    for (int h = threadIdx.x; h < total; h += kAccThreads) {
+      const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
+      const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
+      const float3 m = tile_motion<MODE>(tf, generic, a.field, hx, hy, gx, gy, z);
+      const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = fz_base + m.z;
+      int ix0, iy0, iz0;
+      float fx, fy, fz;
+      split_coord(cx, ix0, fx);
+      split_coord(cy, iy0, fy);
+      split_coord(cz, iz0, fz);
+      const int xa = clampi(ix0, 0, nx - 1), ya = clampi(iy0, 0, ny - 1), za = clampi(iz0, 0, nz - 1);
+      // taps one step up, or the same tap when clamped at the upper face
+      const bool sx = ix0 >= 0 && ix0 < nx - 1, sy = iy0 >= 0 && iy0 < ny - 1, sz = iz0 >= 0 && iz0 < nz - 1;
+      const uint32_t i000 = (uint32_t)za * plane + (uint32_t)ya * nx + (uint32_t)xa;
+      const typename S::V4* p00 = G + i000;
+      const typename S::V4* p01 = sy ? p00 + nx : p00;
+      const typename S::V4* p10 = sz ? p00 + plane : p00;
+      const typename S::V4* p11 = sy ? p10 + nx : p10;
+      float4 c000, c001, c010, c011, c100, c101, c110, c111;
+      c000 = S::load4(p00); c010 = S::load4(p01); c100 = S::load4(p10); c110 = S::load4(p11);
+      if (sx) {
+        c001 = S::load4(p00 + 1); c011 = S::load4(p01 + 1); c101 = S::load4(p10 + 1); c111 = S::load4(p11 + 1);
+      } else {
+        c001 = c000; c011 = c010; c101 = c100; c111 = c110;
       }
-      gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
+      // trilinear on (m, Gx) and (Gy, Gz) pairs with paired FP32 FMAs
+      const float2 tx2 = make_float2(fx, fx), ty2 = make_float2(fy, fy), tz2 = make_float2(fz, fz);
+      const float2 ntx2 = make_float2(-fx, -fx), nty2 = make_float2(-fy, -fy), ntz2 = make_float2(-fz, -fz);
+  #define WR_LERP2(a, b, t, nt) __ffma2_rn(t, b, __ffma2_rn(nt, a, a))
+      const float2 lo00 = WR_LERP2(make_float2(c000.x, c000.y), make_float2(c001.x, c001.y), tx2, ntx2);
+      const float2 lo01 = WR_LERP2(make_float2(c010.x, c010.y), make_float2(c011.x, c011.y), tx2, ntx2);
+      const float2 lo10 = WR_LERP2(make_float2(c100.x, c100.y), make_float2(c101.x, c101.y), tx2, ntx2);
+      const float2 lo11 = WR_LERP2(make_float2(c110.x, c110.y), make_float2(c111.x, c111.y), tx2, ntx2);
+      const float2 lo = WR_LERP2(WR_LERP2(lo00, lo01, ty2, nty2), WR_LERP2(lo10, lo11, ty2, nty2), tz2, ntz2);
+      const uint32_t p = zoff + (uint32_t)gy * nx + gx;
+      it_raw[h] = S::load1(R + p) - lo.x;
+      if (hx >= 1 && hx <= wx && hy >= 1 && hy <= wy) {
+        const float2 hi00 = WR_LERP2(make_float2(c000.z, c000.w), make_float2(c001.z, c001.w), tx2, ntx2);
+        const float2 hi01 = WR_LERP2(make_float2(c010.z, c010.w), make_float2(c011.z, c011.w), tx2, ntx2);
+        const float2 hi10 = WR_LERP2(make_float2(c100.z, c100.w), make_float2(c101.z, c101.w), tx2, ntx2);
+        const float2 hi11 = WR_LERP2(make_float2(c110.z, c110.w), make_float2(c111.z, c111.w), tx2, ntx2);
+        const float2 hi = WR_LERP2(WR_LERP2(hi00, hi01, ty2, nty2), WR_LERP2(hi10, hi11, ty2, nty2), tz2, ntz2);
+        float gxv = lo.y, gyv = hi.x, gzv = hi.y;
+        if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 0);
+        if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 1);
+        if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 2);
+        float excl = 0.f;
+        if (MASK) {
+          bool ex = (__ldg(a.mbits + p) & 1) != 0;
+          if (!ex && a.mmov) {
+            // the cell code covers exactly this sample's corners when the lower
+            // taps were not clamped
+            int code = 2;
+            if (xa == ix0 && ya == iy0 && za == iz0) code = (__ldg(a.mbits + i000) >> 1) & 3;
+            if (code == 1) ex = true;
+            else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
+          }
+          excl = ex ? 1.f : 0.f;
+        }
+        gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
+      }
+  #undef WR_LERP2
+      hx += step_x;
+      hy += step_y;
+      if (hx >= hw) { hx -= hw; ++hy; }
     }
-#undef WR_LERP2
-    hx += step_x;
-    hy += step_y;
-    if (hx >= hw) { hx -= hw; ++hy; }
-  }
-  __syncthreads();
+    __syncthreads();
 
-  float acc[10];
-#pragma unroll
-  for (int k = 0; k < 10; ++k) acc[k] = 0.f;
-  const float my_edge = (float)(y0 + w - (ny - 1));
-  const float mx_edge = (float)(x0 + w - (nx - 1));
-  const float inv_zr = (float)(1.0 / (double)a.zratio);
-  {
-    int ly = threadIdx.x / wx, lx = threadIdx.x - ly * wx;
-    const int sy = kAccThreads / wx, sx = kAccThreads - sy * wx;
-    for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
-      const float* rp = it_raw + ly * hw + lx;
-      float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
-                 (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
-      it *= (1.f / 9.f);
-      float4 g = gsm[i];
-      if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
-      acc[9] = fmaf(it, it, acc[9]);
+    float acc[10];
+  #pragma unroll
+    for (int k = 0; k < 10; ++k) acc[k] = 0.f;
+    const float my_edge = (float)(y0 + w - (ny - 1));
+    const float mx_edge = (float)(x0 + w - (nx - 1));
+    const float inv_zr = (float)(1.0 / (double)a.zratio);
+    {
+      int ly = threadIdx.x / wx, lx = threadIdx.x - ly * wx;
+      const int sy = kAccThreads / wx, sx = kAccThreads - sy * wx;
+      for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
+        const float* rp = it_raw + ly * hw + lx;
+        float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
+                   (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
+        it *= (1.f / 9.f);
+        float4 g = gsm[i];
+        if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
+        acc[9] = fmaf(it, it, acc[9]);
+        if (window) {
+          const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
+          const float iz = g.z * inv_zr;
+          const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
+          acc[0] = fmaf(wgx, g.x, acc[0]);
+          acc[1] = fmaf(wgx, g.y, acc[1]);
+          acc[2] = fmaf(wgx, iz, acc[2]);
+          acc[3] = fmaf(wgy, g.y, acc[3]);
+          acc[4] = fmaf(wgy, iz, acc[4]);
+          acc[5] = fmaf(wgz, iz, acc[5]);
+          acc[6] = fmaf(wgx, it, acc[6]);
+          acc[7] = fmaf(wgy, it, acc[7]);
+          acc[8] = fmaf(wgz, it, acc[8]);
+        }
+        lx += sx;
+        ly += sy;
+        if (lx >= wx) { lx -= wx; ++ly; }
+      }
+    }
+    // warp reduction, then the 8 warps in order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  #pragma unroll
+    for (int k = 0; k < 10; ++k)
+  #pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0)
+  #pragma unroll
+      for (int k = 0; k < 10; ++k) red[warp * 12 + k] = acc[k];
+    __syncthreads();
+    const long long blk = tile;
+    const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
+    if (threadIdx.x < 10) {
+      float t = 0.f;
+      for (int q = 0; q < kAccThreads / 32; ++q) t += red[q * 12 + threadIdx.x];
+      if (threadIdx.x == 9) a.errpart[blk] = (double)t;
+      else if (window) a.sums[cpi * 12 + threadIdx.x] = t;
+    } else if (threadIdx.x == 32) {
+      double pen = 0.0;
       if (window) {
-        const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
-        const float iz = g.z * inv_zr;
-        const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
-        acc[0] = fmaf(wgx, g.x, acc[0]);
-        acc[1] = fmaf(wgx, g.y, acc[1]);
-        acc[2] = fmaf(wgx, iz, acc[2]);
-        acc[3] = fmaf(wgy, g.y, acc[3]);
-        acc[4] = fmaf(wgy, iz, acc[4]);
-        acc[5] = fmaf(wgz, iz, acc[5]);
-        acc[6] = fmaf(wgx, it, acc[6]);
-        acc[7] = fmaf(wgy, it, acc[7]);
-        acc[8] = fmaf(wgz, it, acc[8]);
+        // neighbour difference on the CP grid (getNeiDiff with r = 1,
+        // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
+        // neighbours (edge-replicated) minus the centre, float64 then float32
+        const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
+        // in CP mode the shared-memory CP tile holds the 3x3 neighbourhood
+        const int ox = flags[2], oy = flags[3];
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            if (dx == 0 && dy == 0) continue;
+            const int qy = clampi(ty + dy, 0, ncy - 1), qx = clampi(tx + dx, 0, ncx - 1);
+            const float4 v = (MODE == FIELD_CP) ? tf.cpt[(qy - oy) * kTileCP + (qx - ox)] : b[qy * ncx + qx];
+            sx += 0.125 * (double)v.x;
+            sy += 0.125 * (double)v.y;
+            sz += 0.125 * (double)v.z;
+          }
+        const float4 c = (MODE == FIELD_CP) ? tf.cpt[(ty - oy) * kTileCP + (tx - ox)] : b[ty * ncx + tx];
+        const float ndx = (float)(sx - (double)c.x);
+        const float ndy = (float)(sy - (double)c.y);
+        const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
+        float* o = a.sums + cpi * 12;
+        o[9] = ndx;
+        o[10] = ndy;
+        o[11] = ndz;
+        pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
       }
-      lx += sx;
-      ly += sy;
-      if (lx >= wx) { lx -= wx; ++ly; }
+      a.penpart[blk] = pen;
     }
-  }
-  // warp reduction, then the 8 warps in order
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < 10; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < 10; ++k) red[warp * 12 + k] = acc[k];
-  __syncthreads();
-  const long long blk = ((long long)ty * a.ntx + tx) * nz + z;
-  const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
-  if (threadIdx.x < 10) {
-    float t = 0.f;
-    for (int q = 0; q < kAccThreads / 32; ++q) t += red[q * 12 + threadIdx.x];
-    if (threadIdx.x == 9) a.errpart[blk] = (double)t;
-    else if (window) a.sums[cpi * 12 + threadIdx.x] = t;
-  } else if (threadIdx.x == 32) {
-    double pen = 0.0;
-    if (window) {
-      // neighbour difference on the CP grid (getNeiDiff with r = 1,
-      // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
-      // neighbours (edge-replicated) minus the centre, float64 then float32
-      const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
-      // in CP mode the shared-memory CP tile holds the 3x3 neighbourhood
-      const int ox = flags[2], oy = flags[3];
-      double sx = 0.0, sy = 0.0, sz = 0.0;
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          if (dx == 0 && dy == 0) continue;
-          const int qy = clampi(ty + dy, 0, ncy - 1), qx = clampi(tx + dx, 0, ncx - 1);
-          const float4 v = (MODE == FIELD_CP) ? tf.cpt[(qy - oy) * kTileCP + (qx - ox)] : b[qy * ncx + qx];
-          sx += 0.125 * (double)v.x;
-          sy += 0.125 * (double)v.y;
-          sz += 0.125 * (double)v.z;
-        }
-      const float4 c = (MODE == FIELD_CP) ? tf.cpt[(ty - oy) * kTileCP + (tx - ox)] : b[ty * ncx + tx];
-      const float ndx = (float)(sx - (double)c.x);
-      const float ndy = (float)(sy - (double)c.y);
-      const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
-      float* o = a.sums + cpi * 12;
-      o[9] = ndx;
-      o[10] = ndy;
-      o[11] = ndz;
-      pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
-    }
-    a.penpart[blk] = pen;
+    __syncthreads();   // shared memory is refilled by the next tile
   }
 }
 
@@ -1062,34 +1151,42 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
 
 // max |new - old| over every voxel at a level's first iteration, where the
 // old field is not a function of this level's CPs (utils/calFlow3d_Wei_v1.py:641-643).
-// One CTA per (z slice, tile); both fields come from shared-memory tile factors.
+// Persistent CTAs take (z slice, tile) tiles in turn; both fields come from
+// shared-memory tile factors.
 template <int MODE0>
 __global__ void __launch_bounds__(kAccThreads) k_diff_first(LKState* st, IterArgs a, FieldSrc now) {
   if (!st->do_update) return;
   extern __shared__ float4 smem4[];
-  const int nx = a.mov.nx, ny = a.mov.ny, w = a.w;
-  const int z = blockIdx.x, tx = blockIdx.y, ty = blockIdx.z;
-  const int x0 = tx * w, y0 = ty * w;
-  const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
-  const int hw = wx + 2, hh = wy + 2;
+  const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz, w = a.w;
   TileField tn, to;
   tn.ax = smem4;
   tn.wy = tn.ax + (w + 2) * kTileCP;
   tn.cpt = tn.wy + (w + 2);
+  tn.ld = w + 2;
   to.ax = tn.cpt + kTileCP * kTileCP;
   to.wy = to.ax + (w + 2) * kTileCP;
   to.cpt = to.wy + (w + 2);
+  to.ld = w + 2;
   int* flags = reinterpret_cast<int*>(to.cpt + kTileCP * kTileCP);   // two 4-int slots
   float* red = reinterpret_cast<float*>(flags + 8);
-  build_tile_field<FIELD_CP>(tn, flags, now, a.r, w, x0, y0, hw, hh, z, nx, ny);
-  build_tile_field<MODE0>(to, flags + 4, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
-  const bool gn = flags[0] != 0, go = flags[4] != 0;
+  const int ntiles = nz * a.ntx * a.nty;
   float dmax = 0.f;
-  for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
-    const int ly = i / wx, lx = i - ly * wx;
-    const float3 p = tile_motion<FIELD_CP>(tn, gn, now, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
-    const float3 q = tile_motion<MODE0>(to, go, a.field, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
-    dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(p.x - q.x), fabsf(p.y - q.y)), fabsf(p.z - q.z)));
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int z = tile % nz, txy = tile / nz;
+    const int ty = txy / a.ntx, tx = txy - ty * a.ntx;
+    const int x0 = tx * w, y0 = ty * w;
+    const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
+    const int hw = wx + 2, hh = wy + 2;
+    build_tile_field<FIELD_CP>(tn, flags, now, a.r, w, x0, y0, hw, hh, z, nx, ny);
+    build_tile_field<MODE0>(to, flags + 4, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
+    const bool gn = flags[0] != 0, go = flags[4] != 0;
+    for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
+      const int ly = i / wx, lx = i - ly * wx;
+      const float3 p = tile_motion<FIELD_CP>(tn, gn, now, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
+      const float3 q = tile_motion<MODE0>(to, go, a.field, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
+      dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(p.x - q.x), fabsf(p.y - q.y)), fabsf(p.z - q.z)));
+    }
+    __syncthreads();   // shared memory is refilled by the next tile
   }
   const float m = block_max(dmax, red);
   if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
@@ -1146,15 +1243,12 @@ __global__ void k_cp_init(float4* cp, FieldSrc f, int ncx, int ncy, int nz, int 
 // at some level, and for the coarsest level's initial field)
 template <int MODE0>
 __global__ void k_dense_from(float4* out, FieldSrc f, int nx, int ny, int nz) {
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx);
-    const long long rest = i / nx;
-    const int y = (int)(rest % ny);
-    const int z = (int)(rest / ny);
-    const float3 v = eval_field<MODE0>(f, x, y, z);
-    out[i] = make_float4(v.x, v.y, v.z, 0.f);
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    WR_FOR_COLS(nx, x) {
+      const float3 v = eval_field<MODE0>(f, x, y, z);
+      out[(size_t)row * nx + x] = make_float4(v.x, v.y, v.z, 0.f);
+    }
   }
 }
 
@@ -1170,17 +1264,15 @@ __global__ void k_dense_init_pack(float4* out, const float* c0, const float* c1,
 // final motion (z, y, x, 3)
 template <int MODE>
 __global__ void k_write_motion(float* __restrict__ out, FieldSrc f, int nx, int ny, int nz) {
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx);
-    const long long rest = i / nx;
-    const int y = (int)(rest % ny);
-    const int z = (int)(rest / ny);
-    const float3 v = eval_field<MODE>(f, x, y, z);
-    out[3 * i + 0] = v.x;
-    out[3 * i + 1] = v.y;
-    out[3 * i + 2] = v.z;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    float* o = out + (size_t)row * nx * 3;
+    WR_FOR_COLS(nx, x) {
+      const float3 v = eval_field<MODE>(f, x, y, z);
+      o[3 * x + 0] = v.x;
+      o[3 * x + 1] = v.y;
+      o[3 * x + 2] = v.z;
+    }
   }
 }
 
@@ -1192,34 +1284,32 @@ __global__ void k_write_motion(float* __restrict__ out, FieldSrc f, int nx, int 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_warp(const T* __restrict__ src, const float* __restrict__ motion,
                                                   float* __restrict__ out, int nz, int ny, int nx) {
-  const long long n = (long long)nx * ny * nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx);
-    const long long rest = i / nx;
-    const int y = (int)(rest % ny);
-    const int z = (int)(rest / ny);
-    const float cx = (float)x + __ldg(motion + 3 * i + 0);
-    const float cy = (float)y + __ldg(motion + 3 * i + 1);
-    const float cz = (float)z + __ldg(motion + 3 * i + 2);
-    int x0, y0, z0;
-    float tx_f, ty_f, tz_f;
-    split_coord(cx, x0, tx_f);
-    split_coord(cy, y0, ty_f);
-    split_coord(cz, z0, tz_f);
-    const double tx = tx_f, ty = ty_f, tz = tz_f;
-    const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
-    const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
-    const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
-    const size_t sy = nx, sz = (size_t)nx * ny;
-    const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
-    const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
-    const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
-    const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
-    const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
-    const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
-                     wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
-    out[i] = (float)v;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const float* mrow = motion + (size_t)row * nx * 3;
+    WR_FOR_COLS(nx, x) {
+      const float cx = (float)x + __ldg(mrow + 3 * x + 0);
+      const float cy = (float)y + __ldg(mrow + 3 * x + 1);
+      const float cz = (float)z + __ldg(mrow + 3 * x + 2);
+      int x0, y0, z0;
+      float tx_f, ty_f, tz_f;
+      split_coord(cx, x0, tx_f);
+      split_coord(cy, y0, ty_f);
+      split_coord(cz, z0, tz_f);
+      const double tx = tx_f, ty = ty_f, tz = tz_f;
+      const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
+      const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
+      const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
+      const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
+      const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
+      const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
+      const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
+      const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
+      const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
+                       wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
+      out[(size_t)row * nx + x] = (float)v;
+    }
   }
 }
 

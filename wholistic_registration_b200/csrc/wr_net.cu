@@ -71,7 +71,6 @@ __device__ __forceinline__ long long vox(int n, int z, int y, int x, int Z, int 
 
 constexpr int kWarps = 4;
 constexpr int kMT = 2;     // m16 tiles per warp
-constexpr int kMaxNT = 8;  // n8 tiles (64 output channels)
 
 template <int NT>
 __global__ void __launch_bounds__(kWarps * 32) k_conv_fwd(Conv c, const __nv_bfloat16* __restrict__ x1,

@@ -12,6 +12,21 @@ namespace wr {
 // Field sources of a level's first iteration.
 enum FieldMode { FIELD_CP = 0, FIELD_UP = 1, FIELD_DENSE = 2, FIELD_ZERO = 3 };
 
+// Shift-invariant interior of a resize table: for outputs lo <= o < hi the
+// taps read in[s * o + c0 + t], t < P, with the same weights w[t] for every
+// such output (integer down-scale factor s).  hi <= lo: no such interior.
+constexpr int kSIMaxTaps = 40;
+// A row staged in shared memory in polyphase order (element e at
+// (e mod s) * ls + e / s) gives tap t of output o at off[t] + o: the lanes of
+// a warp, holding consecutive outputs, then read consecutive words.
+struct SITaps {
+  int P, s, c0, lo, hi;
+  int ls;                 // polyphase row length, in_len / s + 1
+  double w[kSIMaxTaps];
+  float wf[kSIMaxTaps];   // the same weights rounded to float32
+  int off[kSIMaxTaps];
+};
+
 struct LevelPlan {
   int nx, ny, nz;     // level extent (x fastest)
   int ncx, ncy;       // control points per slice along x and y
@@ -26,6 +41,7 @@ struct LevelPlan {
   int x_first;
   int up_x_first;
   int tx_taps, ty_taps;   // candidate taps of the full-res -> level tables
+  SITaps six, siy;        // their shift-invariant interiors
   // workspace byte offsets
   size_t ref, movg, mbits, mmov, cp, sums, dense, errpart, penpart;
   size_t tx_w, tx_i, ty_w, ty_i;      // bicubic tables full-res -> level (float64)
@@ -40,6 +56,7 @@ struct Plan {
   int precision;
   LevelPlan lv[WR_MAX_LEVELS];
   size_t tmp_a, tmp_a_bytes, tmp_b, tmp_b_bytes;
+  size_t tab_scratch;  // row-major x tables before their transpose
   size_t state;
   size_t total;
 };
