@@ -8,6 +8,7 @@
 
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "wr_b200.h"
@@ -66,6 +67,9 @@ static SITaps find_si_taps(int in_len, int out_len) {
   while (hi < out_len && fits(hi)) ++hi;
   si.P = P; si.s = s; si.c0 = c0; si.lo = lo; si.hi = hi;
   si.ls = in_len / s + 1;
+  volatile double acc = 0.0;   // tap-order float64 sum, no contraction
+  for (int t = 0; t < P; ++t) acc = acc + w[(size_t)mid * P + t];
+  si.wsum = acc;
   for (int t = 0; t < P; ++t) {
     si.w[t] = w[(size_t)mid * P + t];
     si.wf[t] = (float)si.w[t];
@@ -208,25 +212,66 @@ template <typename T> static T* at_off(void* base, size_t off) {
   return reinterpret_cast<T*>(static_cast<char*>(base) + off);
 }
 
-static size_t iter_smem(int w) { return accumulate_smem(w); }
 
 // x pass of a resize: rows staged in shared memory when the table has a
-// shift-invariant interior and the staged rows fit, else straight from
-// global memory.
+// shift-invariant interior with a down-scale factor of 2, 4 or 8 and the
+// staged rows fit, else straight from global memory.
+template <int S, typename Tin, typename A, typename Tout>
+static bool resample_x_si(const SITaps& si, const Tin* in, Tout* out, int nrows, int nx_in, int nx_out,
+                          const double* w, const int32_t* idx, cudaStream_t s) {
+  if (si.s != S || si.P != 4 * S + 2) return false;
+  size_t smem;
+  void (*kern)(const SITaps, const Tin*, Tout*, int, int, int, const double*, const int32_t*);
+  if constexpr (std::is_same<Tin, uint8_t>::value && std::is_same<A, double>::value &&
+                std::is_same<Tout, double>::value) {
+    const size_t nwords = (nx_in + 31) / 32;
+    smem = (size_t)kStageWarps * (((size_t)nx_in + 15) / 16 * 16 + 8 * (nwords + 1));
+    kern = k_resample_x_mask<S>;
+  } else {
+    smem = (size_t)kStageWarps * S * si.ls * sizeof(A);
+    kern = k_resample_x_si<S, Tin, A, Tout>;
+  }
+  if (smem > 96 * 1024) return false;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  long long g = (nrows + kStageWarps - 1) / kStageWarps;
+  if (g > 148LL * 32) g = 148LL * 32;
+  kern<<<(int)g, dim3(32, kStageWarps), smem, s>>>(si, in, out, nrows, nx_in, nx_out, w, idx);
+  return true;
+}
+
 template <typename Tin, typename A, typename Tout>
 static void resample_x(const SITaps& si, const Tin* in, Tout* out, int nrows, int nx_in, int nx_out,
                        const double* w, const int32_t* idx, int P, int stride, int comp, cudaStream_t s) {
-  const size_t smem = (size_t)kStageWarps * si.s * si.ls * sizeof(A);
-  if (si.hi > si.lo && smem <= 96 * 1024) {
-    auto kern = k_resample_x_staged<Tin, A, Tout>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    long long g = (nrows + kStageWarps - 1) / kStageWarps;
-    if (g > 148LL * 32) g = 148LL * 32;
-    kern<<<(int)g, dim3(32, kStageWarps), smem, s>>>(si, in, out, nrows, nx_in, nx_out, w, idx, P, stride, comp);
-  } else {
-    k_resample_x<Tin, A, Tout><<<row_grid(nrows), kRowBlock, 0, s>>>(si, in, out, 1, nrows, nx_in, nx_out, w, idx, P,
-                                                                     stride, comp);
-  }
+  if (si.hi > si.lo && stride == 1 &&
+      (resample_x_si<2, Tin, A, Tout>(si, in, out, nrows, nx_in, nx_out, w, idx, s) ||
+       resample_x_si<4, Tin, A, Tout>(si, in, out, nrows, nx_in, nx_out, w, idx, s) ||
+       resample_x_si<8, Tin, A, Tout>(si, in, out, nrows, nx_in, nx_out, w, idx, s)))
+    return;
+  k_resample_x<Tin, A, Tout><<<row_grid(nrows), kRowBlock, 0, s>>>(si, in, out, 1, nrows, nx_in, nx_out, w, idx, P,
+                                                                   stride, comp);
+}
+
+// y pass of a resize: the compile-time-tap kernel for a shift-invariant
+// table with a down-scale factor of 2, 4 or 8, else the table kernel.
+template <int S, typename Tin, typename A, typename Tout>
+static bool resample_y_si(const SITaps& si, const Tin* in, Tout* out, int nz, int ny_in, int ny_out, int nx,
+                          const double* w, const int32_t* idx, cudaStream_t s) {
+  if (si.s != S || si.P != 4 * S + 2) return false;
+  k_resample_y_si<S, Tin, A, Tout><<<row_grid((long long)nz * ny_out), kRowBlock, 0, s>>>(si, in, out, nz, ny_in,
+                                                                                       ny_out, nx, w, idx);
+  return true;
+}
+
+template <typename Tin, typename A, typename Tout>
+static void resample_y(const SITaps& si, const Tin* in, Tout* out, int nz, int ny_in, int ny_out, int nx,
+                       const double* w, const int32_t* idx, int P, int stride, int comp, cudaStream_t s) {
+  if (si.hi > si.lo && stride == 1 &&
+      (resample_y_si<2, Tin, A, Tout>(si, in, out, nz, ny_in, ny_out, nx, w, idx, s) ||
+       resample_y_si<4, Tin, A, Tout>(si, in, out, nz, ny_in, ny_out, nx, w, idx, s) ||
+       resample_y_si<8, Tin, A, Tout>(si, in, out, nz, ny_in, ny_out, nx, w, idx, s)))
+    return;
+  k_resample_y<Tin, A, Tout><<<row_grid((long long)nz * ny_out), kRowBlock, 0, s>>>(si, in, out, nz, ny_in, ny_out,
+                                                                                    nx, w, idx, P, stride, comp);
 }
 
 // Separable resize of a full-resolution volume to a level:
@@ -241,11 +286,9 @@ static void resize_to_level(const Plan& P, const LevelPlan& L, void* ws, const T
   const int32_t* tyi = at_off<int32_t>(ws, L.ty_i);
   if (L.x_first) {
     resample_x<Tin, A, A>(L.six, in, tmp, P.nz * P.ny, P.nx, L.nx, txw, txi, L.tx_taps, stride, comp, s);
-    k_resample_y<A, A, Tout><<<row_grid((long long)P.nz * L.ny), kRowBlock, 0, s>>>(
-        L.siy, tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi, L.ty_taps, 1, 0);
+    resample_y<A, A, Tout>(L.siy, tmp, out, P.nz, P.ny, L.ny, L.nx, tyw, tyi, L.ty_taps, 1, 0, s);
   } else {
-    k_resample_y<Tin, A, A><<<row_grid((long long)P.nz * L.ny), kRowBlock, 0, s>>>(
-        L.siy, in, tmp, P.nz, P.ny, L.ny, P.nx, tyw, tyi, L.ty_taps, stride, comp);
+    resample_y<Tin, A, A>(L.siy, in, tmp, P.nz, P.ny, L.ny, P.nx, tyw, tyi, L.ty_taps, stride, comp, s);
     resample_x<A, A, Tout>(L.six, tmp, out, P.nz * L.ny, P.nx, L.nx, txw, txi, L.tx_taps, 1, 0, s);
   }
 }
@@ -366,53 +409,51 @@ static int persistent_grid(K kernel, size_t smem, long long ntiles) {
   return (int)(ntiles < ctas ? (ntiles > 0 ? ntiles : 1) : ctas);
 }
 
-template <int MODE, bool MASK, int PREC>
+template <int MODE, int DIFF0, bool MASK, int PREC>
 static void launch_accumulate1(const IterArgs& a, long long ntiles, size_t smem, cudaStream_t s) {
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_lk_accumulate<MODE, MASK, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int grid = persistent_grid(k_lk_accumulate<MODE, MASK, PREC>, smem, ntiles);
-  k_lk_accumulate<MODE, MASK, PREC><<<grid, kAccThreads, smem, s>>>(a);
+  auto kern = k_lk_accumulate<MODE, DIFF0, MASK, PREC>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = persistent_grid(kern, smem, ntiles);
+  kern<<<grid, kAccThreads, smem, s>>>(a);
 }
 
+template <int MODE, int DIFF0, int PREC>
+static void launch_accumulate2(const IterArgs& a, long long ntiles, size_t smem, bool mask, cudaStream_t s) {
+  if (mask) launch_accumulate1<MODE, DIFF0, true, PREC>(a, ntiles, smem, s);
+  else launch_accumulate1<MODE, DIFF0, false, PREC>(a, ntiles, smem, s);
+}
+
+// diff0: kNoDiff, or the initial-field mode of the level (CP launches only)
 template <int PREC>
-static void launch_accumulate(int mode, const IterArgs& a, long long ntiles, size_t smem, bool mask, cudaStream_t s) {
+static void launch_accumulate(int mode, int diff0, const IterArgs& a, long long ntiles, size_t smem, bool mask,
+                              cudaStream_t s) {
   switch (mode) {
     case FIELD_CP:
-      mask ? launch_accumulate1<FIELD_CP, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_CP, false, PREC>(a, ntiles, smem, s);
+      switch (diff0) {
+        case FIELD_UP: launch_accumulate2<FIELD_CP, FIELD_UP, PREC>(a, ntiles, smem, mask, s); break;
+        case FIELD_DENSE: launch_accumulate2<FIELD_CP, FIELD_DENSE, PREC>(a, ntiles, smem, mask, s); break;
+        case FIELD_ZERO: launch_accumulate2<FIELD_CP, FIELD_ZERO, PREC>(a, ntiles, smem, mask, s); break;
+        default: launch_accumulate2<FIELD_CP, kNoDiff, PREC>(a, ntiles, smem, mask, s);
+      }
       break;
-    case FIELD_UP:
-      mask ? launch_accumulate1<FIELD_UP, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_UP, false, PREC>(a, ntiles, smem, s);
-      break;
-    case FIELD_DENSE:
-      mask ? launch_accumulate1<FIELD_DENSE, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_DENSE, false, PREC>(a, ntiles, smem, s);
-      break;
-    default:
-      mask ? launch_accumulate1<FIELD_ZERO, true, PREC>(a, ntiles, smem, s) : launch_accumulate1<FIELD_ZERO, false, PREC>(a, ntiles, smem, s);
+    case FIELD_UP: launch_accumulate2<FIELD_UP, kNoDiff, PREC>(a, ntiles, smem, mask, s); break;
+    case FIELD_DENSE: launch_accumulate2<FIELD_DENSE, kNoDiff, PREC>(a, ntiles, smem, mask, s); break;
+    default: launch_accumulate2<FIELD_ZERO, kNoDiff, PREC>(a, ntiles, smem, mask, s);
   }
 }
 
+// CP values of a level from its initial field
 template <int MODE0>
-static void level_first(const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f, bool cp_init,
-                        const IterArgs* diff, cudaStream_t s) {
-  if (cp_init)
-    k_cp_init<MODE0><<<grid_for(L.ncp), kThreads, 0, s>>>(at_off<float4>(ws, L.cp), f, L.ncx, L.ncy, L.nz, P.r, P.w);
-  if (diff) {
-    FieldSrc now = diff->field;
-    now.mode = FIELD_CP;
-    const size_t smem = diff_first_smem(P.w);
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_diff_first<MODE0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int grid = persistent_grid(k_diff_first<MODE0>, smem, L.nblk);
-    k_diff_first<MODE0><<<grid, kAccThreads, smem, s>>>(st, *diff, now);
-  }
+static void cp_init(const Plan& P, const LevelPlan& L, void* ws, const FieldSrc& f, cudaStream_t s) {
+  k_cp_init<MODE0><<<grid_for(L.ncp), kThreads, 0, s>>>(at_off<float4>(ws, L.cp), f, L.ncx, L.ncy, L.nz, P.r, P.w);
 }
 
-static void first_dispatch(int mode, const Plan& P, const LevelPlan& L, void* ws, LKState* st, const FieldSrc& f,
-                           bool cp_init, const IterArgs* diff, cudaStream_t s) {
+static void cp_init_dispatch(int mode, const Plan& P, const LevelPlan& L, void* ws, const FieldSrc& f,
+                             cudaStream_t s) {
   switch (mode) {
-    case FIELD_UP: level_first<FIELD_UP>(P, L, ws, st, f, cp_init, diff, s); break;
-    case FIELD_DENSE: level_first<FIELD_DENSE>(P, L, ws, st, f, cp_init, diff, s); break;
-    default: level_first<FIELD_ZERO>(P, L, ws, st, f, cp_init, diff, s); break;
+    case FIELD_UP: cp_init<FIELD_UP>(P, L, ws, f, s); break;
+    case FIELD_DENSE: cp_init<FIELD_DENSE>(P, L, ws, f, s); break;
+    default: cp_init<FIELD_ZERO>(P, L, ws, f, s); break;
   }
 }
 
@@ -475,7 +516,7 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
     n += 1;                                                    // level begin
     if (P.dense_all && !(l == P.levels - 1 && has_init)) n += 1; // dense field
     n += 1;                                                    // cp init
-    n += 4 * P.iter + 1;                                       // iterations + first diff
+    n += 4 * P.iter + (P.iter >= 2 ? 1 : 0);                   // iterations + first-update check
   }
   return n + 1;                                                // final motion
 }
@@ -511,7 +552,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       mode0 = FIELD_DENSE;
     }
     FieldSrc f0 = field_src(P, l, mode0, ws);
-    first_dispatch(mode0, P, L, ws, st, f0, true, nullptr, s);
+    cp_init_dispatch(mode0, P, L, ws, f0, s);
     IterArgs a;
     memset(&a, 0, sizeof(a));
     a.st = st;
@@ -531,15 +572,19 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     a.ntx = L.ntx;
     a.nty = L.nty;
     a.zratio = L.zratio;
-    const size_t smem = iter_smem(P.w);
     const int forced = p->forced_updates[l];
+    a.field0 = f0;
     for (int it = 0; it < P.iter; ++it) {
       const int mode = it == 0 ? mode0 : FIELD_CP;
+      // the launch after the level's first update also measures max |new - initial|
+      const int diff0 = it == 1 ? mode0 : kNoDiff;
       a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
+      const size_t smem = accumulate_smem(P.w, diff0 == FIELD_UP);
       const bool rec = prof && recorded < prof->capacity;
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
-      launch_accumulate<PREC>(mode, a, L.nblk, smem, mask, s);
+      launch_accumulate<PREC>(mode, diff0, a, L.nblk, smem, mask, s);
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
+      if (diff0 != kNoDiff) k_first_post<<<1, 1, 0, s>>>(st, l, forced);
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
       if (PREC == WR_PREC_F32)
         k_update<false><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
@@ -547,12 +592,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       else
         k_update<true><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
                                                              (double)p->movRange, L.zratio_d);
-      if (it == 0) {
-        IterArgs d = a;
-        d.field = f0;
-        first_dispatch(mode0, P, L, ws, st, f0, false, &d, s);
-      }
-      k_post<<<1, 1, 0, s>>>(st, l, forced);
+      k_post<<<1, 1, 0, s>>>(st, l, forced, it == 0 ? 1 : 0);
     }
   }
   const LevelPlan& L0 = P.lv[0];

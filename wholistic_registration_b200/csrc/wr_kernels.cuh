@@ -205,39 +205,139 @@ __global__ void k_resample_x(const __grid_constant__ SITaps si, const Tin* __res
   }
 }
 
-// The x pass with each row staged in shared memory: one warp per row, the
-// row read once with coalesced loads and stored in polyphase order, interior
-// outputs read their taps from shared memory without bank conflicts, edge
-// outputs from the table.  Blocks of 32 x kStageWarps threads; dynamic shared
-// memory kStageWarps * s * ls elements of A.
+// The x pass with each row staged in shared memory, for an integer down-scale
+// factor S (P = 4S + 2 candidate taps, fixed at compile time): one warp per
+// row; the row is read once with coalesced loads and stored in polyphase
+// order, so interior outputs read their taps from shared memory without bank
+// conflicts and with the weights as constant operands; edge outputs read the
+// table.  Blocks of 32 x kStageWarps threads; dynamic shared memory
+// kStageWarps * S * ls elements of A.
 constexpr int kStageWarps = 4;
-template <typename Tin, typename A, typename Tout>
-__global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_staged(
+template <int S, typename Tin, typename A, typename Tout>
+__global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_si(
     const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out, int nrows, int nx_in,
-    int nx_out, const double* __restrict__ w, const int32_t* __restrict__ idx, int P, int stride, int comp) {
+    int nx_out, const double* __restrict__ w, const int32_t* __restrict__ idx) {
+  constexpr int NP = 4 * S + 2;
   extern __shared__ __align__(16) unsigned char stage_raw[];
-  A* buf = reinterpret_cast<A*>(stage_raw) + (size_t)threadIdx.y * si.s * si.ls;
+  const int ls = si.ls;
+  A* buf = reinterpret_cast<A*>(stage_raw) + (size_t)threadIdx.y * S * ls;
   const int lane = threadIdx.x;
   for (int row = blockIdx.x * kStageWarps + threadIdx.y; row < nrows; row += gridDim.x * kStageWarps) {
-    const Tin* src = in + (size_t)row * nx_in * stride + comp;
-    for (int q = lane; q < si.ls; q += 32)
-      for (int ph = 0; ph < si.s; ++ph) {
-        const int e = q * si.s + ph;
-        if (e < nx_in) buf[ph * si.ls + q] = (A)__ldg(src + (size_t)e * stride);
+    const Tin* src = in + (size_t)row * nx_in;
+    for (int e0 = 0; e0 < nx_in; e0 += 32 * 8) {
+      A v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int e = e0 + 32 * k + lane;
+        v[k] = e < nx_in ? (A)__ldg(src + e) : (A)0;
       }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int e = e0 + 32 * k + lane;
+        if (e < nx_in) buf[(e % S) * ls + e / S] = v[k];
+      }
+    }
     __syncwarp();
     Tout* dst = out + (size_t)row * nx_out;
     for (int xo = lane; xo < nx_out; xo += 32) {
       A acc = 0;
       if (xo >= si.lo && xo < si.hi) {
-#pragma unroll 4
-        for (int t = 0; t < si.P; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), buf[si.off[t] + xo]);
+#pragma unroll
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), buf[si.off[t] + xo]);
       } else {
-        for (int t = 0; t < P; ++t)
-          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo),
-                             (A)__ldg(src + (size_t)__ldg(idx + (size_t)t * nx_out + xo) * stride));
+        for (int t = 0; t < NP; ++t)
+          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo), (A)__ldg(src + __ldg(idx + (size_t)t * nx_out + xo)));
       }
       dst[xo] = (Tout)acc;
+    }
+    __syncwarp();
+  }
+}
+
+// The x pass of a uint8 mask in float64, exact.  In a row holding only 0 and
+// 1, a tap with 0 adds an exact zero and a tap with 1 adds its weight, so an
+// output is the tap-order float64 sum of the weights of its set taps: 0 when
+// none is set, si.wsum (the same sum over every tap) when all are; only
+// windows that are mixed sum their taps.  Rows with other values take the
+// plain product sums.  The row is staged as bytes plus ballot words and
+// their prefix popcounts.
+template <int S>
+__global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
+    const __grid_constant__ SITaps si, const uint8_t* __restrict__ in, double* __restrict__ out, int nrows,
+    int nx_in, int nx_out, const double* __restrict__ w, const int32_t* __restrict__ idx) {
+  constexpr int NP = 4 * S + 2;
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  const int nwords = (nx_in + 31) / 32;
+  const int row_bytes = (nx_in + 15) & ~15;
+  unsigned char* base = stage_raw + (size_t)threadIdx.y * (row_bytes + 8 * (nwords + 1));
+  uint8_t* bytes = base;
+  unsigned* words = reinterpret_cast<unsigned*>(base + row_bytes);
+  unsigned* prefix = words + nwords + 1;   // set taps before word k
+  const int lane = threadIdx.x;
+  for (int row = blockIdx.x * kStageWarps + threadIdx.y; row < nrows; row += gridDim.x * kStageWarps) {
+    const uint8_t* src = in + (size_t)row * nx_in;
+    unsigned carry = 0;
+    bool nonbinary = false;
+    for (int k0 = 0; k0 < nwords; k0 += 32) {
+      // lane j ends with word k0 + j: bit i = element (k0 + j) * 32 + i is set
+      uint8_t v[32];
+#pragma unroll
+      for (int b = 0; b < 32; ++b) {
+        const int e = (k0 + b) * 32 + lane;
+        v[b] = e < nx_in ? __ldg(src + e) : (uint8_t)0;
+      }
+      unsigned mine = 0;
+#pragma unroll
+      for (int b = 0; b < 32; ++b) {
+        const int e = (k0 + b) * 32 + lane;
+        if (e < nx_in) bytes[e] = v[b];
+        nonbinary |= v[b] > 1;
+        const unsigned wv = __ballot_sync(0xffffffffu, v[b] != 0);
+        if (lane == b) mine = wv;
+      }
+      const int k = k0 + lane;
+      const unsigned c = __popc(mine);
+      unsigned incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned n = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += n;
+      }
+      if (k < nwords) {
+        words[k] = mine;
+        prefix[k] = carry + incl - c;
+      }
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) prefix[nwords] = carry;
+    nonbinary = __any_sync(0xffffffffu, nonbinary);
+    __syncwarp();
+    double* dst = out + (size_t)row * nx_out;
+    for (int xo = lane; xo < nx_out; xo += 32) {
+      double acc = 0.0;
+      if (xo >= si.lo && xo < si.hi) {
+        const int e0 = S * xo + si.c0, e1 = e0 + NP;   // interior: 0 <= e0, e1 <= nx_in
+        if (nonbinary) {
+#pragma unroll
+          for (int t = 0; t < NP; ++t) acc = __dadd_rn(acc, __dmul_rn(si.w[t], (double)bytes[e0 + t]));
+        } else {
+          const unsigned s0 = prefix[e0 >> 5] + __popc(words[e0 >> 5] & ((1u << (e0 & 31)) - 1u));
+          const unsigned s1 = prefix[e1 >> 5] + ((e1 & 31) ? __popc(words[e1 >> 5] & ((1u << (e1 & 31)) - 1u)) : 0u);
+          const unsigned cnt = s1 - s0;
+          if (cnt == (unsigned)NP) {
+            acc = si.wsum;
+          } else if (cnt != 0) {
+#pragma unroll
+            for (int t = 0; t < NP; ++t)
+              if (bytes[e0 + t]) acc = __dadd_rn(acc, si.w[t]);
+          }
+        }
+      } else {
+        for (int t = 0; t < NP; ++t)
+          acc = __dadd_rn(acc, __dmul_rn(__ldg(w + (size_t)t * nx_out + xo),
+                                         (double)__ldg(src + __ldg(idx + (size_t)t * nx_out + xo))));
+      }
+      dst[xo] = acc;
     }
     __syncwarp();
   }
@@ -269,6 +369,41 @@ __global__ void k_resample_y(const __grid_constant__ SITaps si, const Tin* __res
         const Tin* q = plane + (size_t)x * stride;
         A acc = 0;
         for (int t = 0; t < P; ++t) acc = Acc<A>::madd(acc, __ldg(wr + t), (A)__ldg(q + (size_t)__ldg(ir + t) * rs));
+        dst[x] = (Tout)acc;
+      }
+    }
+  }
+}
+
+// The y pass for an integer down-scale factor S (P = 4S + 2 taps fixed at
+// compile time, weights as constant operands); rows outside the
+// shift-invariant interior read the table.
+template <int S, typename Tin, typename A, typename Tout>
+__global__ void k_resample_y_si(const __grid_constant__ SITaps si, const Tin* __restrict__ in,
+                                Tout* __restrict__ out, int nz, int ny_in, int ny_out, int nx,
+                                const double* __restrict__ w, const int32_t* __restrict__ idx) {
+  constexpr int NP = 4 * S + 2;
+  WR_FOR_ROWS(nz * ny_out, row) {
+    const int z = row / ny_out, yo = row - z * ny_out;
+    const Tin* plane = in + (size_t)z * ny_in * nx;
+    Tout* dst = out + (size_t)row * nx;
+    if (yo >= si.lo && yo < si.hi) {
+      const Tin* r0 = plane + (size_t)(S * yo + si.c0) * nx;
+      WR_FOR_COLS(nx, x) {
+        A v[NP];
+#pragma unroll
+        for (int t = 0; t < NP; ++t) v[t] = (A)__ldg(r0 + (size_t)t * nx + x);
+        A acc = 0;
+#pragma unroll
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), v[t]);
+        dst[x] = (Tout)acc;
+      }
+    } else {
+      const double* wr = w + (size_t)yo * NP;
+      const int32_t* ir = idx + (size_t)yo * NP;
+      WR_FOR_COLS(nx, x) {
+        A acc = 0;
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, __ldg(wr + t), (A)__ldg(plane + (size_t)__ldg(ir + t) * nx + x));
         dst[x] = (Tout)acc;
       }
     }
@@ -614,6 +749,7 @@ struct IterArgs {
   double* __restrict__ penpart;        // per CTA
   CPView cpv;                          // this level's CPs (motion_current at CPs)
   FieldSrc field;                      // motion used for this iteration
+  FieldSrc field0;                     // level's initial field (first-diff launches)
   int r, w, ntx, nty;
   float zratio;
 };
@@ -797,14 +933,18 @@ __device__ __forceinline__ float3 tile_motion(const TileField& tf, bool generic,
   return eval_field<MODE>(f, gx, gy, z);
 }
 
-// Bytes of dynamic shared memory of k_lk_accumulate for patch width w.
-__host__ __device__ inline size_t accumulate_smem(int w) {
+// Bytes of dynamic shared memory of k_lk_accumulate for patch width w
+// (diff_up: a second tile field for the level's up-sampled initial field).
+__host__ __device__ inline size_t accumulate_smem(int w, bool diff_up = false) {
   const size_t hw = (size_t)w + 2;
   return 16 * (size_t)w * w                  // gradients + exclusion of the tile voxels
          + 4 * ((hw * hw + 3) & ~size_t(3))  // It_raw of tile + halo
          + tile_field_smem(w)                // motion factors
-         + 4 * 8 * 12 + 16;                  // reduction scratch, flags
+         + 4 * 8 * 12 + 16                   // reduction scratch, flags
+         + (diff_up ? tile_field_smem(w) + 16 : 0);
 }
+
+constexpr int kNoDiff = -1;
 
 // Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588).
 //
@@ -819,7 +959,12 @@ __host__ __device__ inline size_t accumulate_smem(int w) {
 // voxel once per replicated position (mode="nearest" of
 // utils/calculate.py:51).  Sums are reduced with warp shuffles in a fixed
 // order, so results are deterministic.
-template <int MODE, bool MASK, int PREC>
+//
+// DIFF0 != kNoDiff (the launch after a level's first update, MODE = CP): the
+// kernel also takes max |motion - initial field| over the tile voxels, where
+// the initial field (DIFF0 = UP / DENSE / ZERO) is not a function of this
+// level's CPs (utils/calFlow3d_Wei_v1.py:641-643), into st->maxdiff_bits.
+template <int MODE, int DIFF0, bool MASK, int PREC>
 __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
   typedef Store<PREC> S;
   // a level that has stopped leaves its remaining iteration launches empty
@@ -837,6 +982,13 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
   tf.ld = w + 2;
   int* flags = reinterpret_cast<int*>(tf.cpt + kTileCP * kTileCP);
   float* red = reinterpret_cast<float*>(flags + 4);       // 8 warps * 12
+  TileField tf0;                                          // DIFF0 == FIELD_UP
+  tf0.ax = reinterpret_cast<float4*>(red + 8 * 12);
+  tf0.wy = tf0.ax + (w + 2) * kTileCP;
+  tf0.cpt = tf0.wy + (w + 2);
+  tf0.ld = w + 2;
+  int* flags0 = reinterpret_cast<int*>(tf0.cpt + kTileCP * kTileCP);
+  float dmax = 0.f;
   const int ntiles = nz * a.ntx * a.nty;
   // persistent CTAs walk the tiles z fastest: tile = (ty * ntx + tx) * nz + z
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -847,6 +999,7 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
     const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
     const int hw = wx + 2, hh = wy + 2;
     build_tile_field<MODE>(tf, flags, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
+    if (DIFF0 == FIELD_UP) build_tile_field<FIELD_UP>(tf0, flags0, a.field0, a.r, w, x0, y0, hw, hh, z, nx, ny);
     const bool generic = flags[0] != 0;
 
     const typename S::V4* __restrict__ G = static_cast<const typename S::V4*>(a.mov.g);
@@ -917,6 +1070,11 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
           excl = ex ? 1.f : 0.f;
         }
         gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
+        if (DIFF0 != kNoDiff) {
+          const float3 q = tile_motion<DIFF0 == kNoDiff ? FIELD_ZERO : DIFF0>(
+              tf0, DIFF0 == FIELD_UP ? flags0[0] != 0 : false, a.field0, hx, hy, gx, gy, z);
+          dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(m.x - q.x), fabsf(m.y - q.y)), fabsf(m.z - q.z)));
+        }
       }
   #undef WR_LERP2
       hx += step_x;
@@ -1010,6 +1168,10 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
       a.penpart[blk] = pen;
     }
     __syncthreads();   // shared memory is refilled by the next tile
+  }
+  if (DIFF0 != kNoDiff) {
+    const float mx = block_max(dmax, red);
+    if (threadIdx.x == 0 && mx > 0.f) atomicMax(&a.st->maxdiff_bits, __float_as_uint(mx));
   }
 }
 
@@ -1149,64 +1311,35 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
   if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
 }
 
-// max |new - old| over every voxel at a level's first iteration, where the
-// old field is not a function of this level's CPs (utils/calFlow3d_Wei_v1.py:641-643).
-// Persistent CTAs take (z slice, tile) tiles in turn; both fields come from
-// shared-memory tile factors.
-template <int MODE0>
-__global__ void __launch_bounds__(kAccThreads) k_diff_first(LKState* st, IterArgs a, FieldSrc now) {
-  if (!st->do_update) return;
-  extern __shared__ float4 smem4[];
-  const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz, w = a.w;
-  TileField tn, to;
-  tn.ax = smem4;
-  tn.wy = tn.ax + (w + 2) * kTileCP;
-  tn.cpt = tn.wy + (w + 2);
-  tn.ld = w + 2;
-  to.ax = tn.cpt + kTileCP * kTileCP;
-  to.wy = to.ax + (w + 2) * kTileCP;
-  to.cpt = to.wy + (w + 2);
-  to.ld = w + 2;
-  int* flags = reinterpret_cast<int*>(to.cpt + kTileCP * kTileCP);   // two 4-int slots
-  float* red = reinterpret_cast<float*>(flags + 8);
-  const int ntiles = nz * a.ntx * a.nty;
-  float dmax = 0.f;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int z = tile % nz, txy = tile / nz;
-    const int ty = txy / a.ntx, tx = txy - ty * a.ntx;
-    const int x0 = tx * w, y0 = ty * w;
-    const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
-    const int hw = wx + 2, hh = wy + 2;
-    build_tile_field<FIELD_CP>(tn, flags, now, a.r, w, x0, y0, hw, hh, z, nx, ny);
-    build_tile_field<MODE0>(to, flags + 4, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
-    const bool gn = flags[0] != 0, go = flags[4] != 0;
-    for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
-      const int ly = i / wx, lx = i - ly * wx;
-      const float3 p = tile_motion<FIELD_CP>(tn, gn, now, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
-      const float3 q = tile_motion<MODE0>(to, go, a.field, lx + 1, ly + 1, x0 + lx, y0 + ly, z);
-      dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(p.x - q.x), fabsf(p.y - q.y)), fabsf(p.z - q.z)));
-    }
-    __syncthreads();   // shared memory is refilled by the next tile
-  }
-  const float m = block_max(dmax, red);
-  if (threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxdiff_bits, __float_as_uint(m));
-}
-
-__host__ __device__ inline size_t diff_first_smem(int w) { return 2 * tile_field_smem(w) + 32 + 4 * 64; }
 
 // after an update: log max |delta motion| and apply the 1e-3 rule
-// (utils/calFlow3d_Wei_v1.py:641-654)
-__global__ void k_post(LKState* st, int level, int forced) {
+// (utils/calFlow3d_Wei_v1.py:641-654).  defer: the level's first update,
+// whose max over the voxels the next iteration's launch completes
+// (k_first_post).
+__global__ void k_post(LKState* st, int level, int forced, int defer) {
   if (!st->do_update) return;
-  const float md = __uint_as_float(st->maxdiff_bits);
   WrLKStats& S = st->stats;
   const int u = st->n_updates;
-  if (u < WR_MAX_ITERS) S.max_diff_motion[level][u] = (double)md;
   st->n_updates = u + 1;
   S.updates[level] = u + 1;
+  st->do_update = 0;
+  if (defer) return;
+  const float md = __uint_as_float(st->maxdiff_bits);
+  if (u < WR_MAX_ITERS) S.max_diff_motion[level][u] = (double)md;
   if (forced < 0 && (double)md < 1e-3) st->active = 0;
   st->maxdiff_bits = 0u;
-  st->do_update = 0;
+}
+
+// The level's first update, once the following launch has added max
+// |new - initial| over the voxels: log it and apply the 1e-3 rule.  A level
+// that stops here discards that launch's error and sums (k_decide and
+// k_update skip an inactive level).
+__global__ void k_first_post(LKState* st, int level, int forced) {
+  if (!st->active) return;
+  const float md = __uint_as_float(st->maxdiff_bits);
+  st->stats.max_diff_motion[level][0] = (double)md;
+  if (forced < 0 && (double)md < 1e-3) st->active = 0;
+  st->maxdiff_bits = 0u;
 }
 
 __global__ void k_level_begin(LKState* st, int level, int first) {

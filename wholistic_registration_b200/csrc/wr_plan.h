@@ -25,6 +25,7 @@ struct SITaps {
   double w[kSIMaxTaps];
   float wf[kSIMaxTaps];   // the same weights rounded to float32
   int off[kSIMaxTaps];
+  double wsum;            // the weights summed in tap order in float64
 };
 
 struct LevelPlan {
