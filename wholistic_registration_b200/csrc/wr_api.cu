@@ -208,6 +208,9 @@ static int row_grid(long long nrows) {
 }
 static const dim3 kRowBlock(32, kRowWarps);
 
+// null counts as aligned
+static bool aligned(const void* p, size_t bytes) { return ((uintptr_t)p % bytes) == 0; }
+
 template <typename T> static T* at_off(void* base, size_t off) {
   return reinterpret_cast<T*>(static_cast<char*>(base) + off);
 }
@@ -308,12 +311,19 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
     if (l == 0) {
       // scale 1 on every axis: the resize is an exact copy
       if (!reuse_ref) k_to_level<T, PREC><<<grid_for(L.n), kThreads, 0, s>>>(ref, refl, L.n);
-      k_pack_movg<T, PREC><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
+      // four voxels per lane when rows are a multiple of 4 long and the inputs aligned
+      const bool x4 = L.nx % 4 == 0 && aligned(mov, 4 * sizeof(T)) && aligned(mmov_u8, 4) && aligned(mref_u8, 4);
+      const int g = row_grid((long long)L.nz * L.ny);
+      if (x4) k_pack_movg_x4<T, PREC><<<g, kRowBlock, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
+      else k_pack_movg<T, PREC><<<g, kRowBlock, 0, s>>>(mov, movg, L.nz, L.ny, L.nx);
       // exclusion bits and the moving mask as float, straight from the uint8 masks
-      if (any_mask)
-        k_mask_bits<uint8_t><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(
-            nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8, mmov_u8 ? mmov : nullptr, bits, L.nz, L.ny, L.nx,
-            reuse_ref ? 1 : 0);
+      if (any_mask && x4)
+        k_mask_bits_u8x4<<<g, kRowBlock, 0, s>>>(reuse_ref ? nullptr : mref_u8, mmov_u8, mmov_u8 ? mmov : nullptr, bits,
+                                                 L.nz, L.ny, L.nx, reuse_ref ? 1 : 0);
+      else if (any_mask)
+        k_mask_bits<uint8_t><<<g, kRowBlock, 0, s>>>(nullptr, reuse_ref ? nullptr : mref_u8, mmov_u8,
+                                                     mmov_u8 ? mmov : nullptr, bits, L.nz, L.ny, L.nx,
+                                                     reuse_ref ? 1 : 0);
       continue;
     }
     float* tmpf = at_off<float>(ws, P.tmp_a);

@@ -475,6 +475,110 @@ __global__ void k_pack_movg(const T* __restrict__ m, typename Store<PREC>::V4* _
 // mask bits of a level: bit0 = resized mask_ref > 0; bits 1-2 = class of the
 // trilinear cell whose lower corner is this voxel in the resized mask_mov:
 // 0 = all 8 corners <= 0, 1 = all > 0, 2 = mixed (needs the exact sum).
+// Four consecutive elements of a row (16-byte loads for float, 8 for
+// uint16, 4 for uint8; the caller checks the alignment).
+template <typename T> __device__ __forceinline__ float4 load_x4(const T* p);
+template <> __device__ __forceinline__ float4 load_x4<float>(const float* p) {
+  return __ldg(reinterpret_cast<const float4*>(p));
+}
+template <> __device__ __forceinline__ float4 load_x4<uint16_t>(const uint16_t* p) {
+  const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+  return make_float4((float)(v.x & 0xffffu), (float)(v.x >> 16), (float)(v.y & 0xffffu), (float)(v.y >> 16));
+}
+template <> __device__ __forceinline__ float4 load_x4<uint8_t>(const uint8_t* p) {
+  const unsigned v = __ldg(reinterpret_cast<const unsigned*>(p));
+  return make_float4((float)(v & 0xffu), (float)((v >> 8) & 0xffu), (float)((v >> 16) & 0xffu), (float)(v >> 24));
+}
+
+// k_pack_movg with four voxels per lane (nx a multiple of 4, rows aligned
+// for load_x4): one 4-wide load per neighbouring row, the x neighbours from
+// the lane's own elements and the adjacent lanes.
+template <typename T, int PREC>
+__global__ void k_pack_movg_x4(const T* __restrict__ m, typename Store<PREC>::V4* __restrict__ movg, int nz, int ny,
+                               int nx) {
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const int lane = threadIdx.x;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const size_t base = (size_t)row * nx;
+    const size_t dyp = (size_t)(min(y + 1, ny - 1) - y) * sy, dym = (size_t)(y - max(y - 1, 0)) * sy;
+    const size_t dzp = (size_t)(min(z + 1, nz - 1) - z) * sz, dzm = (size_t)(z - max(z - 1, 0)) * sz;
+    float carry = 0.f;   // last element of the previous chunk
+    for (int x0 = 0; x0 < nx; x0 += 128) {
+      const int x = x0 + 4 * lane, xc = min(x, nx - 4);
+      const size_t i = base + xc;
+      const float4 c = load_x4<T>(m + i);
+      const float4 yp = load_x4<T>(m + i + dyp), ym = load_x4<T>(m + i - dym);
+      const float4 zp = load_x4<T>(m + i + dzp), zm = load_x4<T>(m + i - dzm);
+      const float ahead = load_f<T>(m, base + min(x0 + 128, nx - 1));   // same address in every lane
+      float left = __shfl_up_sync(0xffffffffu, c.w, 1);
+      float right = __shfl_down_sync(0xffffffffu, c.x, 1);
+      if (lane == 0) left = x0 == 0 ? c.x : carry;
+      if (lane == 31) right = ahead;
+      if (x + 4 >= nx) right = c.w;
+      carry = __shfl_sync(0xffffffffu, c.w, 31);
+      if (x < nx) {
+        typename Store<PREC>::V4* o = movg + base + x;
+        o[0] = Store<PREC>::pack4(make_float4(c.x, 0.5f * (c.y - left), 0.5f * (yp.x - ym.x), 0.5f * (zp.x - zm.x)));
+        o[1] = Store<PREC>::pack4(make_float4(c.y, 0.5f * (c.z - c.x), 0.5f * (yp.y - ym.y), 0.5f * (zp.y - zm.y)));
+        o[2] = Store<PREC>::pack4(make_float4(c.z, 0.5f * (c.w - c.y), 0.5f * (yp.z - ym.z), 0.5f * (zp.z - zm.z)));
+        o[3] = Store<PREC>::pack4(make_float4(c.w, 0.5f * (right - c.z), 0.5f * (yp.w - ym.w), 0.5f * (zp.w - zm.w)));
+      }
+    }
+  }
+}
+
+// k_mask_bits for full-resolution uint8 masks with four voxels per lane (nx a
+// multiple of 4, rows 4-byte aligned); same bits and float moving mask.
+__global__ void k_mask_bits_u8x4(const uint8_t* __restrict__ mref_u8, const uint8_t* __restrict__ mmov,
+                                 float* __restrict__ mmov_f, uint8_t* __restrict__ bits, int nz, int ny, int nx,
+                                 int keep_ref_bit) {
+  const int lane = threadIdx.x;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const size_t base = (size_t)row * nx;
+    const size_t dy = (size_t)(min(y + 1, ny - 1) - y) * nx, dz = (size_t)(min(z + 1, nz - 1) - z) * nx * ny;
+    for (int x0 = 0; x0 < nx; x0 += 128) {
+      const int x = x0 + 4 * lane, xc = min(x, nx - 4);
+      const size_t i = base + xc;
+      unsigned b = 0;
+      if (keep_ref_bit) b = __ldg(reinterpret_cast<const unsigned*>(bits + i)) & 0x01010101u;
+      else if (mref_u8) {
+        const unsigned r = __ldg(reinterpret_cast<const unsigned*>(mref_u8 + i));
+        for (int j = 0; j < 4; ++j) b |= ((r >> (8 * j)) & 0xffu) ? (1u << (8 * j)) : 0u;
+      }
+      if (mmov) {
+        // per row of the cell (y, z), (y+1, z), (y, z+1), (y+1, z+1): 4 nonzero flags in bits 0..3
+        unsigned fl[4];
+        const size_t offs[4] = {0, dy, dz, dz + dy};
+        const size_t ahead = base + min(x0 + 128, nx - 1);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const unsigned v = __ldg(reinterpret_cast<const unsigned*>(mmov + i + offs[r]));
+          unsigned f = 0;
+          for (int j = 0; j < 4; ++j) f |= ((v >> (8 * j)) & 0xffu) ? (1u << j) : 0u;
+          unsigned nxt = __shfl_down_sync(0xffffffffu, f, 1) & 1u;          // next lane's first element
+          if (lane == 31) nxt = __ldg(mmov + ahead + offs[r]) != 0 ? 1u : 0u;
+          if (x + 4 >= nx) nxt = (f >> 3) & 1u;                             // edge clamp
+          fl[r] = f | (nxt << 4);
+        }
+        float mf[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const unsigned pair = 3u << j;   // columns j, j+1
+          const unsigned any = (fl[0] | fl[1] | fl[2] | fl[3]) & pair;
+          const unsigned all = (fl[0] & fl[1] & fl[2] & fl[3]) & pair;
+          const unsigned code = any == 0 ? 0u : (all == pair ? 1u : 2u);
+          b |= code << (8 * j + 1);
+          mf[j] = (fl[0] >> j) & 1u ? 1.f : 0.f;
+        }
+        if (mmov_f && x < nx) *reinterpret_cast<float4*>(mmov_f + base + x) = make_float4(mf[0], mf[1], mf[2], mf[3]);
+      }
+      if (x < nx) *reinterpret_cast<unsigned*>(bits + base + x) = b;
+    }
+  }
+}
+
 template <typename TM> __device__ __forceinline__ bool mask_on(const TM* m, size_t i);
 template <> __device__ __forceinline__ bool mask_on<float>(const float* m, size_t i) { return __ldg(m + i) > 0.f; }
 template <> __device__ __forceinline__ bool mask_on<uint8_t>(const uint8_t* m, size_t i) { return __ldg(m + i) != 0; }
@@ -1084,49 +1188,58 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
     __syncthreads();
 
     float acc[10];
-  #pragma unroll
+#pragma unroll
     for (int k = 0; k < 10; ++k) acc[k] = 0.f;
     const float my_edge = (float)(y0 + w - (ny - 1));
     const float mx_edge = (float)(x0 + w - (nx - 1));
     const float inv_zr = (float)(1.0 / (double)a.zratio);
     {
-      int ly = threadIdx.x / wx, lx = threadIdx.x - ly * wx;
-      const int sy = kAccThreads / wx, sx = kAccThreads - sy * wx;
-      for (int i = threadIdx.x; i < wx * wy; i += kAccThreads) {
-        const float* rp = it_raw + ly * hw + lx;
-        float it = (rp[0] + rp[1] + rp[2]) + (rp[hw] + rp[hw + 1] + rp[hw + 2]) +
-                   (rp[2 * hw] + rp[2 * hw + 1] + rp[2 * hw + 2]);
-        it *= (1.f / 9.f);
-        float4 g = gsm[i];
-        if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
-        acc[9] = fmaf(it, it, acc[9]);
-        if (window) {
-          const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
-          const float iz = g.z * inv_zr;
-          const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
-          acc[0] = fmaf(wgx, g.x, acc[0]);
-          acc[1] = fmaf(wgx, g.y, acc[1]);
-          acc[2] = fmaf(wgx, iz, acc[2]);
-          acc[3] = fmaf(wgy, g.y, acc[3]);
-          acc[4] = fmaf(wgy, iz, acc[4]);
-          acc[5] = fmaf(wgz, iz, acc[5]);
-          acc[6] = fmaf(wgx, it, acc[6]);
-          acc[7] = fmaf(wgy, it, acc[7]);
-          acc[8] = fmaf(wgz, it, acc[8]);
+      // Threads take column strips (column lx, output rows ly0 .. ly1 - 1);
+      // the 3x3 box is the sum of three horizontal 3-sums carried down the
+      // strip in registers.
+      const int nstrips = max(1, kAccThreads / wx);
+      const int rows_per = (wy + nstrips - 1) / nstrips;
+      for (int c = threadIdx.x; c < nstrips * wx; c += kAccThreads) {
+        const int strip = c / wx, lx = c - strip * wx;
+        const int ly0 = strip * rows_per, ly1 = min(ly0 + rows_per, wy);
+        if (ly0 >= ly1) continue;
+        const float* col = it_raw + lx;
+        float h0 = (col[ly0 * hw] + col[ly0 * hw + 1]) + col[ly0 * hw + 2];
+        float h1 = (col[(ly0 + 1) * hw] + col[(ly0 + 1) * hw + 1]) + col[(ly0 + 1) * hw + 2];
+        for (int ly = ly0; ly < ly1; ++ly) {
+          const float* rp = col + (ly + 2) * hw;
+          const float h2 = (rp[0] + rp[1]) + rp[2];
+          float it = ((h0 + h1) + h2) * (1.f / 9.f);
+          h0 = h1;
+          h1 = h2;
+          float4 g = gsm[ly * wx + lx];
+          if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
+          acc[9] = fmaf(it, it, acc[9]);
+          if (window) {
+            const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
+            const float iz = g.z * inv_zr;
+            const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
+            acc[0] = fmaf(wgx, g.x, acc[0]);
+            acc[1] = fmaf(wgx, g.y, acc[1]);
+            acc[2] = fmaf(wgx, iz, acc[2]);
+            acc[3] = fmaf(wgy, g.y, acc[3]);
+            acc[4] = fmaf(wgy, iz, acc[4]);
+            acc[5] = fmaf(wgz, iz, acc[5]);
+            acc[6] = fmaf(wgx, it, acc[6]);
+            acc[7] = fmaf(wgy, it, acc[7]);
+            acc[8] = fmaf(wgz, it, acc[8]);
+          }
         }
-        lx += sx;
-        ly += sy;
-        if (lx >= wx) { lx -= wx; ++ly; }
       }
     }
     // warp reduction, then the 8 warps in order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  #pragma unroll
+#pragma unroll
     for (int k = 0; k < 10; ++k)
-  #pragma unroll
+#pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
     if (lane == 0)
-  #pragma unroll
+#pragma unroll
       for (int k = 0; k < 10; ++k) red[warp * 12 + k] = acc[k];
     __syncthreads();
     const long long blk = tile;
