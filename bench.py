@@ -194,7 +194,7 @@ def run_ours(args, wl, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from wholistic_registration_b200 import LKParams, LKRegistrar, warp
+    from wholistic_registration_b200 import LKParams, LKRegistrar
     from wholistic_registration_b200.registrar import KernelProfile
     from wholistic_registration_b200.series import SeriesRegistrar
 
@@ -215,9 +215,10 @@ def run_ours(args, wl, rank, world, local_rank):
     def step(k, prof=None, keep_stats=False):
         f = frames[k % len(frames)]
         # the template's pyramid is built by the first call and reused for the series
-        reg.register(f, template, excl, excl, None, out=motion, profile=prof, reuse_reference=ref_ready[0])
+        # registration and correctMotion of the frame in one call
+        reg.register(f, template, excl, excl, None, out=motion, profile=prof, reuse_reference=ref_ready[0],
+                     warped_out=warped)
         ref_ready[0] = True
-        warp(f, motion, out=warped)
         if keep_stats:
             stats_hist[k].copy_(reg.stats_dev, non_blocking=True)
 

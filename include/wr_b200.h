@@ -174,6 +174,20 @@ WR_API int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, con
                                    void* stream, WrProfile* prof);
 
 /*
+ * getMotion followed by correctMotion of the same moving volume, the step the
+ * reference's series registration takes per frame
+ * (motion = getMotion(mov, ref, option); out = correctMotion(mov, motion)):
+ * replaces a wr_lk_register + wr_warp_trilinear(mov) pair with the same
+ * results, writing motion_out and warped_out ((z,y,x) float32) in one pass
+ * over the full-resolution grid.  prof may be NULL.  No single reference
+ * function corresponds to it.
+ */
+WR_API int wr_lk_register_warp(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                               const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                               float* motion_out, float* warped_out, WrLKStats* stats, void* workspace,
+                               size_t workspace_bytes, void* stream, WrProfile* prof);
+
+/*
  * Pull-warp `src` through `motion`: out(p) = src(p + motion(p)), trilinear,
  * edge-replicated, float32 result (correctMotion, utils/calFlow3d_Wei_v1.py:676-706).
  *   motion : (z,y,x,3) float32 device; out : (z,y,x) float32 device.

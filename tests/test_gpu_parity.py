@@ -188,6 +188,27 @@ def test_reuse_reference_matches_fresh_registration():
     torch.testing.assert_close(kept, fresh, rtol=0, atol=0)
 
 
+@pytest.mark.parametrize("shape,layer", [((8, 96, 80), 2), ((6, 70, 66), 0)])
+def test_register_and_warp_in_one_call_matches_two_calls(shape, layer):
+    """wr_lk_register_warp gives exactly the motion of wr_lk_register and the
+    volume of wr_warp_trilinear on that motion (correctMotion)."""
+    _cf3()
+    from wholistic_registration_b200 import LKParams, LKRegistrar, synthetic, warp
+
+    tmpl, mov, _ = synthetic.make_pair(shape, 31, n_blobs=300, max_disp=(2.5, 2.5, 0.8))
+    excl = (~synthetic.ellipsoid_inclusion(shape, 0.75)).to(torch.uint8)
+    t, m, e = (x.cuda().contiguous() for x in (tmpl, mov, excl))
+    p = LKParams(layer=layer, iter=1 if layer == 0 else 10, r=4, zRatio=1.0, movRange=5.0, smoothPenalty=200.0,
+                 tol=1e-3)
+    reg = LKRegistrar(shape, p)
+    motion = reg.register(m, t, e, e).clone()
+    warped = warp(m, motion)
+    warped_fused = torch.empty(shape, dtype=torch.float32, device="cuda")
+    motion_fused = reg.register(m, t, e, e, warped_out=warped_fused).clone()
+    torch.testing.assert_close(motion_fused, motion, rtol=0, atol=0)
+    torch.testing.assert_close(warped_fused, warped, rtol=0, atol=0)
+
+
 @pytest.mark.parametrize("precision,rms_tol", [(1, 0.02), (2, 0.1)])
 def test_mixed_precision_error_against_fp64_oracle(precision, rms_tol):
     """Levels and gradients stored in float16 (1) or bfloat16 (2), sums and

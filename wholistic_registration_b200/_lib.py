@@ -36,6 +36,7 @@ EXPORTS = (
     "wr_lk_workspace_size",
     "wr_lk_register",
     "wr_lk_register_profiled",
+    "wr_lk_register_warp",
     "wr_warp_trilinear",
     "wr_penalty_factor",
     "wr_penalty_factor_noalloc",
@@ -147,6 +148,8 @@ def load():
         lib.wr_lk_register.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), vp, vp,
                                        ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
         lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
+        lib.wr_lk_register_warp.argtypes = (lib.wr_lk_register.argtypes[:7] + [vp] + lib.wr_lk_register.argtypes[7:]
+                                            + [ctypes.POINTER(WrProfile)])
         lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_penalty_factor.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp, sz, vp]
         lib.wr_penalty_factor_noalloc.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]

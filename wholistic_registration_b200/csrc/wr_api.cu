@@ -533,7 +533,7 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
 
 template <typename T, int PREC>
 static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
-                        const uint8_t* mref, const float* init, float* out, WrLKStats* stats, void* ws,
+                        const uint8_t* mref, const float* init, float* out, float* warped, WrLKStats* stats, void* ws,
                         cudaStream_t s, WrProfile* prof) {
   int recorded = 0;
   LKState* st = at_off<LKState>(ws, P.state);
@@ -606,12 +606,19 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     }
   }
   const LevelPlan& L0 = P.lv[0];
-  if (P.dense_all) {
-    FieldSrc f = field_src(P, 0, FIELD_DENSE, ws);
-    k_write_motion<FIELD_DENSE><<<row_grid((long long)L0.nz * L0.ny), kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+  const int g0 = row_grid((long long)L0.nz * L0.ny);
+  const int mode_out = P.dense_all ? FIELD_DENSE : FIELD_CP;
+  const FieldSrc f = field_src(P, 0, mode_out, ws);
+  if (warped) {
+    // the full-resolution motion and mov warped by it, in one pass
+    if (mode_out == FIELD_DENSE)
+      k_write_motion_warp<FIELD_DENSE, T><<<g0, kRowBlock, 0, s>>>(out, warped, mov, f, L0.nx, L0.ny, L0.nz);
+    else
+      k_write_motion_warp<FIELD_CP, T><<<g0, kRowBlock, 0, s>>>(out, warped, mov, f, L0.nx, L0.ny, L0.nz);
+  } else if (mode_out == FIELD_DENSE) {
+    k_write_motion<FIELD_DENSE><<<g0, kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   } else {
-    FieldSrc f = field_src(P, 0, FIELD_CP, ws);
-    k_write_motion<FIELD_CP><<<row_grid((long long)L0.nz * L0.ny), kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
+    k_write_motion<FIELD_CP><<<g0, kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   }
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
   if (prof) {
@@ -660,18 +667,18 @@ static int noalloc_partials(double** out) {
 
 template <int PREC>
 static int dispatch_dtype(const Plan& P, const WrLKParams* p, const WrVolume* mov, const WrVolume* ref,
-                          const uint8_t* mmov, const uint8_t* mref, const float* init, float* out, WrLKStats* stats,
-                          void* ws, cudaStream_t s, WrProfile* prof) {
+                          const uint8_t* mmov, const uint8_t* mref, const float* init, float* out, float* warped,
+                          WrLKStats* stats, void* ws, cudaStream_t s, WrProfile* prof) {
   switch (mov->dtype) {
     case WR_U16:
       return run_register<uint16_t, PREC>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, mmov, mref,
-                                          init, out, stats, ws, s, prof);
+                                          init, out, warped, stats, ws, s, prof);
     case WR_U8:
       return run_register<uint8_t, PREC>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, mmov, mref, init,
-                                         out, stats, ws, s, prof);
+                                         out, warped, stats, ws, s, prof);
     default:
       return run_register<float, PREC>(P, p, (const float*)mov->data, (const float*)ref->data, mmov, mref, init, out,
-                                       stats, ws, s, prof);
+                                       warped, stats, ws, s, prof);
   }
 }
 
@@ -710,10 +717,12 @@ int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl
                                  workspace, workspace_bytes, stream, nullptr);
 }
 
-int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
-                            const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
-                            float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
-                            void* stream, WrProfile* prof) {
+// getMotion, optionally followed by correctMotion of mov (warped != null),
+// with optional per-launch events around the fused iteration kernel.
+static int register_common(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                           const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                           float* motion_out, float* warped_out, WrLKStats* stats, void* workspace,
+                           size_t workspace_bytes, void* stream, WrProfile* prof) {
   int rc;
   if ((rc = check_volume(mov, "mov"))) return rc;
   if ((rc = check_volume(ref, "ref"))) return rc;
@@ -732,15 +741,32 @@ int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (p->precision) {
     case WR_PREC_F16:
-      return dispatch_dtype<WR_PREC_F16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
-                                         workspace, s, prof);
+      return dispatch_dtype<WR_PREC_F16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
+                                         warped_out, stats, workspace, s, prof);
     case WR_PREC_BF16:
-      return dispatch_dtype<WR_PREC_BF16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
-                                          workspace, s, prof);
+      return dispatch_dtype<WR_PREC_BF16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
+                                          warped_out, stats, workspace, s, prof);
     default:
-      return dispatch_dtype<WR_PREC_F32>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out, stats,
-                                         workspace, s, prof);
+      return dispatch_dtype<WR_PREC_F32>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
+                                         warped_out, stats, workspace, s, prof);
   }
+}
+
+int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                            const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                            float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                            void* stream, WrProfile* prof) {
+  return register_common(mov, ref, excl_mask_mov, excl_mask_ref, p, motion_init, motion_out, nullptr, stats,
+                         workspace, workspace_bytes, stream, prof);
+}
+
+int wr_lk_register_warp(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                        const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init, float* motion_out,
+                        float* warped_out, WrLKStats* stats, void* workspace, size_t workspace_bytes, void* stream,
+                        WrProfile* prof) {
+  if (!warped_out) return fail(WR_E_NULL, "warped_out is NULL");
+  return register_common(mov, ref, excl_mask_mov, excl_mask_ref, p, motion_init, motion_out, warped_out, stats,
+                         workspace, workspace_bytes, stream, prof);
 }
 
 int wr_warp_trilinear(const WrVolume* src, const float* motion, float* out, void* stream) {

@@ -1527,34 +1527,60 @@ __global__ void k_write_motion(float* __restrict__ out, FieldSrc f, int nx, int 
 // trilinear arithmetic on float32 values, float32 result
 // ---------------------------------------------------------------------------
 
+// src sampled at (x, y, z) + m: float64 trilinear weights on the (clamped)
+// float32 corner values, rounded once to float32.
+template <typename T>
+__device__ __forceinline__ float warp_sample(const T* __restrict__ src, int nx, int ny, int nz, int x, int y, int z,
+                                             float mx, float my, float mz) {
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const float cx = (float)x + mx, cy = (float)y + my, cz = (float)z + mz;
+  int x0, y0, z0;
+  float tx_f, ty_f, tz_f;
+  split_coord(cx, x0, tx_f);
+  split_coord(cy, y0, ty_f);
+  split_coord(cz, z0, tz_f);
+  const double tx = tx_f, ty = ty_f, tz = tz_f;
+  const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
+  const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
+  const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
+  const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
+  const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
+  const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
+  const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
+  const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
+  const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
+                   wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
+  return (float)v;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_warp(const T* __restrict__ src, const float* __restrict__ motion,
                                                   float* __restrict__ out, int nz, int ny, int nx) {
-  const size_t sy = nx, sz = (size_t)nx * ny;
   WR_FOR_ROWS(nz * ny, row) {
     const int z = row / ny, y = row - z * ny;
     const float* mrow = motion + (size_t)row * nx * 3;
     WR_FOR_COLS(nx, x) {
-      const float cx = (float)x + __ldg(mrow + 3 * x + 0);
-      const float cy = (float)y + __ldg(mrow + 3 * x + 1);
-      const float cz = (float)z + __ldg(mrow + 3 * x + 2);
-      int x0, y0, z0;
-      float tx_f, ty_f, tz_f;
-      split_coord(cx, x0, tx_f);
-      split_coord(cy, y0, ty_f);
-      split_coord(cz, z0, tz_f);
-      const double tx = tx_f, ty = ty_f, tz = tz_f;
-      const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
-      const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
-      const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
-      const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
-      const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
-      const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
-      const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
-      const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
-      const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
-                       wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
-      out[(size_t)row * nx + x] = (float)v;
+      out[(size_t)row * nx + x] = warp_sample<T>(src, nx, ny, nz, x, y, z, __ldg(mrow + 3 * x + 0),
+                                                 __ldg(mrow + 3 * x + 1), __ldg(mrow + 3 * x + 2));
+    }
+  }
+}
+
+// final motion (z, y, x, 3) and mov warped by it (correctMotion) in one pass:
+// the same values as k_write_motion followed by k_warp
+template <int MODE, typename T>
+__global__ void __launch_bounds__(kThreads) k_write_motion_warp(float* __restrict__ out, float* __restrict__ warped,
+                                                               const T* __restrict__ src, FieldSrc f, int nx, int ny,
+                                                               int nz) {
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    float* o = out + (size_t)row * nx * 3;
+    WR_FOR_COLS(nx, x) {
+      const float3 v = eval_field<MODE>(f, x, y, z);
+      o[3 * x + 0] = v.x;
+      o[3 * x + 1] = v.y;
+      o[3 * x + 2] = v.z;
+      warped[(size_t)row * nx + x] = warp_sample<T>(src, nx, ny, nz, x, y, z, v.x, v.y, v.z);
     }
   }
 }

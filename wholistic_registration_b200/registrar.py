@@ -119,7 +119,8 @@ class LKRegistrar:
         self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
 
     def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
-                 motion_init=None, out=None, stream=None, profile=None, reuse_reference=False) -> torch.Tensor:
+                 motion_init=None, out=None, stream=None, profile=None, reuse_reference=False,
+                 warped_out=None) -> torch.Tensor:
         """Motion (z, y, x, 3) float32 registering ``mov`` onto ``ref``.
 
         Masks are (z, y, x) uint8/bool exclusion masks (True = excluded) or
@@ -127,6 +128,8 @@ class LKRegistrar:
         ``reuse_reference`` keeps the reference pyramid and reference mask
         built by the previous call on this registrar (same ``ref`` and
         ``mask_ref``), as when registering a time series to one template.
+        ``warped_out`` (float32 (z, y, x)) also receives ``mov`` warped by the
+        motion (correctMotion), written in the same pass as the motion.
         """
         if tuple(mov.shape) != self.shape or tuple(ref.shape) != self.shape:
             raise ValueError(f"volumes must have shape {self.shape}")
@@ -155,11 +158,18 @@ class LKRegistrar:
         self._cp.flags = _lib.WR_LK_REUSE_REFERENCE if reuse_reference else 0
         args = (ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
                 out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream))
-        if profile is None:
+        prof = ctypes.byref(profile.begin_call()) if profile is not None else None
+        if warped_out is not None:
+            _require_cuda(warped_out, "warped_out")
+            if tuple(warped_out.shape) != self.shape or warped_out.dtype != torch.float32 \
+                    or not warped_out.is_contiguous():
+                raise ValueError("warped_out must be contiguous float32 (z, y, x)")
+            _lib.check("wr_lk_register_warp",
+                       self.lib.wr_lk_register_warp(*args[:7], warped_out.data_ptr(), *args[7:], prof))
+        elif profile is None:
             _lib.check("wr_lk_register", self.lib.wr_lk_register(*args))
         else:
-            _lib.check("wr_lk_register_profiled",
-                       self.lib.wr_lk_register_profiled(*args, ctypes.byref(profile.begin_call())))
+            _lib.check("wr_lk_register_profiled", self.lib.wr_lk_register_profiled(*args, prof))
         return out
 
     def stats(self) -> _lib.WrLKStats:

@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import torch
 
-from .registrar import LKParams, LKRegistrar, warp
+from .registrar import LKParams, LKRegistrar
 
 
 class SeriesRegistrar:
@@ -70,10 +70,11 @@ class SeriesRegistrar:
                 self.s_run.wait_event(self.in_ready[k])
                 if self.started[k]:
                     self.s_run.wait_event(self.out_free[k])
+                # motion and the frame warped by it (correctMotion) in one call
                 self.reg.register(self.d_in[k], self.template, mask_mov, self.mask_ref, None,
-                                  out=self.d_motion[k], stream=self.s_run, reuse_reference=self.ref_ready)
+                                  out=self.d_motion[k], stream=self.s_run, reuse_reference=self.ref_ready,
+                                  warped_out=self.d_warp[k])
                 self.ref_ready = True
-                warp(self.d_in[k], self.d_motion[k], out=self.d_warp[k], stream=self.s_run)
                 self.in_free[k].record(self.s_run)
                 self.out_ready[k].record(self.s_run)
             with torch.cuda.stream(self.s_out):
