@@ -46,6 +46,7 @@ extern "C" {
 #define WR_ABI_VERSION 1
 #define WR_MAX_LEVELS 8
 #define WR_MAX_ITERS 64
+#define WR_MAX_BATCH 32
 
 /* element types of input volumes */
 enum {
@@ -77,8 +78,16 @@ enum {
   /* The workspace already holds the pyramid of this `ref` and `excl_mask_ref`
      from an earlier call with the same shape and parameters: skip rebuilding
      them (a time series registered against one template). */
-  WR_LK_REUSE_REFERENCE = 1
+  WR_LK_REUSE_REFERENCE = 1,
+  /* Tuning of the fused iteration kernel (results do not depend on it):
+     visit the (z, window) tiles x-fastest instead of z-fastest ... */
+  WR_LK_TILE_ORDER_X = 1 << 8,
+  /* ... and run WR_LK_CTAS_PER_SM(n) persistent CTAs per SM, n in 1..15
+     (0 = as many as fit). */
+  WR_LK_CTAS_PER_SM_SHIFT = 12,
+  WR_LK_CTAS_PER_SM_MASK = 15 << 12
 };
+#define WR_LK_CTAS_PER_SM(n) (((n) & 15) << WR_LK_CTAS_PER_SM_SHIFT)
 
 /* A volume: device pointer, element type and (z, y, x) extent. */
 typedef struct {
@@ -172,6 +181,41 @@ WR_API int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, con
                                    const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
                                    float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
                                    void* stream, WrProfile* prof);
+
+/*
+ * One frame of a batched registration (wr_lk_register_batch).  mov and ref
+ * have the same shape and dtype; shapes may differ between frames.
+ */
+typedef struct {
+  WrVolume mov;
+  WrVolume ref;
+  const uint8_t* excl_mask_mov;   /* or NULL */
+  const uint8_t* excl_mask_ref;   /* or NULL */
+  const float* motion_init;       /* option["motion"] or NULL */
+  float* motion_out;              /* (z,y,x,3) float32 */
+  float* warped_out;              /* correctMotion(mov, motion) (z,y,x) float32, or NULL */
+  WrLKStats* stats;               /* device WrLKStats or NULL */
+} WrLKItem;
+
+/* Workspace bytes of wr_lk_register_batch for these frames and parameters
+   (only the shapes, dtypes and the presence of masks / initial fields are
+   read). */
+WR_API int wr_lk_batch_workspace_size(const WrLKItem* items, int32_t n, const WrLKParams* p, size_t* bytes);
+
+/*
+ * getMotion (and optionally correctMotion) of n <= WR_MAX_BATCH frames with
+ * one parameter set, as the reference's batch loop calls it frame by frame
+ * (utils/registration.py:299-346), but run together: each pyramid level
+ * advances every frame with one persistent launch of the fused iteration
+ * kernel per LK iteration (plus one launch each of the decision, solve and
+ * bookkeeping kernels), each frame keeping its own stopping state, so every
+ * frame's results equal those of a wr_lk_register call on it alone.
+ * The frames must agree on dtype and on which of the masks and motion_init
+ * are present.  WR_LK_REUSE_REFERENCE keeps each frame's reference pyramid
+ * from the previous batch call on the same workspace.  No profiling.
+ */
+WR_API int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, void* workspace,
+                                size_t workspace_bytes, void* stream);
 
 /*
  * getMotion followed by correctMotion of the same moving volume, the step the

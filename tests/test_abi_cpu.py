@@ -49,8 +49,13 @@ def test_struct_layout_matches_header(tmp_path):
                        "forced_updates"],
         "WrLKStats": ["levels", "evals", "updates", "nan_solves", "current_error", "diff_error", "penalty_error",
                       "max_diff_motion"],
+        "WrLKItem": ["mov", "ref", "excl_mask_mov", "excl_mask_ref", "motion_init", "motion_out", "warped_out",
+                     "stats"],
+        "WrProfile": ["acc_begin", "acc_end", "capacity", "recorded", "launches"],
+        "WrConvGeom": ["n", "oz", "iz", "stride", "c1", "c2", "up1", "cout", "act"],
     }
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "wr_b200.h"', 'int main(void){']
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "wr_b200.h"', '#include "wr_net.h"',
+             'int main(void){']
     for st, fs in fields.items():
         lines.append(f'printf("{st} %zu\\n", sizeof({st}));')
         for f in fs:

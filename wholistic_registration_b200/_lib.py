@@ -16,10 +16,17 @@ LIB_PATH = os.path.join(HERE, "_wr_b200.so")
 
 MAX_LEVELS = 8
 MAX_ITERS = 64
+MAX_BATCH = 32
 
 WR_U8, WR_U16, WR_F32 = 1, 2, 3
 WR_PREC_F32, WR_PREC_F16, WR_PREC_BF16 = 0, 1, 2
 WR_LK_REUSE_REFERENCE = 1
+WR_LK_TILE_ORDER_X = 1 << 8
+WR_LK_CTAS_PER_SM_SHIFT = 12
+
+
+def WR_LK_CTAS_PER_SM(n: int) -> int:
+    return (int(n) & 15) << WR_LK_CTAS_PER_SM_SHIFT
 
 ERRORS = {
     1: "WR_E_NULL",
@@ -37,6 +44,8 @@ EXPORTS = (
     "wr_lk_register",
     "wr_lk_register_profiled",
     "wr_lk_register_warp",
+    "wr_lk_batch_workspace_size",
+    "wr_lk_register_batch",
     "wr_warp_trilinear",
     "wr_penalty_factor",
     "wr_penalty_factor_noalloc",
@@ -108,6 +117,19 @@ class WrProfile(ctypes.Structure):
     ]
 
 
+class WrLKItem(ctypes.Structure):
+    _fields_ = [
+        ("mov", WrVolume),
+        ("ref", WrVolume),
+        ("excl_mask_mov", ctypes.c_void_p),
+        ("excl_mask_ref", ctypes.c_void_p),
+        ("motion_init", ctypes.c_void_p),
+        ("motion_out", ctypes.c_void_p),
+        ("warped_out", ctypes.c_void_p),
+        ("stats", ctypes.c_void_p),
+    ]
+
+
 class WrConvGeom(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in
                 ("n", "oz", "oy", "ox", "iz", "iy", "ix", "stride", "c1", "c2", "up1", "cout", "act")]
@@ -148,6 +170,9 @@ def load():
         lib.wr_lk_register.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), vp, vp,
                                        ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
         lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
+        lib.wr_lk_batch_workspace_size.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams),
+                                                   ctypes.POINTER(sz)]
+        lib.wr_lk_register_batch.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams), vp, sz, vp]
         lib.wr_lk_register_warp.argtypes = (lib.wr_lk_register.argtypes[:7] + [vp] + lib.wr_lk_register.argtypes[7:]
                                             + [ctypes.POINTER(WrProfile)])
         lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]

@@ -394,9 +394,10 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
 
 // Grid of a persistent tile kernel: as many CTAs as stay resident on the
 // device at once (occupancy x SM count), at most one per tile.
-// The resident-CTA count is cached per (kernel, shared memory, device).
+// The resident-CTA count is cached per (kernel, shared memory, device);
+// per_sm > 0 caps the CTAs per SM.
 template <typename K>
-static int persistent_grid(K kernel, size_t smem, long long ntiles) {
+static int persistent_grid(K kernel, size_t smem, long long ntiles, int per_sm_cap = 0) {
   struct Entry { const void* fn; size_t smem; int dev; int ctas; };
   static std::mutex mu;
   static std::vector<Entry> cache;
@@ -416,39 +417,45 @@ static int persistent_grid(K kernel, size_t smem, long long ntiles) {
     std::lock_guard<std::mutex> lock(mu);
     cache.push_back(Entry{(const void*)kernel, smem, dev, ctas});
   }
+  if (per_sm_cap > 0) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms > 0 && per_sm_cap * sms < ctas) ctas = per_sm_cap * sms;
+  }
   return (int)(ntiles < ctas ? (ntiles > 0 ? ntiles : 1) : ctas);
 }
 
 template <int MODE, int DIFF0, bool MASK, int PREC>
-static void launch_accumulate1(const IterArgs& a, long long ntiles, size_t smem, cudaStream_t s) {
+static void launch_accumulate1(const IterArgs& a, long long ntiles, size_t smem, int flags, cudaStream_t s) {
   auto kern = k_lk_accumulate<MODE, DIFF0, MASK, PREC>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int grid = persistent_grid(kern, smem, ntiles);
-  kern<<<grid, kAccThreads, smem, s>>>(a);
+  const int grid = persistent_grid(kern, smem, ntiles, (flags & WR_LK_CTAS_PER_SM_MASK) >> WR_LK_CTAS_PER_SM_SHIFT);
+  kern<<<grid, kAccThreads, smem, s>>>(a, (flags & WR_LK_TILE_ORDER_X) ? 1 : 0);
 }
 
 template <int MODE, int DIFF0, int PREC>
-static void launch_accumulate2(const IterArgs& a, long long ntiles, size_t smem, bool mask, cudaStream_t s) {
-  if (mask) launch_accumulate1<MODE, DIFF0, true, PREC>(a, ntiles, smem, s);
-  else launch_accumulate1<MODE, DIFF0, false, PREC>(a, ntiles, smem, s);
+static void launch_accumulate2(const IterArgs& a, long long ntiles, size_t smem, bool mask, int flags,
+                               cudaStream_t s) {
+  if (mask) launch_accumulate1<MODE, DIFF0, true, PREC>(a, ntiles, smem, flags, s);
+  else launch_accumulate1<MODE, DIFF0, false, PREC>(a, ntiles, smem, flags, s);
 }
 
 // diff0: kNoDiff, or the initial-field mode of the level (CP launches only)
 template <int PREC>
 static void launch_accumulate(int mode, int diff0, const IterArgs& a, long long ntiles, size_t smem, bool mask,
-                              cudaStream_t s) {
+                              int flags, cudaStream_t s) {
   switch (mode) {
     case FIELD_CP:
       switch (diff0) {
-        case FIELD_UP: launch_accumulate2<FIELD_CP, FIELD_UP, PREC>(a, ntiles, smem, mask, s); break;
-        case FIELD_DENSE: launch_accumulate2<FIELD_CP, FIELD_DENSE, PREC>(a, ntiles, smem, mask, s); break;
-        case FIELD_ZERO: launch_accumulate2<FIELD_CP, FIELD_ZERO, PREC>(a, ntiles, smem, mask, s); break;
-        default: launch_accumulate2<FIELD_CP, kNoDiff, PREC>(a, ntiles, smem, mask, s);
+        case FIELD_UP: launch_accumulate2<FIELD_CP, FIELD_UP, PREC>(a, ntiles, smem, mask, flags, s); break;
+        case FIELD_DENSE: launch_accumulate2<FIELD_CP, FIELD_DENSE, PREC>(a, ntiles, smem, mask, flags, s); break;
+        case FIELD_ZERO: launch_accumulate2<FIELD_CP, FIELD_ZERO, PREC>(a, ntiles, smem, mask, flags, s); break;
+        default: launch_accumulate2<FIELD_CP, kNoDiff, PREC>(a, ntiles, smem, mask, flags, s);
       }
       break;
-    case FIELD_UP: launch_accumulate2<FIELD_UP, kNoDiff, PREC>(a, ntiles, smem, mask, s); break;
-    case FIELD_DENSE: launch_accumulate2<FIELD_DENSE, kNoDiff, PREC>(a, ntiles, smem, mask, s); break;
-    default: launch_accumulate2<FIELD_ZERO, kNoDiff, PREC>(a, ntiles, smem, mask, s);
+    case FIELD_UP: launch_accumulate2<FIELD_UP, kNoDiff, PREC>(a, ntiles, smem, mask, flags, s); break;
+    case FIELD_DENSE: launch_accumulate2<FIELD_DENSE, kNoDiff, PREC>(a, ntiles, smem, mask, flags, s); break;
+    default: launch_accumulate2<FIELD_ZERO, kNoDiff, PREC>(a, ntiles, smem, mask, flags, s);
   }
 }
 
@@ -531,80 +538,68 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
   return n + 1;                                                // final motion
 }
 
+// Pyramid, tables and initial field of one frame.
 template <typename T, int PREC>
-static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
-                        const uint8_t* mref, const float* init, float* out, float* warped, WrLKStats* stats, void* ws,
-                        cudaStream_t s, WrProfile* prof) {
-  int recorded = 0;
+static void prepare_frame(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
+                          const uint8_t* mref, const float* init, void* ws, cudaStream_t s) {
   LKState* st = at_off<LKState>(ws, P.state);
   int* err_flag = reinterpret_cast<int*>(reinterpret_cast<char*>(st) + sizeof(LKState));
   cudaMemsetAsync(err_flag, 0, sizeof(int), s);
   build_tables(P, ws, err_flag, s);
-  const bool reuse_ref = (p->flags & WR_LK_REUSE_REFERENCE) != 0;
-  build_pyramid<T, PREC>(P, ws, mov, ref, mmov, mref, reuse_ref, s);
+  build_pyramid<T, PREC>(P, ws, mov, ref, mmov, mref, (p->flags & WR_LK_REUSE_REFERENCE) != 0, s);
   if (init) init_field(P, ws, init, s);
-  const bool mask = mmov || mref;
-  const double sps = p->smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
-  const float sps_f = (float)sps;
-  for (int l = P.levels - 1; l >= 0; --l) {
-    const LevelPlan& L = P.lv[l];
-    const bool coarsest = l == P.levels - 1;
-    k_level_begin<<<1, 1, 0, s>>>(st, l, coarsest ? 1 : 0);
-    int mode0;
-    if (coarsest) mode0 = init ? FIELD_DENSE : FIELD_ZERO;
-    else mode0 = FIELD_UP;
-    if (P.dense_all) {
-      // no update can happen at any level: carry dense fields down the pyramid
-      FieldSrc f = field_src(P, l, mode0, ws);
-      float4* dense = at_off<float4>(ws, L.dense);
-      if (mode0 == FIELD_UP) k_dense_from<FIELD_UP><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
-      else if (mode0 == FIELD_ZERO) k_dense_from<FIELD_ZERO><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
-      mode0 = FIELD_DENSE;
-    }
-    FieldSrc f0 = field_src(P, l, mode0, ws);
-    cp_init_dispatch(mode0, P, L, ws, f0, s);
-    IterArgs a;
-    memset(&a, 0, sizeof(a));
-    a.st = st;
-    a.ref = at_off<void>(ws, L.ref);
-    a.mov.g = at_off<void>(ws, L.movg);
-    a.mov.nx = L.nx;
-    a.mov.ny = L.ny;
-    a.mov.nz = L.nz;
-    a.mbits = mask ? at_off<uint8_t>(ws, L.mbits) : nullptr;
-    a.mmov = mmov ? at_off<float>(ws, L.mmov) : nullptr;
-    a.sums = at_off<float>(ws, L.sums);
-    a.errpart = at_off<double>(ws, L.errpart);
-    a.penpart = at_off<double>(ws, L.penpart);
-    a.cpv = cp_view(P, L, ws);
-    a.r = P.r;
-    a.w = P.w;
-    a.ntx = L.ntx;
-    a.nty = L.nty;
-    a.zratio = L.zratio;
-    const int forced = p->forced_updates[l];
-    a.field0 = f0;
-    for (int it = 0; it < P.iter; ++it) {
-      const int mode = it == 0 ? mode0 : FIELD_CP;
-      // the launch after the level's first update also measures max |new - initial|
-      const int diff0 = it == 1 ? mode0 : kNoDiff;
-      a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
-      const size_t smem = accumulate_smem(P.w, diff0 == FIELD_UP);
-      const bool rec = prof && recorded < prof->capacity;
-      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
-      launch_accumulate<PREC>(mode, diff0, a, L.nblk, smem, mask, s);
-      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
-      if (diff0 != kNoDiff) k_first_post<<<1, 1, 0, s>>>(st, l, forced);
-      k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
-      if (PREC == WR_PREC_F32)
-        k_update<false><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
-                                                              (double)p->movRange, L.zratio_d);
-      else
-        k_update<true><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
-                                                             (double)p->movRange, L.zratio_d);
-      k_post<<<1, 1, 0, s>>>(st, l, forced, it == 0 ? 1 : 0);
-    }
+}
+
+// Start of level l for one frame: control state, initial field, CP values and
+// the fused kernel's arguments (field = the level's initial field; mode0 is
+// returned in *mode0).
+static IterArgs begin_level(const Plan& P, int l, void* ws, bool has_init, bool mask, bool has_mmov, int* mode0,
+                            cudaStream_t s) {
+  const LevelPlan& L = P.lv[l];
+  LKState* st = at_off<LKState>(ws, P.state);
+  const bool coarsest = l == P.levels - 1;
+  k_level_begin<<<1, 1, 0, s>>>(st, l, coarsest ? 1 : 0);
+  int m0 = coarsest ? (has_init ? FIELD_DENSE : FIELD_ZERO) : FIELD_UP;
+  if (P.dense_all) {
+    // no update can happen at any level: carry dense fields down the pyramid
+    FieldSrc f = field_src(P, l, m0, ws);
+    float4* dense = at_off<float4>(ws, L.dense);
+    const int g = row_grid((long long)L.nz * L.ny);
+    if (m0 == FIELD_UP) k_dense_from<FIELD_UP><<<g, kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+    else if (m0 == FIELD_ZERO) k_dense_from<FIELD_ZERO><<<g, kRowBlock, 0, s>>>(dense, f, L.nx, L.ny, L.nz);
+    m0 = FIELD_DENSE;
   }
+  const FieldSrc f0 = field_src(P, l, m0, ws);
+  cp_init_dispatch(m0, P, L, ws, f0, s);
+  IterArgs a;
+  memset(&a, 0, sizeof(a));
+  a.st = st;
+  a.ref = at_off<void>(ws, L.ref);
+  a.mov.g = at_off<void>(ws, L.movg);
+  a.mov.nx = L.nx;
+  a.mov.ny = L.ny;
+  a.mov.nz = L.nz;
+  a.mbits = mask ? at_off<uint8_t>(ws, L.mbits) : nullptr;
+  a.mmov = has_mmov ? at_off<float>(ws, L.mmov) : nullptr;
+  a.sums = at_off<float>(ws, L.sums);
+  a.errpart = at_off<double>(ws, L.errpart);
+  a.penpart = at_off<double>(ws, L.penpart);
+  a.cpv = cp_view(P, L, ws);
+  a.r = P.r;
+  a.w = P.w;
+  a.ntx = L.ntx;
+  a.nty = L.nty;
+  a.zratio = L.zratio;
+  a.field = f0;
+  a.field0 = f0;
+  *mode0 = m0;
+  return a;
+}
+
+// Full-resolution motion (and the warped frame), stats.
+template <typename T>
+static void finish_frame(const Plan& P, void* ws, const T* mov, float* out, float* warped, WrLKStats* stats,
+                         cudaStream_t s) {
   const LevelPlan& L0 = P.lv[0];
   const int g0 = row_grid((long long)L0.nz * L0.ny);
   const int mode_out = P.dense_all ? FIELD_DENSE : FIELD_CP;
@@ -620,7 +615,49 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   } else {
     k_write_motion<FIELD_CP><<<g0, kRowBlock, 0, s>>>(out, f, L0.nx, L0.ny, L0.nz);
   }
+  LKState* st = at_off<LKState>(ws, P.state);
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
+}
+
+template <typename T, int PREC>
+static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
+                        const uint8_t* mref, const float* init, float* out, float* warped, WrLKStats* stats, void* ws,
+                        cudaStream_t s, WrProfile* prof) {
+  int recorded = 0;
+  LKState* st = at_off<LKState>(ws, P.state);
+  prepare_frame<T, PREC>(P, p, mov, ref, mmov, mref, init, ws, s);
+  const bool reuse_ref = (p->flags & WR_LK_REUSE_REFERENCE) != 0;
+  const bool mask = mmov || mref;
+  const double sps = p->smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
+  const float sps_f = (float)sps;
+  for (int l = P.levels - 1; l >= 0; --l) {
+    const LevelPlan& L = P.lv[l];
+    int mode0;
+    IterArgs a = begin_level(P, l, ws, init != nullptr, mask, mmov != nullptr, &mode0, s);
+    const FieldSrc f0 = a.field0;
+    const int forced = p->forced_updates[l];
+    for (int it = 0; it < P.iter; ++it) {
+      const int mode = it == 0 ? mode0 : FIELD_CP;
+      // the launch after the level's first update also measures max |new - initial|
+      const int diff0 = it == 1 ? mode0 : kNoDiff;
+      a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
+      const size_t smem = accumulate_smem(P.w, diff0 == FIELD_UP);
+      const bool rec = prof && recorded < prof->capacity;
+      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
+      launch_accumulate<PREC>(mode, diff0, a, L.nblk, smem, mask, p->flags, s);
+      if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
+      if (diff0 != kNoDiff) k_first_post<<<1, 1, 0, s>>>(st, l, forced);
+      k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
+      if (PREC == WR_PREC_F32)
+        k_update<false><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
+                                                              (double)p->movRange, L.zratio_d);
+      else
+        k_update<true><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
+                                                             (double)p->movRange, L.zratio_d);
+      k_post<<<1, 1, 0, s>>>(st, l, forced, it == 0 ? 1 : 0);
+    }
+  }
+  finish_frame<T>(P, ws, mov, out, warped, stats, s);
   if (prof) {
     prof->recorded = recorded;
     prof->launches = count_launches(P, mmov != nullptr, mref != nullptr, init != nullptr, reuse_ref,
@@ -628,6 +665,113 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "wr_lk_register launch");
+  return WR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched registration
+// ---------------------------------------------------------------------------
+
+template <int MODE, int DIFF0, bool MASK, int PREC>
+static void launch_batch1(const BatchIter& b, long long ntiles, size_t smem, int flags, cudaStream_t s) {
+  auto kern = k_lk_accumulate_batch<MODE, DIFF0, MASK, PREC>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = persistent_grid(kern, smem, ntiles, (flags & WR_LK_CTAS_PER_SM_MASK) >> WR_LK_CTAS_PER_SM_SHIFT);
+  kern<<<grid, kAccThreads, smem, s>>>(b);
+}
+
+template <int MODE, int DIFF0, int PREC>
+static void launch_batch2(const BatchIter& b, long long ntiles, size_t smem, bool mask, int flags, cudaStream_t s) {
+  if (mask) launch_batch1<MODE, DIFF0, true, PREC>(b, ntiles, smem, flags, s);
+  else launch_batch1<MODE, DIFF0, false, PREC>(b, ntiles, smem, flags, s);
+}
+
+template <int PREC>
+static void launch_batch(int mode, int diff0, const BatchIter& b, long long ntiles, size_t smem, bool mask, int flags,
+                         cudaStream_t s) {
+  switch (mode) {
+    case FIELD_CP:
+      switch (diff0) {
+        case FIELD_UP: launch_batch2<FIELD_CP, FIELD_UP, PREC>(b, ntiles, smem, mask, flags, s); break;
+        case FIELD_DENSE: launch_batch2<FIELD_CP, FIELD_DENSE, PREC>(b, ntiles, smem, mask, flags, s); break;
+        case FIELD_ZERO: launch_batch2<FIELD_CP, FIELD_ZERO, PREC>(b, ntiles, smem, mask, flags, s); break;
+        default: launch_batch2<FIELD_CP, kNoDiff, PREC>(b, ntiles, smem, mask, flags, s);
+      }
+      break;
+    case FIELD_UP: launch_batch2<FIELD_UP, kNoDiff, PREC>(b, ntiles, smem, mask, flags, s); break;
+    case FIELD_DENSE: launch_batch2<FIELD_DENSE, kNoDiff, PREC>(b, ntiles, smem, mask, flags, s); break;
+    default: launch_batch2<FIELD_ZERO, kNoDiff, PREC>(b, ntiles, smem, mask, flags, s);
+  }
+}
+
+template <typename T, int PREC>
+static int run_batch(const Plan* plans, const size_t* offs, const WrLKItem* items, int n, const WrLKParams* p,
+                     void* workspace, cudaStream_t s) {
+  void* ws[kMaxBatch];
+  for (int i = 0; i < n; ++i) {
+    ws[i] = static_cast<char*>(workspace) + offs[i];
+    prepare_frame<T, PREC>(plans[i], p, (const T*)items[i].mov.data, (const T*)items[i].ref.data,
+                           items[i].excl_mask_mov, items[i].excl_mask_ref, items[i].motion_init, ws[i], s);
+  }
+  const bool has_init = items[0].motion_init != nullptr;
+  const bool has_mmov = items[0].excl_mask_mov != nullptr;
+  const bool mask = has_mmov || items[0].excl_mask_ref != nullptr;
+  const Plan& P0 = plans[0];
+  const double sps = p->smoothPenalty * (double)((2 * P0.r + 1) * (2 * P0.r + 1));
+  const float sps_f = (float)sps;
+  BatchIter b;
+  BatchDecide bd;
+  BatchUpdate bu;
+  BatchState bs;
+  memset(&b, 0, sizeof(b));
+  memset(&bd, 0, sizeof(bd));
+  memset(&bu, 0, sizeof(bu));
+  memset(&bs, 0, sizeof(bs));
+  b.n = bd.n = bu.n = bs.n = n;
+  b.order = (p->flags & WR_LK_TILE_ORDER_X) ? 1 : 0;
+  for (int l = P0.levels - 1; l >= 0; --l) {
+    int mode0 = FIELD_ZERO;
+    FieldSrc f0[kMaxBatch];
+    long long max_ncp = 1;
+    b.tile_start[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      const LevelPlan& L = plans[i].lv[l];
+      b.item[i] = begin_level(plans[i], l, ws[i], has_init, mask, has_mmov, &mode0, s);
+      f0[i] = b.item[i].field0;
+      b.tile_start[i + 1] = b.tile_start[i] + (int)L.nblk;
+      bd.st[i] = bu.st[i] = bs.st[i] = b.item[i].st;
+      bd.errpart[i] = b.item[i].errpart;
+      bd.penpart[i] = b.item[i].penpart;
+      bd.nblk[i] = L.nblk;
+      bd.n_vox[i] = (double)L.n;
+      bu.cp[i] = at_off<float4>(ws[i], L.cp);
+      bu.sums[i] = b.item[i].sums;
+      bu.ncp[i] = L.ncp;
+      if (L.ncp > max_ncp) max_ncp = L.ncp;
+    }
+    const long long ntiles = b.tile_start[n];
+    const int forced = p->forced_updates[l];
+    const double zratio_d = P0.lv[l].zratio_d;
+    const dim3 ugrid((unsigned)((max_ncp + kThreads - 1) / kThreads), (unsigned)n);
+    for (int it = 0; it < P0.iter; ++it) {
+      const int mode = it == 0 ? mode0 : FIELD_CP;
+      const int diff0 = it == 1 ? mode0 : kNoDiff;
+      for (int i = 0; i < n; ++i) b.item[i].field = it == 0 ? f0[i] : field_src(plans[i], l, FIELD_CP, ws[i]);
+      launch_batch<PREC>(mode, diff0, b, ntiles, accumulate_smem(P0.w, diff0 == FIELD_UP), mask, p->flags, s);
+      if (diff0 != kNoDiff) k_first_post_batch<<<1, 32, 0, s>>>(bs, l, forced);
+      k_decide_batch<<<n, 1024, 0, s>>>(bd, sps, l, it, P0.iter, p->tol, forced);
+      if (PREC == WR_PREC_F32)
+        k_update_batch<false><<<ugrid, kThreads, 0, s>>>(bu, sps, sps_f, (double)p->movRange, zratio_d);
+      else
+        k_update_batch<true><<<ugrid, kThreads, 0, s>>>(bu, sps, sps_f, (double)p->movRange, zratio_d);
+      k_post_batch<<<1, 32, 0, s>>>(bs, l, forced, it == 0 ? 1 : 0);
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    finish_frame<T>(plans[i], ws[i], (const T*)items[i].mov.data, items[i].motion_out, items[i].warped_out,
+                    items[i].stats, s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "wr_lk_register_batch launch");
   return WR_OK;
 }
 
@@ -708,6 +852,76 @@ int wr_lk_workspace_size(int32_t nz, int32_t ny, int32_t nx, const WrLKParams* p
   if (rc) return fail(rc, why);
   *bytes = P.total;
   return WR_OK;
+}
+
+// Plans and workspace offsets of a batch (validates the items; with
+// sizes_only the data and output pointers are not looked at).
+static int batch_plans(const WrLKItem* items, int32_t n, const WrLKParams* p, Plan* plans, size_t* offs,
+                       size_t* total, bool sizes_only) {
+  if (!items || !p) return fail(WR_E_NULL, "items or params is NULL");
+  if (n < 1 || n > WR_MAX_BATCH) return fail(WR_E_PARAM, "batch size must be 1..WR_MAX_BATCH");
+  size_t cur = 0;
+  for (int i = 0; i < n; ++i) {
+    const WrLKItem& it = items[i];
+    int rc;
+    if (sizes_only) {
+      WrVolume m = it.mov, r = it.ref;
+      m.data = r.data = items;   // any non-null address: only shapes and dtypes are checked
+      if ((rc = check_volume(&m, "mov"))) return rc;
+      if ((rc = check_volume(&r, "ref"))) return rc;
+    } else {
+      if ((rc = check_volume(&it.mov, "mov"))) return rc;
+      if ((rc = check_volume(&it.ref, "ref"))) return rc;
+      if (!it.motion_out) return fail(WR_E_NULL, "motion_out is NULL");
+    }
+    if (it.mov.nz != it.ref.nz || it.mov.ny != it.ref.ny || it.mov.nx != it.ref.nx)
+      return fail(WR_E_SHAPE, "mov and ref shapes differ");
+    if (it.mov.dtype != it.ref.dtype || it.mov.dtype != items[0].mov.dtype)
+      return fail(WR_E_DTYPE, "every volume of a batch must have one dtype");
+    if ((it.excl_mask_mov != nullptr) != (items[0].excl_mask_mov != nullptr) ||
+        (it.excl_mask_ref != nullptr) != (items[0].excl_mask_ref != nullptr) ||
+        (it.motion_init != nullptr) != (items[0].motion_init != nullptr))
+      return fail(WR_E_PARAM, "the frames of a batch must agree on which masks and initial fields are given");
+    const char* why;
+    rc = make_plan(it.mov.nz, it.mov.ny, it.mov.nx, p, true, true, true, &plans[i], &why);
+    if (rc) return fail(rc, why);
+    offs[i] = cur;
+    cur = align_up(cur + plans[i].total);
+  }
+  *total = cur;
+  return WR_OK;
+}
+
+int wr_lk_batch_workspace_size(const WrLKItem* items, int32_t n, const WrLKParams* p, size_t* bytes) {
+  if (!bytes) return fail(WR_E_NULL, "bytes is NULL");
+  static thread_local Plan plans[WR_MAX_BATCH];
+  size_t offs[WR_MAX_BATCH];
+  return batch_plans(items, n, p, plans, offs, bytes, true);
+}
+
+int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  static thread_local Plan plans[WR_MAX_BATCH];
+  size_t offs[WR_MAX_BATCH], total = 0;
+  int rc = batch_plans(items, n, p, plans, offs, &total, false);
+  if (rc) return rc;
+  if (!workspace) return fail(WR_E_NULL, "workspace is NULL");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256) return fail(WR_E_WORKSPACE, "workspace must be 256-byte aligned");
+  if (workspace_bytes < total) return fail(WR_E_WORKSPACE, "workspace smaller than wr_lk_batch_workspace_size");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int dtype = items[0].mov.dtype;
+#define WR_BATCH_DISPATCH(PRECV)                                                                        \
+  switch (dtype) {                                                                                      \
+    case WR_U16: return run_batch<uint16_t, PRECV>(plans, offs, items, n, p, workspace, s);             \
+    case WR_U8: return run_batch<uint8_t, PRECV>(plans, offs, items, n, p, workspace, s);               \
+    default: return run_batch<float, PRECV>(plans, offs, items, n, p, workspace, s);                     \
+  }
+  switch (p->precision) {
+    case WR_PREC_F16: WR_BATCH_DISPATCH(WR_PREC_F16)
+    case WR_PREC_BF16: WR_BATCH_DISPATCH(WR_PREC_BF16)
+    default: WR_BATCH_DISPATCH(WR_PREC_F32)
+  }
+#undef WR_BATCH_DISPATCH
 }
 
 int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,

@@ -117,6 +117,17 @@ class LKRegistrar:
         base = self.workspace.data_ptr()
         self._ws_ptr = (base + 255) // 256 * 256
         self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
+        # launch-shape bits of WrLKParams.flags (tile order, CTAs per SM); results do not depend on them
+        self.tune_flags = 0
+
+    def autotune(self, dtype=torch.uint16, mask=True, use_cache=True, report=None) -> int:
+        """Pick the fused kernel's launch shape for this registrar's shape and
+        parameters (``autotune.tune``, cached) and use it from now on."""
+        from . import autotune
+
+        self.tune_flags = autotune.tune(self.shape, self.params, dtype=dtype, mask=mask, device=self.device,
+                                        use_cache=use_cache, report=report)
+        return self.tune_flags
 
     def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
                  motion_init=None, out=None, stream=None, profile=None, reuse_reference=False,
@@ -155,7 +166,7 @@ class LKRegistrar:
             init_ptr = motion_init.data_ptr()
         if out is None:
             out = torch.empty(self.shape + (3,), dtype=torch.float32, device=self.device)
-        self._cp.flags = _lib.WR_LK_REUSE_REFERENCE if reuse_reference else 0
+        self._cp.flags = self.tune_flags | (_lib.WR_LK_REUSE_REFERENCE if reuse_reference else 0)
         args = (ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
                 out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream))
         prof = ctypes.byref(profile.begin_call()) if profile is not None else None
