@@ -222,6 +222,10 @@ def run_ours(args, wl, rank, world, local_rank):
         if keep_stats:
             stats_hist[k].copy_(reg.stats_dev, non_blocking=True)
 
+    tune_report = {}
+    if not args.no_autotune:
+        # launch shape of the fused kernel for this workload (results do not depend on it)
+        reg.autotune(dtype=frames[0].dtype, mask=True, use_cache=False, report=tune_report)
     for k in range(args.warmup):
         step(k)
     torch.cuda.synchronize()
@@ -313,6 +317,9 @@ def run_ours(args, wl, rank, world, local_rank):
         "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
         "clocks": clocks.summary() if clocks else None,
     }
+    res["config"]["autotune"] = {"flags": reg.tune_flags, "ms_per_candidate": tune_report} if tune_report else None
+    if not args.no_batch:
+        res["config"]["batched_small_frames"] = run_batched_small(device)
 
     # learned warm start + float16 levels (the headline path) on the same frames
     ws = None
@@ -338,6 +345,7 @@ def run_ours(args, wl, rank, world, local_rank):
         host_motion = [torch.empty(wl["shape"] + (3,), dtype=torch.float32).pin_memory() for _ in range(2)]
         host_warp = [torch.empty(wl["shape"], dtype=torch.float32).pin_memory() for _ in range(2)]
         series = SeriesRegistrar(template, params, mask_ref=excl, mask_mov=excl)
+        series.reg.tune_flags = reg.tune_flags
         ek = max(4, min(args.steps, 16))
         seq = [host_frames[i % n_host] for i in range(ek)]
         outs_m = [host_motion[i % 2] for i in range(ek)]
@@ -364,6 +372,54 @@ def run_ours(args, wl, rank, world, local_rank):
                       "api": "SeriesRegistrar.run (pinned host frames -> host motion + warped volume)"}
         res["gpu_launches_e2e_per_step"] = launches_per_step
     return res, [updates_sum[l] / args.steps for l in range(levels)]
+
+
+def run_batched_small(device, n=16, reps=3):
+    """Frames small enough to leave most of the GPU idle one by one (the
+    64x256x256 configuration, layer 2, r 16): registration + warp of n frames
+    one call each, and as one batched call replayed from a CUDA graph."""
+    import torch
+
+    from wholistic_registration_b200 import LKParams, LKRegistrar, penalty_factor, synthetic
+    from wholistic_registration_b200.batch import BatchRegistrar
+
+    shape = (64, 256, 256)
+    tmpl, _, _ = synthetic.make_pair(shape, 4242, n_blobs=2000, max_disp=(4.0, 4.0, 1.5), device=device)
+    movs = [synthetic.make_pair(shape, 4300 + k, n_blobs=2000, max_disp=(4.0, 4.0, 1.5), device=device,
+                                template=tmpl.float())[1].contiguous() for k in range(n)]
+    tmpl = tmpl.contiguous()
+    excl = (~synthetic.ellipsoid_inclusion(shape, 0.7, device=device)).to(torch.uint8)
+    factor = float(penalty_factor(tmpl.float().contiguous()))
+    p = LKParams(layer=2, iter=10, r=16, zRatio=1.0, movRange=5.0, smoothPenalty=0.08 * factor, tol=1e-3)
+    reg = LKRegistrar(shape, p, device)
+    motion = torch.empty(shape + (3,), dtype=torch.float32, device=device)
+    warped = torch.empty(shape, dtype=torch.float32, device=device)
+
+    def one_by_one():
+        for k in range(n):
+            reg.register(movs[k], tmpl, excl, excl, out=motion, warped_out=warped, reuse_reference=True)
+
+    br = BatchRegistrar([shape] * n, p, device, warp=True, graph=True)
+    tm, ex = [tmpl] * n, [excl] * n
+    br.register(movs, tm, ex, ex)
+
+    def batched():
+        br.register(movs, tm, ex, ex, reuse_reference=True)
+
+    out = {"frames": n, "shape_zyx": list(shape), "layer": 2, "r": 16}
+    reg.register(movs[0], tmpl, excl, excl, out=motion, warped_out=warped)
+    for name, fn in (("one_call_per_frame", one_by_one), ("batched_cuda_graph", batched)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name + "_volumes_per_s"] = round(n * reps / (e0.elapsed_time(e1) * 1e-3), 2)
+    out["speedup"] = round(out["batched_cuda_graph_volumes_per_s"] / out["one_call_per_frame_volumes_per_s"], 3)
+    return out
 
 
 def run_warmstart(args, wl, template, excl, frames, params, device, world, weights):
@@ -549,6 +605,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-warmstart", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -21,7 +21,7 @@ SRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "_wr_b200.so")
 SOURCES = ["wr_api.cu", "wr_net.cu"]
-DEPS = ["wr_api.cu", "wr_net.cu", "wr_kernels.cuh", "wr_plan.h", "wr_resize_table.cuh"]
+DEPS = ["wr_api.cu", "wr_net.cu", "wr_kernels.cuh", "wr_acc_tile.inc", "wr_plan.h", "wr_resize_table.cuh"]
 
 
 def nvcc_path() -> str:

@@ -427,10 +427,12 @@ static int persistent_grid(K kernel, size_t smem, long long ntiles, int per_sm_c
 
 template <int MODE, int DIFF0, bool MASK, int PREC>
 static void launch_accumulate1(const IterArgs& a, long long ntiles, size_t smem, int flags, cudaStream_t s) {
-  auto kern = k_lk_accumulate<MODE, DIFF0, MASK, PREC>;
+  // the tile order is a template parameter: a run-time order costs the kernel registers
+  auto kern = (flags & WR_LK_TILE_ORDER_X) ? k_lk_accumulate<MODE, DIFF0, MASK, PREC, 1>
+                                           : k_lk_accumulate<MODE, DIFF0, MASK, PREC, 0>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int grid = persistent_grid(kern, smem, ntiles, (flags & WR_LK_CTAS_PER_SM_MASK) >> WR_LK_CTAS_PER_SM_SHIFT);
-  kern<<<grid, kAccThreads, smem, s>>>(a, (flags & WR_LK_TILE_ORDER_X) ? 1 : 0);
+  kern<<<grid, kAccThreads, smem, s>>>(a);
 }
 
 template <int MODE, int DIFF0, int PREC>

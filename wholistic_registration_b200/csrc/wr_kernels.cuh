@@ -1086,207 +1086,6 @@ __device__ __forceinline__ int tile_of(int k, int order, int nz, int ntx, int nt
   return (ty * ntx + tx) * nz + z;
 }
 
-// One tile of the fused iteration (the body of k_lk_accumulate, below):
-// ends with a barrier, after which the shared memory may be refilled.
-template <int MODE, int DIFF0, bool MASK, int PREC>
-__device__ __forceinline__ void accumulate_tile(const IterArgs& a, int tile, const AccSmem& sm, float& dmax) {
-  typedef Store<PREC> S;
-  const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
-  const int w = a.w;
-  const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
-  float4* gsm = sm.gsm;
-  float* it_raw = sm.it_raw;
-  const TileField& tf = sm.tf;
-  int* flags = sm.flags;
-  float* red = sm.red;
-  const TileField& tf0 = sm.tf0;
-  int* flags0 = sm.flags0;
-  const int z = tile % nz, txy = tile / nz;
-  const int ty = txy / a.ntx, tx = txy - ty * a.ntx;
-  const bool window = tx < ncx && ty < ncy;
-  const int x0 = tx * w, y0 = ty * w;
-  const int wx = min(x0 + w, nx) - x0, wy = min(y0 + w, ny) - y0;
-  const int hw = wx + 2, hh = wy + 2;
-  build_tile_field<MODE>(tf, flags, a.field, a.r, w, x0, y0, hw, hh, z, nx, ny);
-  if (DIFF0 == FIELD_UP) build_tile_field<FIELD_UP>(tf0, flags0, a.field0, a.r, w, x0, y0, hw, hh, z, nx, ny);
-  const bool generic = flags[0] != 0;
-
-  const typename S::V4* __restrict__ G = static_cast<const typename S::V4*>(a.mov.g);
-  const typename S::V1* __restrict__ R = static_cast<const typename S::V1*>(a.ref);
-  const uint32_t plane = (uint32_t)nx * (uint32_t)ny;
-  const uint32_t zoff = (uint32_t)z * plane;
-  const int total = hh * hw;
-  const float fz_base = (float)z;
-  int hy = threadIdx.x / hw, hx = threadIdx.x - hy * hw;
-  const int step_y = kAccThreads / hw, step_x = kAccThreads - step_y * hw;
-  for (int h = threadIdx.x; h < total; h += kAccThreads) {
-    const int gx = clampi(x0 - 1 + hx, 0, nx - 1);
-    const int gy = clampi(y0 - 1 + hy, 0, ny - 1);
-    const float3 m = tile_motion<MODE>(tf, generic, a.field, hx, hy, gx, gy, z);
-    const float cx = (float)gx + m.x, cy = (float)gy + m.y, cz = fz_base + m.z;
-    int ix0, iy0, iz0;
-    float fx, fy, fz;
-    split_coord(cx, ix0, fx);
-    split_coord(cy, iy0, fy);
-    split_coord(cz, iz0, fz);
-    const int xa = clampi(ix0, 0, nx - 1), ya = clampi(iy0, 0, ny - 1), za = clampi(iz0, 0, nz - 1);
-    // taps one step up, or the same tap when clamped at the upper face
-    const bool sx = ix0 >= 0 && ix0 < nx - 1, sy = iy0 >= 0 && iy0 < ny - 1, sz = iz0 >= 0 && iz0 < nz - 1;
-    const uint32_t i000 = (uint32_t)za * plane + (uint32_t)ya * nx + (uint32_t)xa;
-    const typename S::V4* p00 = G + i000;
-    const typename S::V4* p01 = sy ? p00 + nx : p00;
-    const typename S::V4* p10 = sz ? p00 + plane : p00;
-    const typename S::V4* p11 = sy ? p10 + nx : p10;
-    float4 c000, c001, c010, c011, c100, c101, c110, c111;
-    c000 = S::load4(p00); c010 = S::load4(p01); c100 = S::load4(p10); c110 = S::load4(p11);
-    if (sx) {
-      c001 = S::load4(p00 + 1); c011 = S::load4(p01 + 1); c101 = S::load4(p10 + 1); c111 = S::load4(p11 + 1);
-    } else {
-      c001 = c000; c011 = c010; c101 = c100; c111 = c110;
-    }
-    // trilinear on (m, Gx) and (Gy, Gz) pairs with paired FP32 FMAs
-    const float2 tx2 = make_float2(fx, fx), ty2 = make_float2(fy, fy), tz2 = make_float2(fz, fz);
-    const float2 ntx2 = make_float2(-fx, -fx), nty2 = make_float2(-fy, -fy), ntz2 = make_float2(-fz, -fz);
-#define WR_LERP2(a, b, t, nt) __ffma2_rn(t, b, __ffma2_rn(nt, a, a))
-    const float2 lo00 = WR_LERP2(make_float2(c000.x, c000.y), make_float2(c001.x, c001.y), tx2, ntx2);
-    const float2 lo01 = WR_LERP2(make_float2(c010.x, c010.y), make_float2(c011.x, c011.y), tx2, ntx2);
-    const float2 lo10 = WR_LERP2(make_float2(c100.x, c100.y), make_float2(c101.x, c101.y), tx2, ntx2);
-    const float2 lo11 = WR_LERP2(make_float2(c110.x, c110.y), make_float2(c111.x, c111.y), tx2, ntx2);
-    const float2 lo = WR_LERP2(WR_LERP2(lo00, lo01, ty2, nty2), WR_LERP2(lo10, lo11, ty2, nty2), tz2, ntz2);
-    const uint32_t p = zoff + (uint32_t)gy * nx + gx;
-    it_raw[h] = S::load1(R + p) - lo.x;
-    if (hx >= 1 && hx <= wx && hy >= 1 && hy <= wy) {
-      const float2 hi00 = WR_LERP2(make_float2(c000.z, c000.w), make_float2(c001.z, c001.w), tx2, ntx2);
-      const float2 hi01 = WR_LERP2(make_float2(c010.z, c010.w), make_float2(c011.z, c011.w), tx2, ntx2);
-      const float2 hi10 = WR_LERP2(make_float2(c100.z, c100.w), make_float2(c101.z, c101.w), tx2, ntx2);
-      const float2 hi11 = WR_LERP2(make_float2(c110.z, c110.w), make_float2(c111.z, c111.w), tx2, ntx2);
-      const float2 hi = WR_LERP2(WR_LERP2(hi00, hi01, ty2, nty2), WR_LERP2(hi10, hi11, ty2, nty2), tz2, ntz2);
-      float gxv = lo.y, gyv = hi.x, gzv = hi.y;
-      if (!(cx >= 1.f && cx <= (float)(nx - 2))) gxv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 0);
-      if (!(cy >= 1.f && cy <= (float)(ny - 2))) gyv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 1);
-      if (!(cz >= 1.f && cz <= (float)(nz - 2))) gzv = clipped_gradient<PREC>(a.mov, cx, cy, cz, 2);
-      float excl = 0.f;
-      if (MASK) {
-        bool ex = (__ldg(a.mbits + p) & 1) != 0;
-        if (!ex && a.mmov) {
-          // the cell code covers exactly this sample's corners when the lower
-          // taps were not clamped
-          int code = 2;
-          if (xa == ix0 && ya == iy0 && za == iz0) code = (__ldg(a.mbits + i000) >> 1) & 3;
-          if (code == 1) ex = true;
-          else if (code == 2) ex = warped_mask_exact(a.mmov, nx, ny, nz, cx, cy, cz);
-        }
-        excl = ex ? 1.f : 0.f;
-      }
-      gsm[(hy - 1) * wx + (hx - 1)] = make_float4(gxv, gyv, gzv, excl);
-      if (DIFF0 != kNoDiff) {
-        const float3 q = tile_motion<DIFF0 == kNoDiff ? FIELD_ZERO : DIFF0>(
-            tf0, DIFF0 == FIELD_UP ? flags0[0] != 0 : false, a.field0, hx, hy, gx, gy, z);
-        dmax = fmaxf(dmax, fmaxf(fmaxf(fabsf(m.x - q.x), fabsf(m.y - q.y)), fabsf(m.z - q.z)));
-      }
-    }
-#undef WR_LERP2
-    hx += step_x;
-    hy += step_y;
-    if (hx >= hw) { hx -= hw; ++hy; }
-  }
-  __syncthreads();
-
-  float acc[10];
-#pragma unroll
-  for (int k = 0; k < 10; ++k) acc[k] = 0.f;
-  const float my_edge = (float)(y0 + w - (ny - 1));
-  const float mx_edge = (float)(x0 + w - (nx - 1));
-  const float inv_zr = (float)(1.0 / (double)a.zratio);
-  {
-    // Threads take column strips (column lx, output rows ly0 .. ly1 - 1);
-    // the 3x3 box is the sum of three horizontal 3-sums carried down the
-    // strip in registers.
-    const int nstrips = max(1, kAccThreads / wx);
-    const int rows_per = (wy + nstrips - 1) / nstrips;
-    for (int c = threadIdx.x; c < nstrips * wx; c += kAccThreads) {
-      const int strip = c / wx, lx = c - strip * wx;
-      const int ly0 = strip * rows_per, ly1 = min(ly0 + rows_per, wy);
-      if (ly0 >= ly1) continue;
-      const float* col = it_raw + lx;
-      float h0 = (col[ly0 * hw] + col[ly0 * hw + 1]) + col[ly0 * hw + 2];
-      float h1 = (col[(ly0 + 1) * hw] + col[(ly0 + 1) * hw + 1]) + col[(ly0 + 1) * hw + 2];
-      for (int ly = ly0; ly < ly1; ++ly) {
-        const float* rp = col + (ly + 2) * hw;
-        const float h2 = (rp[0] + rp[1]) + rp[2];
-        float it = ((h0 + h1) + h2) * (1.f / 9.f);
-        h0 = h1;
-        h1 = h2;
-        float4 g = gsm[ly * wx + lx];
-        if (MASK && g.w != 0.f) { it = 0.f; g.x = 0.f; g.y = 0.f; g.z = 0.f; }
-        acc[9] = fmaf(it, it, acc[9]);
-        if (window) {
-          const float wt = ((x0 + lx == nx - 1) ? mx_edge : 1.f) * ((y0 + ly == ny - 1) ? my_edge : 1.f);
-          const float iz = g.z * inv_zr;
-          const float wgx = wt * g.x, wgy = wt * g.y, wgz = wt * iz;
-          acc[0] = fmaf(wgx, g.x, acc[0]);
-          acc[1] = fmaf(wgx, g.y, acc[1]);
-          acc[2] = fmaf(wgx, iz, acc[2]);
-          acc[3] = fmaf(wgy, g.y, acc[3]);
-          acc[4] = fmaf(wgy, iz, acc[4]);
-          acc[5] = fmaf(wgz, iz, acc[5]);
-          acc[6] = fmaf(wgx, it, acc[6]);
-          acc[7] = fmaf(wgy, it, acc[7]);
-          acc[8] = fmaf(wgz, it, acc[8]);
-        }
-      }
-    }
-  }
-  // warp reduction, then the 8 warps in order
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < 10; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < 10; ++k) red[warp * 12 + k] = acc[k];
-  __syncthreads();
-  const long long blk = tile;
-  const long long cpi = ((long long)z * ncy + ty) * ncx + tx;
-  if (threadIdx.x < 10) {
-    float t = 0.f;
-    for (int q = 0; q < kAccThreads / 32; ++q) t += red[q * 12 + threadIdx.x];
-    if (threadIdx.x == 9) a.errpart[blk] = (double)t;
-    else if (window) a.sums[cpi * 12 + threadIdx.x] = t;
-  } else if (threadIdx.x == 32) {
-    double pen = 0.0;
-    if (window) {
-      // neighbour difference on the CP grid (getNeiDiff with r = 1,
-      // utils/calFlow3d_Wei_v1.py:69-98,488-495): mean of the 8 in-plane
-      // neighbours (edge-replicated) minus the centre, float64 then float32
-      const float4* b = a.cpv.cp + (size_t)z * ncy * ncx;
-      // in CP mode the shared-memory CP tile holds the 3x3 neighbourhood
-      const int ox = flags[2], oy = flags[3];
-      double sx = 0.0, sy = 0.0, sz = 0.0;
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          if (dx == 0 && dy == 0) continue;
-          const int qy = clampi(ty + dy, 0, ncy - 1), qx = clampi(tx + dx, 0, ncx - 1);
-          const float4 v = (MODE == FIELD_CP) ? tf.cpt[(qy - oy) * kTileCP + (qx - ox)] : b[qy * ncx + qx];
-          sx += 0.125 * (double)v.x;
-          sy += 0.125 * (double)v.y;
-          sz += 0.125 * (double)v.z;
-        }
-      const float4 c = (MODE == FIELD_CP) ? tf.cpt[(ty - oy) * kTileCP + (tx - ox)] : b[ty * ncx + tx];
-      const float ndx = (float)(sx - (double)c.x);
-      const float ndy = (float)(sy - (double)c.y);
-      const float ndz = __fmul_rn((float)(sz - (double)c.z), a.zratio);
-      float* o = a.sums + cpi * 12;
-      o[9] = ndx;
-      o[10] = ndy;
-      o[11] = ndz;
-      pen = (double)(ndx * ndx + ndy * ndy + ndz * ndz);
-    }
-    a.penpart[blk] = pen;
-  }
-  __syncthreads();   // shared memory is refilled by the next tile
-}
 
 // Fused LK iteration (utils/calFlow3d_Wei_v1.py:442-588).
 //
@@ -1306,19 +1105,32 @@ __device__ __forceinline__ void accumulate_tile(const IterArgs& a, int tile, con
 // kernel also takes max |motion - initial field| over the tile voxels, where
 // the initial field (DIFF0 = UP / DENSE / ZERO) is not a function of this
 // level's CPs (utils/calFlow3d_Wei_v1.py:641-643), into st->maxdiff_bits.
-template <int MODE, int DIFF0, bool MASK, int PREC>
-__global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a, int order) {
+template <int MODE, int DIFF0, bool MASK, int PREC, int ORDER>
+__global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
+  typedef Store<PREC> S;
   // a level that has stopped leaves its remaining iteration launches empty
   if (!*(volatile const int*)&a.st->active) return;
   extern __shared__ float4 smem4[];
-  const AccSmem sm(smem4, a.w);
+  const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
+  const int w = a.w;
+  const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
+  const AccSmem sm(smem4, w);
+  float4* gsm = sm.gsm;
+  float* it_raw = sm.it_raw;
+  const TileField tf = sm.tf;
+  int* flags = sm.flags;
+  float* red = sm.red;
+  const TileField tf0 = sm.tf0;
+  int* flags0 = sm.flags0;
   float dmax = 0.f;
-  const int ntiles = a.mov.nz * a.ntx * a.nty;
+  const int ntiles = nz * a.ntx * a.nty;
   // persistent CTAs take tiles in turn
-  for (int k = blockIdx.x; k < ntiles; k += gridDim.x)
-    accumulate_tile<MODE, DIFF0, MASK, PREC>(a, tile_of(k, order, a.mov.nz, a.ntx, a.nty), sm, dmax);
+  for (int k = blockIdx.x; k < ntiles; k += gridDim.x) {
+    const int tile = ORDER ? tile_of(k, ORDER, nz, a.ntx, a.nty) : k;
+#include "wr_acc_tile.inc"
+  }
   if (DIFF0 != kNoDiff) {
-    const float mx = block_max(dmax, sm.red);
+    const float mx = block_max(dmax, red);
     if (threadIdx.x == 0 && mx > 0.f) atomicMax(&a.st->maxdiff_bits, __float_as_uint(mx));
   }
 }
@@ -1531,8 +1343,16 @@ __device__ __forceinline__ void flush_max(float& dmax, LKState* st, float* red) 
 
 template <int MODE, int DIFF0, bool MASK, int PREC>
 __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate_batch(const __grid_constant__ BatchIter b) {
+  typedef Store<PREC> S;
   extern __shared__ float4 smem4[];
   const AccSmem sm(smem4, b.item[0].w);   // one patch radius for the batch
+  float4* gsm = sm.gsm;
+  float* it_raw = sm.it_raw;
+  const TileField tf = sm.tf;
+  int* flags = sm.flags;
+  float* red = sm.red;
+  const TileField tf0 = sm.tf0;
+  int* flags0 = sm.flags0;
   float dmax = 0.f;
   int cur = 0;
   for (int k = blockIdx.x; k < b.tile_start[b.n]; k += gridDim.x) {
@@ -1544,8 +1364,11 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate_batch(const __
     }
     const IterArgs& a = b.item[i];
     if (!*(volatile const int*)&a.st->active) continue;
-    accumulate_tile<MODE, DIFF0, MASK, PREC>(a, tile_of(k - b.tile_start[i], b.order, a.mov.nz, a.ntx, a.nty), sm,
-                                             dmax);
+    const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
+    const int w = a.w;
+    const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
+    const int tile = tile_of(k - b.tile_start[i], b.order, nz, a.ntx, a.nty);
+#include "wr_acc_tile.inc"
   }
   if (DIFF0 != kNoDiff) flush_max(dmax, b.item[cur].st, sm.red);
 }
