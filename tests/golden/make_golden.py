@@ -166,13 +166,105 @@ def make_primitive_cases(ref, out_dir):
     print("primitives written")
 
 
+class _RegionProps:
+    def __init__(self, coords):
+        self.coords = coords
+        self.area = len(coords)
+
+
+def _skimage_standin():
+    """scikit-image (>= 0.21, the reference's pyproject.toml:21) is not
+    installed here.  The reference's mask module is run with these stand-ins,
+    which restate the four functions it calls from their documented
+    semantics: binary_erosion = ndimage.binary_erosion(border_value=1),
+    binary_dilation = ndimage.binary_dilation(border_value=0), binary_opening
+    = dilation of the erosion, label(connectivity=ndim) = ndimage.label with a
+    full 3x3x3 structure, regionprops = area and coordinates per label."""
+    from scipy import ndimage
+
+    morph = types.ModuleType("skimage.morphology")
+    measure = types.ModuleType("skimage.measure")
+
+    def binary_erosion(image, footprint):
+        return ndimage.binary_erosion(image, structure=footprint, border_value=1)
+
+    def binary_dilation(image, footprint):
+        return ndimage.binary_dilation(image, structure=footprint, border_value=0)
+
+    def binary_opening(image, footprint):
+        return binary_dilation(binary_erosion(image, footprint), footprint)
+
+    def label(vol, connectivity):
+        st = ndimage.generate_binary_structure(vol.ndim, connectivity)
+        return ndimage.label(vol, structure=st)[0]
+
+    def regionprops(lab):
+        return [_RegionProps(np.argwhere(lab == k)) for k in range(1, int(lab.max()) + 1)]
+
+    morph.binary_dilation, morph.binary_opening = binary_dilation, binary_opening
+    measure.label, measure.regionprops = label, regionprops
+    pkg = types.ModuleType("skimage")
+    pkg.morphology, pkg.measure = morph, measure
+    return {"skimage": pkg, "skimage.morphology": morph, "skimage.measure": measure}
+
+
+# name: (x, y, z) shape, seed, background, outlier blobs, thresFactor, maskRange
+MASK_CASES = {
+    "mask_a": ((66, 70, 6), 11, 100.0, 12, 3.0, (5, 5000)),
+    "mask_b": ((40, 56, 6), 12, 300.0, 6, 2.5, (20, 400)),
+    "mask_c": ((96, 96, 8), 13, 50.0, 30, 4.0, (1, 10 ** 9)),
+}
+
+
+def make_mask_cases(root, out_dir):
+    try:
+        import skimage  # noqa: F401
+    except ImportError:
+        sys.modules.update(_skimage_standin())
+    src = os.path.join(root, "src", "wholistic_registration")
+    if "wholistic_registration" not in sys.modules:
+        pkg = types.ModuleType("wholistic_registration")
+        pkg.__path__ = [src]
+        sys.modules["wholistic_registration"] = pkg
+    mask = importlib.import_module("wholistic_registration.utils.mask")
+    prep = importlib.import_module("wholistic_registration.utils.preprocess")
+    rec = {}
+    for name, (shape, seed, bg, nblob, thres, rng_) in MASK_CASES.items():
+        rng = np.random.default_rng(seed)
+        vol = rng.poisson(bg, size=shape).astype(np.float64)
+        for _ in range(nblob):
+            c = [rng.integers(0, s) for s in shape]
+            rad = rng.integers(1, 4)
+            amp = rng.uniform(3, 20) * np.sqrt(bg) * rng.choice([-1, 1])
+            sl = tuple(slice(max(0, ci - rad), min(s, ci + rad + 1)) for ci, s in zip(c, shape))
+            vol[sl] += amp
+        vol = np.clip(vol, 0, 65535).astype(np.uint16)
+        m = mask.getMask(vol, thres)
+        f = mask.bwareafilt3_wei(m, list(rng_))
+        mu, sg = prep.robust_mean_std(vol.astype(np.float32))
+        rec[f"{name}_vol"] = vol
+        rec[f"{name}_mask"] = m
+        rec[f"{name}_filtered"] = f
+        rec[f"{name}_params"] = np.array([thres, rng_[0], rng_[1]], np.float64)
+        rec[f"{name}_musig"] = np.array([mu, sg], np.float32)
+    np.savez_compressed(os.path.join(out_dir, "masks.npz"), **rec)
+    print("masks written")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", choices=["primitives", "motion", "masks"], default=None)
     args = ap.parse_args()
+    if args.only in (None, "masks"):
+        make_mask_cases(args.ref, HERE)
+    if args.only == "masks":
+        return
     ref = load_reference(args.ref)
-    make_primitive_cases(ref, HERE)
-    make_motion_cases(ref, HERE)
+    if args.only in (None, "primitives"):
+        make_primitive_cases(ref, HERE)
+    if args.only in (None, "motion"):
+        make_motion_cases(ref, HERE)
 
 
 if __name__ == "__main__":

@@ -85,3 +85,21 @@ def test_penalty_factor():
     arrays, meta = load_motion_case("mask_r3_l1_z2")
     f = O.smooth_penalty_norm_factor(arrays["ref"].astype(np.float64), arrays["mask_ref"])
     np.testing.assert_allclose(f, float(arrays["penalty_factor"]), rtol=1e-12)
+
+
+MASK_CASES = ("mask_a", "mask_b", "mask_c")
+
+
+@pytest.mark.parametrize("name", MASK_CASES)
+def test_mask_oracle_matches_reference_fixture(name):
+    from oracle import mask_oracle as M
+
+    d = np.load(os.path.join(GOLDEN, "masks.npz"))
+    vol = d[f"{name}_vol"]
+    thres, lo, hi = d[f"{name}_params"]
+    mu, sg = M.robust_mean_std(vol.astype(np.float32))
+    np.testing.assert_array_equal(np.array([mu, sg], np.float32), d[f"{name}_musig"])
+    m = M.get_mask(vol, float(thres))
+    np.testing.assert_array_equal(m, d[f"{name}_mask"])
+    f, _ = M.bwareafilt3(m, (lo, hi))
+    np.testing.assert_array_equal(f, d[f"{name}_filtered"])

@@ -64,6 +64,10 @@ EXPORTS = (
     "wr_net_masked_sse",
     "wr_net_pool_flow",
     "wr_net_upsample_flow",
+    "wr_mask_last_error",
+    "wr_mask_workspace_size",
+    "wr_get_mask",
+    "wr_bwareafilt3",
 )
 
 
@@ -196,9 +200,11 @@ def load():
         lib.wr_net_masked_sse.argtypes = [vp, ctypes.POINTER(WrVolume), vp, vp, vp]
         lib.wr_net_pool_flow.argtypes = [vp, ci, ci, ci, ci, vp, vp]
         lib.wr_net_upsample_flow.argtypes = [vp, ci, ci, ci, ci, vp, vp]
+        lib.wr_mask_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
+        lib.wr_get_mask.argtypes = [ctypes.POINTER(WrVolume), ctypes.c_double, ctypes.c_double, vp, vp, vp, sz, vp]
+        lib.wr_bwareafilt3.argtypes = [vp, i32, i32, i32, ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, sz, vp]
         for name in EXPORTS:
-            getattr(lib, name).restype = (ctypes.c_char_p if name in ("wr_last_error", "wr_net_last_error")
-                                          else ctypes.c_int)
+            getattr(lib, name).restype = (ctypes.c_char_p if name.endswith("last_error") else ctypes.c_int)
         if lib.wr_abi_version() != 1:
             raise ImportError("wr_b200 ABI version mismatch")
         _lib = lib
@@ -208,7 +214,13 @@ def load():
 def check(fn, code):
     if code != 0:
         lib = load()
-        msg = (lib.wr_net_last_error() if fn.startswith("wr_net") else lib.wr_last_error()).decode(errors="replace")
+        if fn.startswith("wr_net"):
+            raw = lib.wr_net_last_error()
+        elif fn in ("wr_get_mask", "wr_bwareafilt3") or fn.startswith("wr_mask"):
+            raw = lib.wr_mask_last_error()
+        else:
+            raw = lib.wr_last_error()
+        msg = raw.decode(errors="replace")
         if code > 0:
             raise ArgumentError(fn, code, msg)
         raise WrError(fn, code, msg)

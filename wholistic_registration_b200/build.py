@@ -2,10 +2,12 @@
 
     python -m wholistic_registration_b200.build
 
-Compiles ``csrc/wr_api.cu`` (which includes every kernel) with nvcc into
-``wholistic_registration_b200/_wr_b200.so``.  The library exports only the
-plain C ABI declared in ``include/wr_b200.h``; it links the CUDA runtime
-statically, so it needs nothing from torch.
+Compiles ``csrc/wr_api.cu`` (the registration path), ``csrc/wr_net.cu``
+(the warm-start network) and ``csrc/wr_mask.cu`` (outlier masks) with nvcc
+into ``wholistic_registration_b200/_wr_b200.so``.  The library exports only
+the plain C ABI declared in ``include/wr_b200.h``, ``include/wr_net.h`` and
+``include/wr_mask.h``; it links the CUDA runtime statically, so it needs
+nothing from torch.
 """
 
 from __future__ import annotations
@@ -20,8 +22,8 @@ ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "_wr_b200.so")
-SOURCES = ["wr_api.cu", "wr_net.cu"]
-DEPS = ["wr_api.cu", "wr_net.cu", "wr_kernels.cuh", "wr_acc_tile.inc", "wr_plan.h", "wr_resize_table.cuh"]
+SOURCES = ["wr_api.cu", "wr_net.cu", "wr_mask.cu"]
+DEPS = ["wr_api.cu", "wr_net.cu", "wr_mask.cu", "wr_kernels.cuh", "wr_acc_tile.inc", "wr_plan.h", "wr_resize_table.cuh"]
 
 
 def nvcc_path() -> str:
@@ -46,7 +48,7 @@ def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, d) for d in DEPS] + [os.path.join(INCLUDE, h) for h in ("wr_b200.h", "wr_net.h")]
+    deps = [os.path.join(SRC, d) for d in DEPS] + [os.path.join(INCLUDE, h) for h in ("wr_b200.h", "wr_net.h", "wr_mask.h")]
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
