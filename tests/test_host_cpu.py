@@ -38,3 +38,22 @@ def test_flag_bits_match_header():
     assert re.search(r"WR_LK_CTAS_PER_SM_SHIFT = 12", h)
     assert re.search(r"#define WR_MAX_BATCH 32", h)
     assert _lib.WR_LK_TILE_ORDER_X == 1 << 8 and _lib.WR_LK_CTAS_PER_SM(3) == 3 << 12 and _lib.MAX_BATCH == 32
+
+
+def test_wrapper_host_helpers(tmp_path):
+    import numpy as np
+
+    from wholistic_registration_b200.registration import _load_config, _mse, transform
+
+    p = tmp_path / "c.toml"
+    p.write_text('[mask]\nthresFactor = 5\nmaskRange = [5, 4000]\n')
+    assert _load_config(p)["mask"]["maskRange"] == [5, 4000]
+    assert _load_config({"a": 1}) == {"a": 1}
+    a = torch.tensor([1, 5, 65535], dtype=torch.int32).to(torch.uint16)
+    b = torch.tensor([3, 2, 0], dtype=torch.int32).to(torch.uint16)
+    an, bn = a.to(torch.int32).numpy().astype(np.uint16), b.to(torch.int32).numpy().astype(np.uint16)
+    assert _mse(a, b) == float(np.mean((an - bn) ** 2))
+    x = torch.tensor([0.0, 9.0, 99.0], dtype=torch.float64)
+    assert torch.allclose(transform(x, 2, "log10"), 2 * torch.log10(1 + x))
+    with pytest.raises(ValueError):
+        transform(x, 1, "cube")
