@@ -81,12 +81,23 @@ def pick_initial_reference(frames: torch.Tensor, max_corr_frames: int = 20, spat
     cc = cc / (diag[:, None] * diag[None, :])
     ncorr = min(max_corr_frames, T - 1)
     if ncorr < 1:
-        return frames.to(torch.float64).mean(dim=0), torch.arange(T, device=frames.device)
+        idx = torch.arange(T, device=frames.device)
+        return _mean_of(frames, idx), idx
     ccsort = torch.sort(cc, dim=1, descending=True).values
     best = ccsort[:, 1:ncorr + 1].mean(dim=1)
     imax = int(torch.argmax(best).item())
     top = torch.argsort(-cc[imax], stable=True)[:ncorr]
-    return frames[top].to(torch.float64).mean(dim=0), top
+    return _mean_of(frames, top), top
+
+
+def _mean_of(frames, idx):
+    """float64 mean of frames[idx] over the first axis, added in index
+    order as NumPy's axis-0 mean does (one frame converted at a time)."""
+    acc = None
+    for i in idx.tolist():
+        f = frames[int(i)].to(torch.float64)
+        acc = f if acc is None else acc + f
+    return acc / len(idx)
 
 
 def _mse(a, b) -> float:
@@ -129,7 +140,7 @@ def _template(mem, ca, reference_image, config, device):
     if channels["dual_channel"] and ca is None:
         raise ValueError("[ERROR] Calcium image stack shouldn't be empty")
     if channels["dual_channel"] and refer["pick_reference_auto"] and channels["k"] != 0:
-        ca_ref = ca[indsort].to(torch.float64).mean(dim=0)
+        ca_ref = _mean_of(ca, indsort)
         ca_ref_t = transform(ca_ref, channels["k"], channels["function"])
         return membrane_ref.to(torch.float64) + ca_ref_t, ca_ref_t.mean(), ca_ref_t.std(unbiased=False)
     return membrane_ref, None, None
