@@ -33,6 +33,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# DRAM bytes (read + write) per level voxel of one k_lk_accumulate launch, measured with
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a level-0 launch of the
+# 64x512x512 workload (366.7 MB for 16.78 M voxels); the traffic of a launch grows with
+# the voxels it processes, so the bench scales it to its own launches.
+TRAFFIC_BYTES_PER_VOXEL = 21.86
 
 WORKLOADS = {
     # z, y, x, frames, blobs, max displacement (x, y, z), drift, mask coverage, layer, r, iter
@@ -298,7 +303,8 @@ def run_ours(args, wl, rank, world, local_rank):
             "layer": wl["layer"], "r": wl["r"], "iter": wl["iter"],
             "path": {"f32": "plain-fp32", "f16": "plain, levels in float16", "bf16": "plain, levels in bfloat16"}[args.precision],
             "mask": f"ellipsoid inclusion {wl['coverage']}" if wl["coverage"] else "none",
-            "l2": "inputs larger than L2 (each frame 268 MB > 126 MB)",
+            "l2": (f"inputs larger than L2: each frame {n_vox * 2 / 1e6:.0f} MB, its level-0 moving level "
+                   f"(m, Gx, Gy, Gz) {n_vox * 16 / 1e6:.0f} MB, L2 126 MB"),
             "parallelism": f"frames sharded over {world} rank(s), no collective",
             "evals_per_level_mean": [round(evals_sum[l] / args.steps, 2) for l in range(levels)],
             "updates_per_level_mean": [round(updates_sum[l] / args.steps, 2) for l in range(levels)],
@@ -310,7 +316,10 @@ def run_ours(args, wl, rank, world, local_rank):
             "kernel": "k_lk_accumulate (fused warp + It + gradients + window sums)",
             "bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
-            "peak_kind": pk_kind, "traffic": None, "active_launches": active_launches,
+            "peak_kind": pk_kind,
+            "traffic": round(alg_bytes / bpv * TRAFFIC_BYTES_PER_VOXEL / active_launches) if active_launches else None,
+            "traffic_note": "bytes per active launch: ncu-measured DRAM bytes per voxel x voxels per launch",
+            "active_launches": active_launches,
             "active_ms_per_step": round(act_ms / args.steps, 4), "idle_launch_ms_per_step": round(idle_ms / args.steps, 4),
             "bytes_per_voxel": bpv,
         },
