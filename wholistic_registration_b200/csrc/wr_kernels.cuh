@@ -750,33 +750,6 @@ struct VolView {
   int nx, ny, nz;
 };
 
-template <int PREC>
-__device__ __forceinline__ float m_at(const VolView& v, int x, int y, int z) {
-  return Store<PREC>::load_m(static_cast<const typename Store<PREC>::V4*>(v.g) + ((size_t)z * v.ny + y) * v.nx + x);
-}
-
-// Trilinear sample of the m channel at an arbitrary coordinate (map_coordinates
-// order=1, mode="nearest").
-template <int PREC>
-__device__ __forceinline__ float sample_m(const VolView& v, float cx, float cy, float cz) {
-  int x0, y0, z0;
-  float tx, ty, tz;
-  split_coord(cx, x0, tx);
-  split_coord(cy, y0, ty);
-  split_coord(cz, z0, tz);
-  int xa = clampi(x0, 0, v.nx - 1), xb = clampi(x0 + 1, 0, v.nx - 1);
-  int ya = clampi(y0, 0, v.ny - 1), yb = clampi(y0 + 1, 0, v.ny - 1);
-  int za = clampi(z0, 0, v.nz - 1), zb = clampi(z0 + 1, 0, v.nz - 1);
-  float c000 = m_at<PREC>(v, xa, ya, za), c001 = m_at<PREC>(v, xb, ya, za);
-  float c010 = m_at<PREC>(v, xa, yb, za), c011 = m_at<PREC>(v, xb, yb, za);
-  float c100 = m_at<PREC>(v, xa, ya, zb), c101 = m_at<PREC>(v, xb, ya, zb);
-  float c110 = m_at<PREC>(v, xa, yb, zb), c111 = m_at<PREC>(v, xb, yb, zb);
-  float e00 = fmaf(tx, c001 - c000, c000), e01 = fmaf(tx, c011 - c010, c010);
-  float e10 = fmaf(tx, c101 - c100, c100), e11 = fmaf(tx, c111 - c110, c110);
-  float f0 = fmaf(ty, e01 - e00, e00), f1 = fmaf(ty, e11 - e10, e10);
-  return fmaf(tz, f1 - f0, f0);
-}
-
 // float64 trilinear of a float32 volume, cast to float32 (scipy's arithmetic
 // for the warped exclusion mask).
 __device__ __forceinline__ float sample_f64(const float* v, int nx, int ny, int nz, float cx, float cy, float cz) {
@@ -866,23 +839,6 @@ struct IterArgs {
   int r, w, ntx, nty;
   float zratio;
 };
-
-// Central difference of two trilinear samples at c +- e_axis with the shifted
-// coordinate clipped to the volume (utils/calFlow3d_Wei_v1.py:134-206); the
-// general form, used within one voxel of the volume faces.
-template <int PREC>
-__device__ __noinline__ float clipped_gradient(VolView v, float cx, float cy, float cz, int axis) {
-  if (axis == 0) {
-    const float hi = fminf(fmaxf(cx + 1.f, 0.f), (float)(v.nx - 1)), lo = fminf(fmaxf(cx - 1.f, 0.f), (float)(v.nx - 1));
-    return 0.5f * (sample_m<PREC>(v, hi, cy, cz) - sample_m<PREC>(v, lo, cy, cz));
-  }
-  if (axis == 1) {
-    const float hi = fminf(fmaxf(cy + 1.f, 0.f), (float)(v.ny - 1)), lo = fminf(fmaxf(cy - 1.f, 0.f), (float)(v.ny - 1));
-    return 0.5f * (sample_m<PREC>(v, cx, hi, cz) - sample_m<PREC>(v, cx, lo, cz));
-  }
-  const float hi = fminf(fmaxf(cz + 1.f, 0.f), (float)(v.nz - 1)), lo = fminf(fmaxf(cz - 1.f, 0.f), (float)(v.nz - 1));
-  return 0.5f * (sample_m<PREC>(v, cx, cy, hi) - sample_m<PREC>(v, cx, cy, lo));
-}
 
 // warped moving exclusion mask > 0, evaluated exactly (float64 sum, float32 result)
 __device__ __noinline__ bool warped_mask_exact(const float* mmov, int nx, int ny, int nz, float cx, float cy, float cz) {
