@@ -121,6 +121,8 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.ncx = cp_count(L.nx, P.r, P.w);
     L.ncy = cp_count(L.ny, P.r, P.w);
     if (L.ncx < 1 || L.ncy < 1) { *why = "a pyramid level has no control point (volume too small for r)"; return WR_E_NOCP; }
+    // implied by the line above for r >= 1; the iteration kernel's tap pairs rely on it
+    if (L.nx < 3 || L.ny < 3) { *why = "a pyramid level is narrower than 3 voxels"; return WR_E_NOCP; }
     L.ntx = L.ncx + (L.nx > L.ncx * P.w ? 1 : 0);
     L.nty = L.ncy + (L.ny > L.ncy * P.w ? 1 : 0);
     L.n = (long long)L.nx * L.ny * L.nz;

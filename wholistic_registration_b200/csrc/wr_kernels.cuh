@@ -54,15 +54,6 @@ __device__ __forceinline__ void split_coord(float c, int& i0, float& t) {
   i0 = (int)f;
 }
 
-// The same split for callers that clamp the tap afterwards: the device's
-// float -> int conversion saturates out-of-range values (and maps NaN to 0),
-// so no pinning is needed.
-__device__ __forceinline__ void split_coord_fast(float c, int& i0, float& t) {
-  const float f = floorf(c);
-  t = c - f;
-  i0 = __float2int_rz(f);
-}
-
 // Storage of a level's (m, Gx, Gy, Gz) and of the reference level.
 // WR_PREC_F32: float4 / float.  WR_PREC_F16: 4 x half / half holding half
 // the value (so that uint16 data, up to 65535, stays inside the float16
