@@ -57,3 +57,19 @@ def test_wrapper_host_helpers(tmp_path):
     assert torch.allclose(transform(x, 2, "log10"), 2 * torch.log10(1 + x))
     with pytest.raises(ValueError):
         transform(x, 1, "cube")
+
+
+def test_division_multiplier_bound():
+    """The tile-index division of the iteration kernel: m = ceil(2^32 / d)
+    and q = (n * m) >> 32 equal n // d whenever n * d <= 2^32 (the bound the
+    host checks before handing the kernel a multiplier)."""
+    import numpy as np
+
+    rng = np.random.default_rng(7)
+    for d in list(range(2, 300)) + [int(v) for v in rng.integers(300, 1 << 16, size=200)]:
+        m = ((1 << 32) + d - 1) // d
+        nmax = (1 << 32) // d
+        ns = np.concatenate([np.arange(0, min(nmax, 5000)), rng.integers(0, nmax + 1, size=2000),
+                             [nmax, nmax - 1, (nmax // d) * d, (nmax // d) * d - 1]])
+        ns = ns[(ns >= 0) & (ns <= nmax)].astype(object)
+        assert all((int(n) * m) >> 32 == int(n) // d for n in ns), d

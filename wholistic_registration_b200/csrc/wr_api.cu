@@ -554,6 +554,13 @@ static void prepare_frame(const Plan& P, const WrLKParams* p, const T* mov, cons
   if (init) init_field(P, ws, init, s);
 }
 
+// Multiplier of div_magic for divisor d and dividends below nmax: ceil(2^32 / d)
+// when every such dividend n has n * d <= 2^32, else 0 (plain division).
+static uint32_t host_div_magic(long long d, long long nmax) {
+  if (d <= 1 || (nmax - 1) * d > (1LL << 32)) return 0;
+  return (uint32_t)(((1ULL << 32) + (unsigned long long)d - 1) / (unsigned long long)d);
+}
+
 // Start of level l for one frame: control state, initial field, CP values and
 // the fused kernel's arguments (field = the level's initial field; mode0 is
 // returned in *mode0).
@@ -594,6 +601,8 @@ static IterArgs begin_level(const Plan& P, int l, void* ws, bool has_init, bool 
   a.ntx = L.ntx;
   a.nty = L.nty;
   a.zratio = L.zratio;
+  a.nz_magic = host_div_magic(L.nz, L.nblk);
+  a.ntx_magic = host_div_magic(L.ntx, (long long)L.ntx * L.nty);
   a.field = f0;
   a.field0 = f0;
   *mode0 = m0;

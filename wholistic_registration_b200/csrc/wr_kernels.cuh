@@ -815,6 +815,22 @@ __device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float 
                      fmaf(t, b.w - a.w, a.w));
 }
 
+// floor(n / d) by a multiply-high: m = ceil(2^32 / d) gives the exact
+// quotient for every n >= 0 with n * d <= 2^32 (n = qd + r: the product
+// n m / 2^32 exceeds n / d by n e / (d 2^32), e = m d - 2^32 < d, which keeps
+// it below q + 1).  m = 0 marks a divisor without a multiplier (d = 1 or the
+// bound not met); host_div_magic computes m.
+__device__ __forceinline__ int div_magic(int n, int d, uint32_t m) {
+  return m ? (int)__umulhi((uint32_t)n, m) : (d == 1 ? n : n / d);
+}
+
+// floor(n / d) for 0 <= n < 4096 and 1 <= d < 4096: (n + 0.5) / d is at least
+// 0.5 / d away from the integers on either side, far more than the error of
+// the approximate float quotient, so truncating it is exact.
+__device__ __forceinline__ int div_small(int n, int d) {
+  return (int)__fdividef((float)n + 0.5f, (float)d);
+}
+
 struct IterArgs {
   LKState* st;
   const void* __restrict__ ref;        // reference level in the call's storage
@@ -829,6 +845,7 @@ struct IterArgs {
   FieldSrc field0;                     // level's initial field (first-diff launches)
   int r, w, ntx, nty;
   float zratio;
+  uint32_t nz_magic, ntx_magic;        // div_magic multipliers of nz and ntx for the tile indexes
 };
 
 // warped moving exclusion mask > 0, evaluated exactly (float64 sum, float32 result)
@@ -881,16 +898,20 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
   if (threadIdx.x == 0) *generic_flag = 0;
   if (MODE == FIELD_CP) {
     const CPView& g = f.cpv;
-    // CP tile origin: the lowest CP index used by the tile's first column / row
     float t;
-    const int cx0 = cp_factor(clampi(x0 - 1, 0, nx - 1), r, w, g.ncx, t).x;
-    const int cy0 = cp_factor(clampi(y0 - 1, 0, ny - 1), r, w, g.ncy, t).x;
-    if (threadIdx.x == 0) { generic_flag[2] = cx0; generic_flag[3] = cy0; }
-    if (threadIdx.x < kTileCP * kTileCP) {
-      const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
-      tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+    if (threadIdx.x < 32) {
+      // one warp finds the CP tile origin (the lowest CP index used by the
+      // tile's first column / row) and loads the CP tile
+      const int cx0 = cp_factor(clampi(x0 - 1, 0, nx - 1), r, w, g.ncx, t).x;
+      const int cy0 = cp_factor(clampi(y0 - 1, 0, ny - 1), r, w, g.ncy, t).x;
+      if (threadIdx.x == 0) { generic_flag[2] = cx0; generic_flag[3] = cy0; }
+      if (threadIdx.x < kTileCP * kTileCP) {
+        const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
+        tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+      }
     }
     __syncthreads();
+    const int cx0 = generic_flag[2], cy0 = generic_flag[3];
     if (threadIdx.x < hw) {
       const int gx = clampi(x0 - 1 + (int)threadIdx.x, 0, nx - 1);
       const int2 c = cp_factor(gx, r, w, g.ncx, t);
@@ -916,16 +937,21 @@ __device__ void build_tile_field(const TileField& tf, int* generic_flag, const F
     const UpView& u = f.up;
     const CPView& g = u.src;
     float t;
-    // coarse CP origin: lowest CP index reached from the first column / row
-    const int gx0 = clampi(x0 - 1, 0, nx - 1), gy0 = clampi(y0 - 1, 0, ny - 1);
-    int cx0 = cp_factor(u.ix[2 * gx0], r, w, g.ncx, t).x, cy0 = cp_factor(u.iy[2 * gy0], r, w, g.ncy, t).x;
-    if (u.wx[2 * gx0 + 1] != 0.f) cx0 = min(cx0, cp_factor(u.ix[2 * gx0 + 1], r, w, g.ncx, t).x);
-    if (u.wy[2 * gy0 + 1] != 0.f) cy0 = min(cy0, cp_factor(u.iy[2 * gy0 + 1], r, w, g.ncy, t).x);
-    if (threadIdx.x < kTileCP * kTileCP) {
-      const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
-      tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+    if (threadIdx.x < 32) {
+      // one warp finds the coarse CP origin (lowest CP index reached from the
+      // first column / row) and loads the CP tile
+      const int gx0 = clampi(x0 - 1, 0, nx - 1), gy0 = clampi(y0 - 1, 0, ny - 1);
+      int cx0 = cp_factor(u.ix[2 * gx0], r, w, g.ncx, t).x, cy0 = cp_factor(u.iy[2 * gy0], r, w, g.ncy, t).x;
+      if (u.wx[2 * gx0 + 1] != 0.f) cx0 = min(cx0, cp_factor(u.ix[2 * gx0 + 1], r, w, g.ncx, t).x);
+      if (u.wy[2 * gy0 + 1] != 0.f) cy0 = min(cy0, cp_factor(u.iy[2 * gy0 + 1], r, w, g.ncy, t).x);
+      if (threadIdx.x == 0) { generic_flag[2] = cx0; generic_flag[3] = cy0; }
+      if (threadIdx.x < kTileCP * kTileCP) {
+        const int jr = threadIdx.x / kTileCP, jc = threadIdx.x % kTileCP;
+        tf.cpt[threadIdx.x] = g.cp[((size_t)z * g.ncy + min(cy0 + jr, g.ncy - 1)) * g.ncx + min(cx0 + jc, g.ncx - 1)];
+      }
     }
     __syncthreads();
+    const int cx0 = generic_flag[2], cy0 = generic_flag[3];
     if (threadIdx.x < hw) {
       const int gx = clampi(x0 - 1 + (int)threadIdx.x, 0, nx - 1);
       float wv[kTileCP] = {0.f, 0.f, 0.f, 0.f};
