@@ -23,7 +23,12 @@ SRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "_wr_b200.so")
 SOURCES = ["wr_api.cu", "wr_net.cu", "wr_mask.cu"]
-DEPS = ["wr_api.cu", "wr_net.cu", "wr_mask.cu", "wr_kernels.cuh", "wr_acc_tile.inc", "wr_plan.h", "wr_resize_table.cuh"]
+
+
+def _deps() -> list[str]:
+    """Every source and header the library is built from."""
+    out = [os.path.join(SRC, f) for f in sorted(os.listdir(SRC)) if f.endswith((".cu", ".cuh", ".inc", ".h"))]
+    return out + [os.path.join(INCLUDE, f) for f in sorted(os.listdir(INCLUDE)) if f.endswith(".h")]
 
 
 def nvcc_path() -> str:
@@ -48,8 +53,7 @@ def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, d) for d in DEPS] + [os.path.join(INCLUDE, h) for h in ("wr_b200.h", "wr_net.h", "wr_mask.h")]
-    return all(os.path.getmtime(d) <= t for d in deps)
+    return all(os.path.getmtime(d) <= t for d in _deps())
 
 
 def build(force: bool = False, verbose: bool = True) -> str:
