@@ -64,3 +64,23 @@ def option_from_case(arrays, meta):
 def updates_per_layer(arrays, meta):
     """Number of motion updates the reference performed at each layer."""
     return {l: len(arrays[f"layer_{l}/max_diff_motion"]) for l in range(meta["layer"] + 1)}
+
+
+def xres_case_names():
+    import json
+
+    with open(os.path.join(GOLDEN, "xres_cases.json")) as fh:
+        return sorted(json.load(fh))
+
+
+def load_xres_case(name):
+    """(arrays, option) for a golden getMotion_v2 case (wrong-region correction off)."""
+    import json
+
+    with open(os.path.join(GOLDEN, "xres_cases.json")) as fh:
+        meta = json.load(fh)[name]
+    arrays = dict(np.load(os.path.join(GOLDEN, f"xres_{name}.npz")))
+    option = dict(meta)
+    option.update({"mask_ref": arrays["mask_ref"].copy(), "mask_mov": arrays["mask_mov"].copy(),
+                   "motion": arrays.get("motion_init"), "wrong_region_enable": False})
+    return arrays, option

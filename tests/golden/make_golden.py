@@ -251,14 +251,98 @@ def make_mask_cases(root, out_dir):
     print("masks written")
 
 
+# name: mov (x, y, z), ref (x, y, z), zRatio, zRatio_HR, r, layer, iter, tol, smoothPenalty, masks, init
+XRES_CASES = {
+    "xr_small_r3_l1": ((40, 48, 6), (40, 48, 9), 3.0, 2.0, 3, 1, 6, 1e-3, 0.05, False, False),
+    "xr_mask_r2_l1": ((48, 40, 5), (48, 40, 10), 2.0, 1.0, 2, 1, 8, 1e-3, 0.05, True, False),
+    "xr_init_r4_l2": ((64, 56, 4), (64, 56, 8), 4.0, 2.0, 4, 2, 8, 1e-4, 0.02, False, True),
+    "xr_ragged_r3_l2": ((70, 66, 6), (70, 66, 12), 2.5, 1.25, 3, 2, 10, 1e-3, 0.05, True, False),
+    "xr_iter1_r2_l1": ((32, 32, 4), (32, 32, 4), 1.0, 1.0, 2, 1, 1, 1e-3, 0.05, False, False),
+    "xr_refwide_r2_l1": ((40, 40, 5), (48, 44, 10), 2.0, 1.0, 2, 1, 8, 1e-3, 0.05, True, False),
+}
+
+
+def xres_pair(mov_shape, ref_shape, zr, zr_hr, seed):
+    """Moving and reference stacks of one blob field sampled at z spacings zr
+    and zr_hr (physical units per z index), the moving one displaced by a
+    smooth field and Poisson-noised.  (x, y, z) layout, float32."""
+    rng = np.random.default_rng(seed)
+    n_blobs = max(20, mov_shape[0] * mov_shape[1] // 12)
+    zphys = max(mov_shape[2] * zr, ref_shape[2] * zr_hr)
+    cx = rng.uniform(0, max(mov_shape[0], ref_shape[0]), n_blobs)
+    cy = rng.uniform(0, max(mov_shape[1], ref_shape[1]), n_blobs)
+    cz = rng.uniform(0, zphys, n_blobs)
+    amp = rng.uniform(50, 400, n_blobs)
+    sig = rng.uniform(1.5, 3.0, n_blobs)
+
+    def render(shape, zs, dx=0.0, dy=0.0, dz=0.0):
+        X, Y, Z = np.meshgrid(np.arange(shape[0], dtype=np.float64), np.arange(shape[1], dtype=np.float64),
+                              np.arange(shape[2], dtype=np.float64) * zs, indexing="ij")
+        X, Y, Z = X + dx, Y + dy, Z + dz
+        out = np.full(shape, 100.0)
+        for i in range(n_blobs):
+            out += amp[i] * np.exp(-((X - cx[i]) ** 2 + (Y - cy[i]) ** 2 + ((Z - cz[i]) / 1.5) ** 2) / (2 * sig[i] ** 2))
+        return out
+
+    X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in mov_shape], indexing="ij")
+    dx = 1.2 * np.sin(2 * np.pi * Y / 37.0 + 0.3) + 0.5
+    dy = 1.0 * np.cos(2 * np.pi * X / 41.0) - 0.4
+    dz = 0.6 * np.sin(2 * np.pi * (X + Y) / 53.0)
+    ref = render(ref_shape, zr_hr)
+    mov = render(mov_shape, zr, dx, dy, dz)
+    mov = rng.poisson(np.clip(mov, 0, None)).astype(np.float32)
+    ref = rng.poisson(np.clip(ref, 0, None)).astype(np.float32)
+    return mov, ref
+
+
+def make_xres_cases(root, out_dir):
+    src = os.path.join(root, "src", "wholistic_registration")
+    if "wholistic_registration" not in sys.modules:
+        pkg = types.ModuleType("wholistic_registration")
+        pkg.__path__ = [src]
+        sys.modules["wholistic_registration"] = pkg
+    cf = importlib.import_module("wholistic_registration.utils.calFlowCrossResolution")
+    index = {}
+    for i, (name, (ms, rs, zr, zrh, r, layer, it, tol, sp, masks, use_init)) in enumerate(XRES_CASES.items()):
+        mov, ref = xres_pair(ms, rs, zr, zrh, 100 + i)
+        rng = np.random.default_rng(200 + i)
+        mmov = np.zeros(ms, np.uint8)
+        mref = np.zeros(rs, np.uint8)
+        if masks:
+            mmov[: ms[0] // 6, : ms[1] // 5, :] = 1
+            X, Y, Z = np.meshgrid(*[np.arange(n) for n in rs], indexing="ij")
+            mref[((X - 0.7 * rs[0]) / (0.2 * rs[0])) ** 2 + ((Y - 0.6 * rs[1]) / (0.25 * rs[1])) ** 2 < 1] = 1
+        init = None
+        if use_init:
+            X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in ms], indexing="ij")
+            init = np.stack([0.4 * np.sin(X / 9.0), 0.3 * np.cos(Y / 7.0), 0.1 + 0 * Z], -1).astype(np.float32)
+            init += rng.normal(scale=0.05, size=init.shape).astype(np.float32)
+        option = {"mask_ref": mref.copy(), "mask_mov": mmov.copy(), "layer": layer, "iter": it, "r": r,
+                  "zRatio": zr, "zRatio_HR": zrh, "smoothPenalty": sp, "movRange": 5.0, "tol": tol,
+                  "motion": init, "wrong_region_enable": False}
+        phase, motion, sampled = cf.getMotion_v2(mov.copy(), ref.copy(), option)
+        rec = {"mov": mov, "ref": ref, "mask_mov": mmov, "mask_ref": mref, "phase": np.asarray(phase, np.float32),
+               "motion": np.asarray(motion, np.float32), "ref_sampled": np.asarray(sampled, np.float64)}
+        if init is not None:
+            rec["motion_init"] = init
+        np.savez_compressed(os.path.join(out_dir, f"xres_{name}.npz"), **rec)
+        index[name] = {"layer": layer, "iter": it, "r": r, "zRatio": zr, "zRatio_HR": zrh, "tol": tol,
+                       "smoothPenalty": sp, "movRange": 5.0}
+        print(f"{name}: mov {ms} ref {rs} max |motion| {float(np.abs(motion).max()):.3f}")
+    with open(os.path.join(out_dir, "xres_cases.json"), "w") as fh:
+        json.dump(index, fh, indent=1, sort_keys=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["primitives", "motion", "masks"], default=None)
+    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres"], default=None)
     args = ap.parse_args()
     if args.only in (None, "masks"):
         make_mask_cases(args.ref, HERE)
-    if args.only == "masks":
+    if args.only in (None, "xres"):
+        make_xres_cases(args.ref, HERE)
+    if args.only in ("masks", "xres"):
         return
     ref = load_reference(args.ref)
     if args.only in (None, "primitives"):

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_motion_case, motion_case_names, option_from_case
+from conftest import GOLDEN, load_motion_case, load_xres_case, motion_case_names, option_from_case, xres_case_names
 from oracle import lk_oracle as O
 
 PRIM = os.path.join(GOLDEN, "primitives.npz")
@@ -103,3 +103,35 @@ def test_mask_oracle_matches_reference_fixture(name):
     np.testing.assert_array_equal(m, d[f"{name}_mask"])
     f, _ = M.bwareafilt3(m, (lo, hi))
     np.testing.assert_array_equal(f, d[f"{name}_filtered"])
+
+
+@pytest.mark.parametrize("name", xres_case_names())
+def test_xres_oracle_matches_reference(name):
+    """The getMotion_v2 restatement reproduces the reference's run on the
+    same inputs (phase, motion, sampled reference)."""
+    from oracle import xres_oracle as X
+
+    arrays, option = load_xres_case(name)
+    phase, motion, sampled, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], option)
+    np.testing.assert_allclose(motion, arrays["motion"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(phase, arrays["phase"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(sampled, arrays["ref_sampled"], rtol=1e-12, atol=1e-9)
+
+
+def test_xres_spline_restatement_matches_scipy():
+    """Edge padding + recursive cubic B-spline prefilter + 64-tap evaluation
+    (the CUDA path's algorithm) against scipy's map_coordinates(order=3,
+    mode="nearest") for coordinates inside, near and beyond the faces."""
+    from oracle import xres_oracle as X
+
+    rng = np.random.default_rng(3)
+    vol = rng.normal(100.0, 30.0, size=(13, 9, 6))
+    coef = X.bspline_coefficients(vol)
+    # inside and a few voxels beyond the faces the two agree to rounding; more
+    # than the 12-voxel padding beyond a face only the prefilter's start-up at
+    # the padded ends differs, damped by 0.268^12 (relative 1e-7)
+    for lo, hi, tol in ((0.0, 0.0, 1e-11), (-4.0, 4.0, 1e-11), (-40.0, 40.0, 3e-7)):
+        pts = [rng.uniform(lo, n - 1 + hi, 3000) for n in vol.shape]
+        got = X.cubic_sample(coef, *pts)
+        want = X.cubic_sample_scipy(vol, *pts)
+        np.testing.assert_allclose(got, want, rtol=0, atol=tol * np.abs(vol).max())
