@@ -1,0 +1,62 @@
+/*
+ * wr_xres.h - C ABI of the cross-resolution registration (getMotion_v2).
+ *
+ * Replaces the reference entry point (path relative to src/wholistic_registration/)
+ *
+ *   wr_xres_register   utils/calFlowCrossResolution.py:2470-2663
+ *                      getMotion_v2(data_mov, data_ref, option) with
+ *                      option["wrong_region_enable"] = False
+ *
+ * The moving stack lives on the iteration grid, the reference stack on its own
+ * grid (another z spacing, possibly other x / y extents); the reference is
+ * read through its cubic B-spline (map_coordinates order 3, mode "nearest")
+ * at the phase p = (x, y, z zRatio / zRatio_HR) + motion.
+ *
+ * Layouts are the (z, y, x) memory order of the reference's (x, y, z) arrays:
+ * volumes (nz, ny, nx) float32, fields (nz, ny, nx, 3) float32 with component
+ * 0 along x.  All pointers are device pointers on the caller's stream.
+ */
+#ifndef WR_XRES_H
+#define WR_XRES_H
+
+#include "wr_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Workspace bytes for a moving stack (nz, ny, nx) and a reference stack
+ * (nzh, nyh, nxh).  p->precision must be WR_PREC_F32; p->zRatio is the
+ * moving stack's z spacing (option["zRatio"]), zRatio_HR the reference's
+ * (option["zRatio_HR"]).  has_mask_ref: a reference exclusion mask will be
+ * passed (its spline coefficients need room).
+ */
+WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nzh, int32_t nyh, int32_t nxh,
+                                  const WrLKParams* p, float zRatio_HR, int32_t has_mask_ref, size_t* bytes);
+
+/*
+ * getMotion_v2 without the wrong-region correction.
+ *   mov            (nz, ny, nx) float32 moving stack
+ *   ref            (nzh, nyh, nxh) float32 reference stack
+ *   excl_mask_mov  (nz, ny, nx) uint8 or NULL; excl_mask_ref (nzh, nyh, nxh)
+ *                  uint8 or NULL: option["mask_mov"] / ["mask_ref"], values
+ *                  resized per level and excluded where > 0.5
+ *   motion_init    (nz, ny, nx, 3) or NULL: option["motion"]
+ *   p              layer, iter, r, zRatio, smoothPenalty, movRange, tol,
+ *                  forced_updates (replay, -1 = off), flags (launch shape)
+ * Outputs (any may be NULL): phase_out and motion_out (nz, ny, nx, 3),
+ * ref_sampled_out (nz, ny, nx) = the reference's spline at the phase;
+ * stats as for wr_lk_register (device or host-pinned WrLKStats).
+ */
+WR_API int wr_xres_register(const float* mov, int32_t nz, int32_t ny, int32_t nx, const float* ref, int32_t nzh,
+                            int32_t nyh, int32_t nxh, const uint8_t* excl_mask_mov, const uint8_t* excl_mask_ref,
+                            const float* motion_init, const WrLKParams* p, float zRatio_HR, float* phase_out,
+                            float* motion_out, float* ref_sampled_out, WrLKStats* stats, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WR_XRES_H */

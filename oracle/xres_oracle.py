@@ -114,14 +114,18 @@ def cubic_sample(coef, px, py, pz):
     return out
 
 
-def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None):
+def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=None):
     """``getMotion_v2`` with ``wrong_region_enable=False``.
 
     Returns (phase_new float32 (x,y,z,3), motion float32 (x,y,z,3),
     data_ref_sampled float64 (x,y,z), log) where log["layer_l"] holds the
     diffError / penaltyError / currentError lists and the max |motion change|
     of every update.  ``replay_updates`` maps layer -> number of updates to
-    perform, overriding the stopping rules.
+    perform, overriding the stopping rules.  ``window_noise = (seed, rel)``
+    multiplies every window sum by (1 + rel N(0, 1)): a model of
+    single-precision accumulation, used by the tests to measure how far the
+    reference's own result moves under rounding-level changes (it is chaotic
+    where a window is nearly empty or the phase leaves the reference volume).
     """
     mask_ref_full = np.asarray(option["mask_ref"], dtype=np.float32)
     mask_mov_full = np.asarray(option["mask_mov"], dtype=np.float32)
@@ -139,6 +143,7 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None):
     motion = None
     log = {}
     phase_new = ref_sampled = None
+    noise_rng = np.random.default_rng(window_noise[0]) if window_noise is not None else None
 
     for layer in range(n_layer, -1, -1):
         lg = {"diffError": [], "penaltyError": [], "currentError": [], "max_diff_motion": []}
@@ -224,6 +229,9 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None):
                 "zz": gz * gz, "xt": gx * res, "yt": gy * res, "zt": gz * res,
             }
             sums = {k: _window_sums_segmented(v, r, ncx, ncy) for k, v in prods.items()}
+            if window_noise is not None:
+                for k in sums:
+                    sums[k] = sums[k] * (1.0 + window_noise[1] * noise_rng.standard_normal(sums[k].shape))
             v = solve_flow_with_penalty(sums, sps, nei_sum)
             dist = np.maximum(np.sqrt(np.sum(v ** 2, axis=3)) / mov_range, 1.0)
             v = v / dist[..., None]

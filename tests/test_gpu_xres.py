@@ -1,0 +1,120 @@
+"""Cross-resolution registration (getMotion_v2, wrong-region correction off)
+on the GPU against fixtures from the reference's own run and against the
+oracle restatement.
+
+Tolerances: motion and phase within 1e-3 voxel (max abs) wherever the
+reference's own result is stable, the sampled reference within 1e-4 relative
+to its range (float32 spline coefficients and accumulation against the
+reference's float64), and the same number of motion updates per level as the
+reference's run (read from the oracle, which reproduces that run exactly).
+
+"Stable": the cross-resolution scheme is chaotic where a window is nearly
+empty (masks) or the phase leaves the reference volume (the z = 0 slice with
+motion pointing out): there the reference's own motion moves by more than
+1e-3 voxel when its window sums change at the level of single-precision
+rounding.  The oracle measures that spread per voxel (six runs with every
+window sum scaled by 1 + 3e-7 N(0, 1)); the bound is 1e-3 + 3 x spread, and
+at most 0.1 % of the voxels may exceed it.  A 1 % error in zRatio_HR, planted
+in the oracle, breaks the bound in 35-58 % of the voxels of every case.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_xres_case, xres_case_names
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _updates_per_level(log):
+    return {int(k.split("_")[1]): len(v["max_diff_motion"]) for k, v in log.items()}
+
+
+def _reference_spread(arrays, option, motion_ref):
+    """Per-voxel max |motion change| of the oracle when its window sums are
+    perturbed at single-precision rounding level (six seeds)."""
+    from oracle import xres_oracle as X
+
+    spread = np.zeros_like(motion_ref)
+    for seed in range(6):
+        _, m, _, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option), window_noise=(seed, 3e-7))
+        spread = np.maximum(spread, np.abs(m - motion_ref))
+    return spread
+
+
+@pytest.mark.parametrize("name", xres_case_names())
+def test_xres_matches_reference_run(name):
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    arrays, option = load_xres_case(name)
+    phase, motion, sampled = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(option))
+    assert phase.shape == arrays["phase"].shape and motion.shape == arrays["motion"].shape
+    assert phase.dtype == np.float32 and motion.dtype == np.float32 and sampled.dtype == np.float64
+    _, _, _, log = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option))
+    dev_log, _ = C.last_registrar.error_log()
+    want = _updates_per_level(log)
+    got = {int(k.split("_")[1]): len(v["max_diff_motion"]) for k, v in dev_log.items()}
+    assert got == want, f"updates per level {got} vs reference {want}"
+    spread = _reference_spread(arrays, option, arrays["motion"])
+    bound = 1e-3 + 3.0 * spread
+    # the chaotic part stays small (11 % of the voxels in the worst case)
+    assert (3.0 * spread > 1e-3).mean() < 0.15, "the case is ill-conditioned almost everywhere"
+    err_m = np.abs(motion - arrays["motion"])
+    err_p = np.abs(phase - arrays["phase"])
+    assert (err_m > bound).mean() <= 1e-3, f"motion: max excess {float((err_m - bound).max()):.3g}"
+    assert (err_p > bound).mean() <= 1e-3, f"phase: max excess {float((err_p - bound).max()):.3g}"
+    assert float(err_m.max()) < 0.5
+    # the sampled reference: against the fixture where the motion is stable,
+    # and everywhere against the spline evaluated at this run's own phase
+    span = float(np.ptp(arrays["ref_sampled"])) or 1.0
+    stable = (3.0 * spread).max(axis=-1) <= 1e-3
+    np.testing.assert_allclose(sampled[stable], arrays["ref_sampled"][stable], rtol=0, atol=1e-4 * span)
+    own = X.cubic_sample_scipy(arrays["ref"].astype(np.float64), phase[..., 0], phase[..., 1], phase[..., 2])
+    np.testing.assert_allclose(sampled, own, rtol=0, atol=1e-4 * span)
+
+
+def test_xres_errors_follow_reference_log():
+    """Per-iteration diff / penalty errors of the device run track the
+    reference's (oracle) log within float32 accumulation error."""
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    arrays, option = load_xres_case("xr_mask_r2_l1")
+    C.getMotion_v2(arrays["mov"], arrays["ref"], dict(option))
+    dev_log, _ = C.last_registrar.error_log()
+    _, _, _, log = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option))
+    for layer, lv in log.items():
+        d = dev_log[layer]
+        assert len(d["diffError"]) == len(lv["diffError"])
+        np.testing.assert_allclose(d["diffError"], lv["diffError"], rtol=2e-4)
+        np.testing.assert_allclose(d["penaltyError"], lv["penaltyError"], rtol=2e-3, atol=1e-9)
+
+
+def test_xres_torch_inputs_stay_on_device():
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    arrays, option = load_xres_case("xr_small_r3_l1")
+    mov = torch.from_numpy(arrays["mov"]).cuda()
+    ref = torch.from_numpy(arrays["ref"]).cuda()
+    phase, motion, sampled = C.getMotion_v2(mov, ref, dict(option))
+    assert phase.is_cuda and motion.is_cuda and sampled.is_cuda
+    np.testing.assert_allclose(motion.cpu().numpy(), arrays["motion"], rtol=0, atol=1e-3)
+
+
+def test_xres_rejects_unbuilt_options():
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    arrays, option = load_xres_case("xr_small_r3_l1")
+    opt = dict(option)
+    opt["wrong_region_enable"] = True
+    with pytest.raises(NotImplementedError):
+        C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
+    opt = dict(option)
+    opt["phase"] = np.zeros(arrays["mov"].shape + (3,), np.float32)
+    with pytest.raises(NotImplementedError):
+        C.getMotion_v2(arrays["mov"], arrays["ref"], opt)

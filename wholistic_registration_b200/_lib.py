@@ -1,4 +1,4 @@
-"""ctypes binding of the C ABI in ``include/wr_b200.h``.
+"""ctypes binding of the C ABI in ``include/wr_b200.h`` (and ``wr_net.h``, ``wr_mask.h``, ``wr_xres.h``).
 
 The shared library ``_wr_b200.so`` is built in-tree by
 ``wholistic_registration_b200.build``.  Loading fails loudly when it is
@@ -68,6 +68,8 @@ EXPORTS = (
     "wr_mask_workspace_size",
     "wr_get_mask",
     "wr_bwareafilt3",
+    "wr_xres_workspace_size",
+    "wr_xres_register",
 )
 
 
@@ -203,6 +205,11 @@ def load():
         lib.wr_mask_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
         lib.wr_get_mask.argtypes = [ctypes.POINTER(WrVolume), ctypes.c_double, ctypes.c_double, vp, vp, vp, sz, vp]
         lib.wr_bwareafilt3.argtypes = [vp, i32, i32, i32, ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, sz, vp]
+        P = ctypes.POINTER(WrLKParams)
+        lib.wr_xres_workspace_size.argtypes = [i32, i32, i32, i32, i32, i32, P, ctypes.c_float, i32,
+                                               ctypes.POINTER(sz)]
+        lib.wr_xres_register.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, vp, P, ctypes.c_float,
+                                         vp, vp, vp, vp, vp, sz, vp]
         for name in EXPORTS:
             getattr(lib, name).restype = (ctypes.c_char_p if name.endswith("last_error") else ctypes.c_int)
         if lib.wr_abi_version() != 1:

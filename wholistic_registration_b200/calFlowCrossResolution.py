@@ -1,0 +1,203 @@
+"""Drop-in replacement for the reference's cross-resolution entry point.
+
+``getMotion_v2(data_mov, data_ref, option, verbose=False)`` keeps the
+signature, option keys, array layout and return values of
+``utils/calFlowCrossResolution.py:2470-2663``: the moving stack (x, y, z) and a
+reference stack (x_hr, y_hr, z_hr) sampled with another z spacing
+(``zRatio`` / ``zRatio_HR``: physical units per z index), registered by the
+pyramid patch-wise Lucas-Kanade scheme with the reference read through its
+cubic B-spline at the phase (x, y, z zRatio / zRatio_HR) + motion.  It
+returns ``(phase_new, motion_current, data_ref_sampled)``: two (x, y, z, 3)
+float32 fields and the reference sampled at the phase (float64, as the
+reference returns it).
+
+Every computation runs on the GPU through the sm_100a library
+(``wr_xres_register``); the call raises if the library or a CUDA device is
+missing.  NumPy inputs give NumPy outputs; CUDA torch tensors in the same
+(x, y, z) layout give CUDA tensors.
+
+Not built here: the wrong-region correction the reference runs by default
+(``wrong_region_enable=True``: bad-region detection on the CP errors, a trap
+mask in reference space and two re-runs, :2240-2467) and an initial
+``option["phase"]``; both raise ``NotImplementedError`` instead of silently
+computing something else.  One optional key extends the options:
+``forced_updates`` (layer -> number of motion updates, replaying another
+run's iteration counts).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .registrar import LKParams, _stream_ptr, stats_to_log
+
+__all__ = ["getMotion_v2", "XresRegistrar"]
+
+
+class XresRegistrar:
+    """Cross-resolution registration of a (z, y, x) moving stack onto a
+    (zh, yh, xh) reference stack on one GPU (``wr_xres_register``)."""
+
+    def __init__(self, shape_zyx, ref_shape_zyx, params: LKParams, zRatio_HR: float, has_mask_ref: bool = True,
+                 device=None):
+        self.lib = _lib.load()
+        self.shape = tuple(int(s) for s in shape_zyx)
+        self.ref_shape = tuple(int(s) for s in ref_shape_zyx)
+        self.params = params
+        self.zRatio_HR = float(zRatio_HR)
+        self.has_mask_ref = bool(has_mask_ref)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self._cp = params.to_c()
+        nbytes = ctypes.c_size_t(0)
+        _lib.check("wr_xres_workspace_size",
+                   self.lib.wr_xres_workspace_size(*self.shape, *self.ref_shape, ctypes.byref(self._cp),
+                                                   self.zRatio_HR, int(self.has_mask_ref), ctypes.byref(nbytes)))
+        self.workspace_bytes = int(nbytes.value)
+        self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
+        self._ws_ptr = (self.workspace.data_ptr() + 255) // 256 * 256
+        self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
+
+    @staticmethod
+    def _check(t, name, shape, dtypes):
+        if t is None:
+            return None
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous CUDA tensor")
+        if tuple(t.shape) != tuple(shape) or t.dtype not in dtypes:
+            raise ValueError(f"{name} must be {tuple(shape)} of {dtypes}")
+        return t.data_ptr()
+
+    def register(self, mov, ref, mask_mov=None, mask_ref=None, motion_init=None, phase_out=None, motion_out=None,
+                 sampled_out=None, stream=None):
+        """(phase, motion, sampled) as (z, y, x, 3), (z, y, x, 3), (z, y, x) float32 tensors."""
+        if mask_ref is not None and not self.has_mask_ref:
+            raise ValueError("this registrar was built without room for a reference mask")
+        pm = self._check(mov, "mov", self.shape, (torch.float32,))
+        pr = self._check(ref, "ref", self.ref_shape, (torch.float32,))
+        if mask_mov is not None and mask_mov.dtype == torch.bool:
+            mask_mov = mask_mov.view(torch.uint8)
+        if mask_ref is not None and mask_ref.dtype == torch.bool:
+            mask_ref = mask_ref.view(torch.uint8)
+        pmm = self._check(mask_mov, "mask_mov", self.shape, (torch.uint8,))
+        pmr = self._check(mask_ref, "mask_ref", self.ref_shape, (torch.uint8,))
+        pin = self._check(motion_init, "motion_init", self.shape + (3,), (torch.float32,))
+        new = lambda shp: torch.empty(shp, dtype=torch.float32, device=self.device)  # noqa: E731
+        phase_out = new(self.shape + (3,)) if phase_out is None else phase_out
+        motion_out = new(self.shape + (3,)) if motion_out is None else motion_out
+        sampled_out = new(self.shape) if sampled_out is None else sampled_out
+        for t, name, shp in ((phase_out, "phase_out", self.shape + (3,)), (motion_out, "motion_out", self.shape + (3,)),
+                             (sampled_out, "sampled_out", self.shape)):
+            self._check(t, name, shp, (torch.float32,))
+        _lib.check("wr_xres_register",
+                   self.lib.wr_xres_register(pm, *self.shape, pr, *self.ref_shape, pmm, pmr, pin,
+                                             ctypes.byref(self._cp), self.zRatio_HR, phase_out.data_ptr(),
+                                             motion_out.data_ptr(), sampled_out.data_ptr(), self.stats_dev.data_ptr(),
+                                             self._ws_ptr, self.workspace_bytes, _stream_ptr(stream)))
+        return phase_out, motion_out, sampled_out
+
+    def stats(self) -> _lib.WrLKStats:
+        return _lib.WrLKStats.from_buffer_copy(self.stats_dev.cpu().numpy().tobytes())
+
+    def error_log(self):
+        return stats_to_log(self.stats(), self.params.layer + 1)
+
+
+def _to_device(a, device, dtype):
+    """(x, y, z[, 3]) array -> contiguous (z, y, x[, 3]) CUDA tensor."""
+    if isinstance(a, torch.Tensor):
+        t = a.to(device=device, dtype=dtype)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a).astype(np.float32 if dtype == torch.float32 else
+                                                                       np.float64, copy=False))).to(device)
+        t = t.to(dtype)
+    perm = (2, 1, 0, 3) if t.dim() == 4 else (2, 1, 0)
+    return t.permute(*perm).contiguous()
+
+
+def _mask_to_device(m, shape_xyz, device):
+    """Exclusion mask (x, y, z) -> (z, y, x) uint8 CUDA tensor, or None for
+    an all-zero / scalar-zero mask.  Values are kept (the reference resizes
+    the float32 cast of the mask and thresholds it at 0.5)."""
+    if m is None or np.isscalar(m) or (hasattr(m, "ndim") and m.ndim == 0):
+        if m is not None and float(np.asarray(m)) > 0.5:
+            raise ValueError("a scalar exclusion mask must be 0")
+        return None
+    if isinstance(m, torch.Tensor):
+        t = m.to(device)
+        if tuple(t.shape) != tuple(shape_xyz):
+            raise ValueError(f"mask shape {tuple(t.shape)} does not match the volume {tuple(shape_xyz)}")
+        vals = t
+    else:
+        a = np.asarray(m)
+        if tuple(a.shape) != tuple(shape_xyz):
+            raise ValueError(f"mask shape {a.shape} does not match the volume {tuple(shape_xyz)}")
+        vals = torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    if vals.dtype == torch.bool:
+        vals = vals.to(torch.uint8)
+    if vals.dtype != torch.uint8:
+        f = vals.to(torch.float32)
+        if bool(((f != 0) & (f != 1)).any()):
+            raise ValueError("exclusion masks must hold 0/1 (or bool) values")
+        vals = f.to(torch.uint8)
+    return vals.permute(2, 1, 0).contiguous()
+
+
+_cache: dict = {}
+last_registrar = None   # the XresRegistrar of the latest getMotion_v2 call (its error_log / stats)
+
+
+def getMotion_v2(data_mov, data_ref, option, verbose=False):
+    """Cross-resolution registration (utils/calFlowCrossResolution.py:2470-2663).
+
+    Returns (phase_new, motion_current, data_ref_sampled) in the reference's
+    (x, y, z[, 3]) layout.
+    """
+    if bool(option.get("wrong_region_enable", True)):
+        raise NotImplementedError("the wrong-region correction of getMotion_v2 is not built on this path; "
+                                  "pass option['wrong_region_enable'] = False")
+    if option.get("phase") is not None:
+        raise NotImplementedError("an initial option['phase'] is not supported on this path")
+    as_torch = isinstance(data_mov, torch.Tensor)
+    device = data_mov.device if as_torch and data_mov.is_cuda else torch.device("cuda", torch.cuda.current_device())
+    mov = _to_device(data_mov, device, torch.float32)
+    ref = _to_device(data_ref, device, torch.float32)
+    shape_xyz = tuple(mov.shape[::-1])
+    ref_xyz = tuple(ref.shape[::-1])
+    mask_mov = _mask_to_device(option["mask_mov"], shape_xyz, device)
+    mask_ref = _mask_to_device(option["mask_ref"], ref_xyz, device)
+    init = option.get("motion")
+    init_t = None if init is None else _to_device(init, device, torch.float32)
+    params = LKParams(
+        layer=int(option["layer"]), iter=int(option["iter"]), r=int(option["r"]),
+        zRatio=float(option.get("zRatio", 1.0)), movRange=float(option.get("movRange", 5.0)),
+        smoothPenalty=float(option["smoothPenalty"]), tol=float(option.get("tol", 1e-3)),
+        forced_updates=dict(option.get("forced_updates") or {}))
+    zr_hr = float(option["zRatio_HR"])
+    key = (tuple(mov.shape), tuple(ref.shape), params.layer, params.iter, params.r, params.zRatio, params.movRange,
+           params.smoothPenalty, params.tol, tuple(sorted(params.forced_updates.items())), zr_hr,
+           mask_ref is not None, str(device))
+    reg = _cache.get(key)
+    if reg is None:
+        if len(_cache) > 4:
+            _cache.clear()
+        reg = XresRegistrar(tuple(mov.shape), tuple(ref.shape), params, zr_hr, mask_ref is not None, device)
+        _cache[key] = reg
+    global last_registrar
+    last_registrar = reg
+    phase, motion, sampled = reg.register(mov, ref, mask_mov, mask_ref, init_t)
+    if verbose:
+        log, err = reg.error_log()
+        for name, lv in log.items():
+            for i, (d, p) in enumerate(zip(lv["diffError"], lv["penaltyError"])):
+                print(f"[{name}] iter={i:02d} error={d + p:.4f} diff={d:.4f} penalty={p:.4f}")
+    phase = phase.permute(2, 1, 0, 3)
+    motion = motion.permute(2, 1, 0, 3)
+    sampled = sampled.permute(2, 1, 0).to(torch.float64)
+    if as_torch:
+        return phase.contiguous(), motion.contiguous(), sampled.contiguous()
+    return (np.ascontiguousarray(phase.cpu().numpy()), np.ascontiguousarray(motion.cpu().numpy()),
+            np.ascontiguousarray(sampled.cpu().numpy()))

@@ -14,6 +14,9 @@
 #include "wr_b200.h"
 #include "wr_kernels.cuh"
 #include "wr_plan.h"
+#include "wr_xres.cuh"
+#include "wr_xres.h"
+#include <cmath>
 
 namespace wr {
 
@@ -659,7 +662,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
       launch_accumulate<PREC>(mode, diff0, a, L.nblk, smem, mask, p->flags, s);
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_end[recorded++], s);
-      if (diff0 != kNoDiff) k_first_post<<<1, 1, 0, s>>>(st, l, forced);
+      if (diff0 != kNoDiff) k_first_post<<<1, 1, 0, s>>>(st, l, forced, kMotionTol);
       k_decide<<<1, 1024, 0, s>>>(st, a.errpart, a.penpart, L.nblk, (double)L.n, sps, l, it, P.iter, p->tol, forced);
       if (PREC == WR_PREC_F32)
         k_update<false><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
@@ -667,7 +670,7 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
       else
         k_update<true><<<grid_for(L.ncp), kThreads, 0, s>>>(st, at_off<float4>(ws, L.cp), a.sums, L.ncp, sps, sps_f,
                                                              (double)p->movRange, L.zratio_d);
-      k_post<<<1, 1, 0, s>>>(st, l, forced, it == 0 ? 1 : 0);
+      k_post<<<1, 1, 0, s>>>(st, l, forced, it == 0 ? 1 : 0, kMotionTol);
     }
   }
   finish_frame<T>(P, ws, mov, out, warped, stats, s);
@@ -850,6 +853,8 @@ static int check_volume(const WrVolume* v, const char* name) {
 }  // namespace wr
 
 using namespace wr;
+
+#include "wr_xres_host.inc"
 
 extern "C" {
 

@@ -1121,6 +1121,10 @@ __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate(IterArgs a) {
 // error evaluation and stopping rules (utils/calFlow3d_Wei_v1.py:101-131,501-530)
 // ---------------------------------------------------------------------------
 
+// F32HIST: the error history is a float32 array compared with the new
+// error as NumPy does for a Python float (cast to float32 first), the
+// cross-resolution rule (utils/calFlowCrossResolution.py:2093,2140-2152).
+template <bool F32HIST = false>
 __device__ __forceinline__ void decide_body(LKState* st, const double* __restrict__ errpart,
                                             const double* __restrict__ penpart, long long nblk, double n_vox,
                                             double sps, int level, int it, int iter, double tol, int forced) {
@@ -1159,14 +1163,22 @@ __device__ __forceinline__ void decide_body(LKState* st, const double* __restric
   } else if (it == iter - 1) {
     stop = true;
   } else {
-    int n_le = (st->old_err[0] <= cur) + (st->old_err[1] <= cur) + (st->old_err[2] <= cur);
-    if (n_le > 1) stop = true;
-    else if (fabs(st->old_err[2] - cur) < tol) stop = true;
-    else {
-      stop = false;
+    if (F32HIST) {
+      const float cf = (float)cur;
+      const int n_le = ((float)st->old_err[0] <= cf) + ((float)st->old_err[1] <= cf) + ((float)st->old_err[2] <= cf);
+      if (n_le > 1) stop = true;
+      else if (fabsf(__fsub_rn((float)st->old_err[2], cf)) < (float)tol) stop = true;
+      else stop = false;
+    } else {
+      const int n_le = (st->old_err[0] <= cur) + (st->old_err[1] <= cur) + (st->old_err[2] <= cur);
+      if (n_le > 1) stop = true;
+      else if (fabs(st->old_err[2] - cur) < tol) stop = true;
+      else stop = false;
+    }
+    if (!stop) {
       st->old_err[0] = st->old_err[1];
       st->old_err[1] = st->old_err[2];
-      st->old_err[2] = cur;
+      st->old_err[2] = F32HIST ? (double)(float)cur : cur;
     }
   }
   if (stop) {
@@ -1181,6 +1193,12 @@ __global__ void k_decide(LKState* st, const double* __restrict__ errpart, const 
                          long long nblk, double n_vox, double sps, int level, int it, int iter, double tol,
                          int forced) {
   decide_body(st, errpart, penpart, nblk, n_vox, sps, level, it, iter, tol, forced);
+}
+
+__global__ void k_decide_f32hist(LKState* st, const double* __restrict__ errpart, const double* __restrict__ penpart,
+                                 long long nblk, double n_vox, double sps, int level, int it, int iter, double tol,
+                                 int forced) {
+  decide_body<true>(st, errpart, penpart, nblk, n_vox, sps, level, it, iter, tol, forced);
 }
 
 // ---------------------------------------------------------------------------
@@ -1268,11 +1286,17 @@ __global__ void __launch_bounds__(kThreads) k_update(LKState* st, float4* cp, co
 }
 
 
-// after an update: log max |delta motion| and apply the 1e-3 rule
+// getMotion stops a level once an update moves no voxel by 1e-3 or more
+// (utils/calFlow3d_Wei_v1.py:641-654); the float32 maximum compared with the
+// float32 threshold gives the same decisions as the float64 comparison.
+constexpr float kMotionTol = 1e-3f;
+
+// after an update: log max |delta motion| and stop the level when it is below
+// md_tol (kMotionTol for getMotion, tol for the cross-resolution path)
 // (utils/calFlow3d_Wei_v1.py:641-654).  defer: the level's first update,
 // whose max over the voxels the next iteration's launch completes
 // (k_first_post).
-__device__ __forceinline__ void k_post_body(LKState* st, int level, int forced, int defer) {
+__device__ __forceinline__ void k_post_body(LKState* st, int level, int forced, int defer, float md_tol) {
   if (!st->do_update) return;
   WrLKStats& S = st->stats;
   const int u = st->n_updates;
@@ -1282,25 +1306,29 @@ __device__ __forceinline__ void k_post_body(LKState* st, int level, int forced, 
   if (defer) return;
   const float md = __uint_as_float(st->maxdiff_bits);
   if (u < WR_MAX_ITERS) S.max_diff_motion[level][u] = (double)md;
-  if (forced < 0 && (double)md < 1e-3) st->active = 0;
+  if (forced < 0 && md < md_tol) st->active = 0;
   st->maxdiff_bits = 0u;
 }
 
-__global__ void k_post(LKState* st, int level, int forced, int defer) { k_post_body(st, level, forced, defer); }
+__global__ void k_post(LKState* st, int level, int forced, int defer, float md_tol) {
+  k_post_body(st, level, forced, defer, md_tol);
+}
 
 // The level's first update, once the following launch has added max
-// |new - initial| over the voxels: log it and apply the 1e-3 rule.  A level
+// |new - initial| over the voxels: log it and apply the md_tol rule.  A level
 // that stops here discards that launch's error and sums (k_decide and
 // k_update skip an inactive level).
-__device__ __forceinline__ void k_first_post_body(LKState* st, int level, int forced) {
+__device__ __forceinline__ void k_first_post_body(LKState* st, int level, int forced, float md_tol) {
   if (!st->active) return;
   const float md = __uint_as_float(st->maxdiff_bits);
   st->stats.max_diff_motion[level][0] = (double)md;
-  if (forced < 0 && (double)md < 1e-3) st->active = 0;
+  if (forced < 0 && md < md_tol) st->active = 0;
   st->maxdiff_bits = 0u;
 }
 
-__global__ void k_first_post(LKState* st, int level, int forced) { k_first_post_body(st, level, forced); }
+__global__ void k_first_post(LKState* st, int level, int forced, float md_tol) {
+  k_first_post_body(st, level, forced, md_tol);
+}
 
 // ---------------------------------------------------------------------------
 // batched registration: the frames of a batch (shapes may differ) advance
@@ -1395,11 +1423,11 @@ struct BatchState {
 
 // one thread per frame
 __global__ void k_post_batch(const __grid_constant__ BatchState b, int level, int forced, int defer) {
-  if (threadIdx.x < b.n) k_post_body(b.st[threadIdx.x], level, forced, defer);
+  if (threadIdx.x < b.n) k_post_body(b.st[threadIdx.x], level, forced, defer, kMotionTol);
 }
 
 __global__ void k_first_post_batch(const __grid_constant__ BatchState b, int level, int forced) {
-  if (threadIdx.x < b.n) k_first_post_body(b.st[threadIdx.x], level, forced);
+  if (threadIdx.x < b.n) k_first_post_body(b.st[threadIdx.x], level, forced, kMotionTol);
 }
 
 __global__ void k_level_begin(LKState* st, int level, int first) {
