@@ -33,28 +33,134 @@ __global__ void k_spline_pad(const T* __restrict__ in, double* __restrict__ out,
   }
 }
 
-// Cubic B-spline prefilter of independent lines, in place: gain 6, causal
-// then anti-causal recursion with the pole sqrt(3) - 2 (Unser's recursive
-// filter), both started as if the line continued with its end values.  Line
-// i starts at (i % na) * sa + (i / na) * sb and has n elements `stride` apart.
-__global__ void k_spline_lines(double* __restrict__ c, long long nlines, int n, long long stride, long long na,
-                               long long sa, long long sb) {
-  const double z = -0.26794919243112270;   // sqrt(3) - 2
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= nlines) return;
-  double* p = c + (i % na) * sa + (i / na) * sb;
-  const double s_end = 6.0 * p[(long long)(n - 1) * stride];
-  double prev = 6.0 * p[0] / (1.0 - z);
-  p[0] = prev;
-  for (int k = 1; k < n; ++k) {
-    prev = 6.0 * p[(long long)k * stride] + z * prev;
-    p[(long long)k * stride] = prev;
+// Cubic B-spline prefilter (Unser's recursive filter): gain 6, a causal
+// recursion c+[k] = 6 s[k] + z c+[k-1] and an anti-causal one
+// c-[k] = z (c-[k+1] - c+[k]) with the pole z = sqrt(3) - 2, both started as
+// if the line continued with its end values:
+//   c+[0] = 6 s[0] / (1 - z),
+//   c-[n-1] = -z (6 s[n-1] / (1 - z)^2 + (c+[n-1] - 6 s[n-1] / (1 - z)) / (1 - z^2)).
+constexpr double kSplineZ = -0.26794919243112270;   // sqrt(3) - 2
+
+__device__ __forceinline__ double spline_tail(double c_last, double s_end6) {
+  const double z = kSplineZ;
+  return -z * (s_end6 / ((1.0 - z) * (1.0 - z)) + (c_last - s_end6 / (1.0 - z)) / (1.0 - z * z));
+}
+
+// x lines (contiguous rows of n), one warp per row, in place: both
+// recursions as warp scans of 32-element chunks (c_l = u_l + z c_{l-1} by
+// five shuffle steps, then the carry of the previous chunk times z^(l+1)).
+__global__ void k_spline_rows(double* __restrict__ c, long long nrows, int n) {
+  const double z = kSplineZ;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;   // whole warps leave together
+  double* p = c + row * (long long)n;
+  double zl = z;              // z^(lane + 1)
+  for (int i = 0; i < lane; ++i) zl *= z;
+  const double z2 = z * z, z4 = z2 * z2, z8 = z4 * z4, z16 = z8 * z8;
+  const double s_end6 = 6.0 * p[n - 1];
+  double carry = 0.0;
+  for (int b = 0; b < n; b += 32) {
+    const int k = b + lane;
+    double v = k < n ? 6.0 * p[k] : 0.0;
+    if (k == 0) v = v / (1.0 - z);
+    double t = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane >= 1) v = fma(z, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 2);
+    if (lane >= 2) v = fma(z2, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 4);
+    if (lane >= 4) v = fma(z4, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 8);
+    if (lane >= 8) v = fma(z8, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 16);
+    if (lane >= 16) v = fma(z16, t, v);
+    v = fma(zl, carry, v);
+    if (k < n) p[k] = v;
+    carry = __shfl_sync(0xffffffffu, v, 31);
   }
-  double next = -z * (s_end / ((1.0 - z) * (1.0 - z)) + (prev - s_end / (1.0 - z)) / (1.0 - z * z));
-  p[(long long)(n - 1) * stride] = next;
-  for (int k = n - 2; k >= 0; --k) {
-    next = z * (next - p[(long long)k * stride]);
-    p[(long long)k * stride] = next;
+  __syncwarp();
+  const double tail = spline_tail(p[n - 1], s_end6);
+  carry = 0.0;
+  for (int b = 0; b < n; b += 32) {
+    const int k = n - 1 - (b + lane);   // lane 0 of the first chunk is the last element
+    double v = k >= 0 ? -z * p[k] : 0.0;
+    if (k == n - 1) v = tail;
+    double t = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane >= 1) v = fma(z, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 2);
+    if (lane >= 2) v = fma(z2, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 4);
+    if (lane >= 4) v = fma(z4, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 8);
+    if (lane >= 8) v = fma(z8, t, v);
+    t = __shfl_up_sync(0xffffffffu, v, 16);
+    if (lane >= 16) v = fma(z16, t, v);
+    v = fma(zl, carry, v);
+    if (k >= 0) p[k] = v;
+    carry = __shfl_sync(0xffffffffu, v, 31);
+  }
+}
+
+// Strided lines (y or z), split into segments of kSplineSeg elements, one
+// thread per (line, segment), consecutive threads on consecutive lines.  A
+// segment's recursion starts kSplineWarm elements early from zero (its error
+// decays as |z|^28 < 1e-16) unless that reaches the line's end, where the
+// exact start value is used.  Out of place: the causal pass reads src and
+// writes c+ to dst, storing c-[n-1] in place of c+[n-1]; the anti-causal
+// pass reads that and writes c- back.  Line i starts at
+// (i % na) * sa + (i / na) * sb, elements `stride` apart.
+constexpr int kSplineSeg = 64, kSplineWarm = 28;
+
+__global__ void k_spline_causal(const double* __restrict__ src, double* __restrict__ dst, long long nlines, int n,
+                                long long stride, long long na, long long sa, long long sb) {
+  const double z = kSplineZ;
+  const int nseg = (n + kSplineSeg - 1) / kSplineSeg;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nlines * nseg) return;
+  const long long line = i % nlines;
+  const int sgm = (int)(i / nlines);
+  const long long base = (line % na) * sa + (line / na) * sb;
+  const int k0 = sgm * kSplineSeg, k1 = min(k0 + kSplineSeg, n), kw = max(k0 - kSplineWarm, 0);
+  double c;
+  int k;
+  if (kw == 0) {
+    c = 6.0 * src[base] / (1.0 - z);
+    if (k0 == 0) dst[base] = c;
+    k = 1;
+  } else {
+    c = 0.0;
+    k = kw;
+  }
+  for (; k < k1; ++k) {
+    c = fma(z, c, 6.0 * src[base + k * stride]);
+    if (k >= k0) dst[base + k * stride] = c;
+  }
+  if (k1 == n) dst[base + (long long)(n - 1) * stride] = spline_tail(c, 6.0 * src[base + (long long)(n - 1) * stride]);
+}
+
+__global__ void k_spline_anticausal(const double* __restrict__ src, double* __restrict__ dst, long long nlines, int n,
+                                    long long stride, long long na, long long sa, long long sb) {
+  const double z = kSplineZ;
+  const int nseg = (n + kSplineSeg - 1) / kSplineSeg;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nlines * nseg) return;
+  const long long line = i % nlines;
+  const int sgm = (int)(i / nlines);
+  const long long base = (line % na) * sa + (line / na) * sb;
+  const int k0 = sgm * kSplineSeg, k1 = min(k0 + kSplineSeg, n), ke = min(k1 + kSplineWarm, n);
+  double c;
+  int k;
+  if (ke == n) {
+    c = src[base + (long long)(n - 1) * stride];
+    if (n - 1 < k1) dst[base + (long long)(n - 1) * stride] = c;
+    k = n - 2;
+  } else {
+    c = 0.0;
+    k = ke - 1;
+  }
+  for (; k >= k0; --k) {
+    c = z * (c - src[base + k * stride]);
+    if (k < k1) dst[base + k * stride] = c;
   }
 }
 
