@@ -55,6 +55,46 @@ WR_API int wr_xres_register(const float* mov, int32_t nz, int32_t ny, int32_t nx
                             float* motion_out, float* ref_sampled_out, WrLKStats* stats, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/*
+ * The continuous reference H (utils/calFlowCrossResolution.py:463-478,
+ * 1144-1154): cubic B-spline of vol (nz, ny, nx) float32, map_coordinates
+ * order 3, mode "nearest", at n points coords (n, 3) = (x, y, z) in vol's
+ * index space; out (n) float32.  Workspace from wr_spline_workspace_size.
+ */
+WR_API int wr_spline_workspace_size(int32_t nz, int32_t ny, int32_t nx, size_t* bytes);
+WR_API int wr_spline_sample(const float* vol, int32_t nz, int32_t ny, int32_t nx, const float* coords, int64_t n,
+                            float* out, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Fixed-plane projections of mapped samples (utils/calFlowCrossResolution.py:
+ * 480-569 + 878-1141 and 571-660 + 700-876): n samples values (n) at
+ * coords (n, 3) = (x, y, z) in reference space, nplanes target z values;
+ * output planes (nplanes, xout, yout) float32 with xout = ceil(xref / ds),
+ * yout = ceil(yref / ds) (the reference's internal "zxy" order).
+ *
+ * wr_project_planes_max: max of the samples within z_window of a plane over
+ * the XY pixels a sample reaches (nearest != 0: the rounded pixel; else
+ * floor .. floor + 1, widened by extra_radius); values are shifted by
+ * max(1 - min, 0) for the max and back, as the reference does; pixels
+ * without a sample get fill_value (has_fill) or -inf.
+ *
+ * wr_project_planes_weighted: bilinear XY splat of the samples with z weight
+ * mode 0 hard, 1 triangular, 2 gaussian (z_sigma <= 0: z_window / 2);
+ * out = sum(v w) / sum(w) where sum(w) > eps, else fill_value; weight_out
+ * (may be NULL) receives sum(w).
+ *
+ * Workspace: 8 bytes per output pixel plus 256 (wr_project_workspace_size).
+ */
+WR_API int wr_project_workspace_size(int32_t nplanes, int32_t xref, int32_t yref, int32_t ds, size_t* bytes);
+WR_API int wr_project_planes_max(const float* values, const float* coords, int64_t n, const float* target_z,
+                                 int32_t nplanes, int32_t xref, int32_t yref, int32_t ds, float z_window,
+                                 int32_t nearest, int32_t extra_radius, float fill_value, int32_t has_fill, float* out,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+WR_API int wr_project_planes_weighted(const float* values, const float* coords, int64_t n, const float* target_z,
+                                      int32_t nplanes, int32_t xref, int32_t yref, int32_t ds, float z_window,
+                                      float z_sigma, int32_t mode, float fill_value, float eps, float* out,
+                                      float* weight_out, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,13 @@ SciPy.
 Arrays use the reference's internal (x, y, z) layout.  Parity is pinned
 against fixtures made by running the reference itself
 (``tests/golden/make_golden.py --only xres``).
+
+``project_max`` / ``project_weighted`` restate the reference's two
+fixed-plane projection kernels (``_PROJECT_TO_PLANES_NANMAX_SRC`` and
+``_PROJECT_TO_PLANES_WEIGHTED_AVG_SRC``, :480-660) and their wrappers
+(:700-1141).  Those exist only as CuPy RawKernels, which cannot run here:
+parity unpinned for the projections (the restatement follows the kernel
+source line by line; no reference output exists to pin it).
 """
 
 from __future__ import annotations
@@ -49,7 +56,8 @@ from .lk_oracle import (
     trilinear,
 )
 
-__all__ = ["cubic_sample_scipy", "bspline_coefficients", "cubic_sample", "get_motion_v2", "SPLINE_PAD"]
+__all__ = ["cubic_sample_scipy", "bspline_coefficients", "cubic_sample", "get_motion_v2", "SPLINE_PAD",
+           "project_max", "project_weighted"]
 
 SPLINE_PAD = 12                       # SciPy's edge padding before the prefilter (mode "nearest")
 _Z1 = float(np.sqrt(3.0) - 2.0)       # pole of the cubic B-spline prefilter
@@ -250,3 +258,96 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
         phase_new, ref_sampled, valid, res = evaluate(motion)
 
     return phase_new, motion, ref_sampled, log
+
+
+def project_max(values, coords, target_z, xref, yref, ds=1, z_window=1.5, nearest=False, extra=0, fill=0.0):
+    """Max splat (calFlowCrossResolution.py:480-569, 878-1141): values (n,),
+    coords (n, 3) = (x, y, z); returns (nplanes, xout, yout) float32."""
+    values = np.asarray(values, np.float32).ravel()
+    coords = np.asarray(coords, np.float32).reshape(-1, 3)
+    target_z = np.atleast_1d(np.asarray(target_z, np.float32))
+    xout, yout = (xref + ds - 1) // ds, (yref + ds - 1) // ds
+    fin = values[np.isfinite(values)]
+    shift = np.float32(max(np.float32(-fin.min() + np.float32(1.0)), np.float32(0.0))) if fin.size else np.float32(0.0)
+    shifted = (values + shift).astype(np.float32)
+    out = np.full((len(target_z), xout, yout), -np.inf, np.float32)
+    for i in range(values.size):
+        v = shifted[i]
+        x, y, z = coords[i]
+        if not (np.isfinite(v) and np.isfinite(x) and np.isfinite(y) and np.isfinite(z)):
+            continue
+        if nearest:
+            xs = [int(np.floor(np.float32(x + np.float32(0.5))))]
+            ys = [int(np.floor(np.float32(y + np.float32(0.5))))]
+        else:
+            xf, yf = int(np.floor(x)), int(np.floor(y))
+            xs = range(xf - extra, xf + 2 + extra)
+            ys = range(yf - extra, yf + 2 + extra)
+        for p, z0 in enumerate(target_z):
+            if abs(np.float32(z - z0)) > np.float32(z_window):
+                continue
+            for xi in xs:
+                if xi < 0 or xi >= xref or xi // ds >= xout:
+                    continue
+                for yi in ys:
+                    if yi < 0 or yi >= yref or yi // ds >= yout:
+                        continue
+                    o = out[p, xi // ds, yi // ds]
+                    out[p, xi // ds, yi // ds] = max(o, v)
+    valid = np.isfinite(out)
+    out = np.where(valid, (out - shift).astype(np.float32), out)
+    if fill is not None:
+        out = np.where(np.isfinite(out), out, np.float32(fill)).astype(np.float32)
+    return out
+
+
+def project_weighted(values, coords, target_z, xref, yref, ds=1, z_window=1.5, z_sigma=None, mode=2, fill=0.0,
+                     eps=1e-6):
+    """Weighted bilinear splat (calFlowCrossResolution.py:571-660, 700-876);
+    returns (planes, summed weights), both (nplanes, xout, yout), float64
+    sums (the CUDA kernel accumulates float32 atomically)."""
+    values = np.asarray(values, np.float32).ravel()
+    coords = np.asarray(coords, np.float32).reshape(-1, 3)
+    target_z = np.atleast_1d(np.asarray(target_z, np.float32))
+    xout, yout = (xref + ds - 1) // ds, (yref + ds - 1) // ds
+    sv = np.zeros((len(target_z), xout, yout))
+    sw = np.zeros((len(target_z), xout, yout))
+    sigma = np.float32(z_window * 0.5 if z_sigma is None or z_sigma <= 0 else z_sigma)
+    for i in range(values.size):
+        v = float(values[i])
+        x, y, z = (float(c) for c in coords[i])
+        if not all(np.isfinite([v, x, y, z])):
+            continue
+        if x < 0 or x > xref - 1 or y < 0 or y > yref - 1:
+            continue
+        xo_f, yo_f = x / ds, y / ds
+        xo0, yo0 = int(np.floor(xo_f)), int(np.floor(yo_f))
+        dx, dy = xo_f - xo0, yo_f - yo0
+        for p, z0 in enumerate(target_z):
+            dz = abs(z - float(z0))
+            if dz > z_window:
+                continue
+            if mode == 0:
+                wz = 1.0
+            elif mode == 1:
+                wz = max(1.0 - dz / (z_window + 1e-6), 0.0)
+            else:
+                wz = float(np.exp(-0.5 * dz * dz / (float(sigma) ** 2 + 1e-6)))
+            if wz <= 0:
+                continue
+            for ax in (0, 1):
+                xo = xo0 + ax
+                if xo < 0 or xo >= xout:
+                    continue
+                wx = 1.0 - dx if ax == 0 else dx
+                for ay in (0, 1):
+                    yo = yo0 + ay
+                    if yo < 0 or yo >= yout:
+                        continue
+                    w = wx * (1.0 - dy if ay == 0 else dy) * wz
+                    if w <= 0:
+                        continue
+                    sv[p, xo, yo] += v * w
+                    sw[p, xo, yo] += w
+    out = np.where(sw > eps, sv / np.maximum(sw, eps), fill)
+    return out, sw

@@ -118,3 +118,77 @@ def test_xres_rejects_unbuilt_options():
     opt["phase"] = np.zeros(arrays["mov"].shape + (3,), np.float32)
     with pytest.raises(NotImplementedError):
         C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
+
+
+def _projection_case(seed=5):
+    rng = np.random.default_rng(seed)
+    X, Y, K = 20, 18, 4
+    coords = np.stack([rng.uniform(-2, 22, (X, Y, K)), rng.uniform(-2, 20, (X, Y, K)),
+                       rng.uniform(-1, 7, (X, Y, K))], -1).astype(np.float32)
+    values = rng.normal(50, 80, (X, Y, K)).astype(np.float32)
+    values[0, 0, 0] = np.nan
+    coords[1, 1, 1, 0] = np.inf
+    ref = rng.normal(100, 20, (21, 19, 6)).astype(np.float32)
+    return coords, values, ref
+
+
+@pytest.mark.parametrize("mode,extra,ds", [("subpixel_footprint", 0, 1), ("subpixel_footprint", 1, 2), ("nearest", 0, 3)])
+def test_projection_max_matches_restatement(mode, extra, ds):
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    coords, values, ref = _projection_case()
+    planes = [0.0, 2.5, 5.0]
+    got = C.project_coords_to_fixed_planes_gpu(coords, ref, planes, values_xyk=values, z_window=1.2,
+                                               downsample_xy=ds, fill_value=-7.0, return_numpy=True,
+                                               output_order="zxy", xy_splat_mode=mode, xy_extra_radius=extra)
+    want = X.project_max(values, coords, planes, ref.shape[0], ref.shape[1], ds, 1.2, mode == "nearest", extra, -7.0)
+    np.testing.assert_array_equal(got, want)
+    zyx = C.project_coords_to_fixed_planes_gpu(coords, ref, planes, values_xyk=values, z_window=1.2,
+                                               downsample_xy=ds, fill_value=-7.0, return_numpy=True,
+                                               xy_splat_mode=mode, xy_extra_radius=extra)
+    np.testing.assert_array_equal(zyx, want.transpose(0, 2, 1))
+
+
+@pytest.mark.parametrize("wmode", ["hard", "triangular", "gaussian"])
+def test_projection_weighted_matches_restatement(wmode):
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    coords, values, ref = _projection_case(6)
+    planes = [1.0, 3.0]
+    out, w = C.project_coords_to_fixed_planes_weighted_gpu(coords, ref, planes, values_xyk=values, z_window=1.5,
+                                                           z_weight_mode=wmode, downsample_xy=2, return_numpy=True,
+                                                           output_order="zxy")
+    want, want_w = X.project_weighted(values, coords, planes, ref.shape[0], ref.shape[1], 2, 1.5, None,
+                                      {"hard": 0, "triangular": 1, "gaussian": 2}[wmode])
+    np.testing.assert_allclose(w, want_w, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(out, want, rtol=1e-4, atol=1e-3)
+
+
+def test_continuous_H_matches_scipy():
+    """Spline values H(coords) from the device prefilter and sampler against
+    SciPy's map_coordinates (the library call the reference makes)."""
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    coords, _, ref = _projection_case(7)
+    H = C.generate_continuous_H_gpu(ref, zRatio=2.0)
+    got = C.apply_H_to_matrix_gpu(torch.from_numpy(coords).cuda(), H).cpu().numpy()
+    want = X.cubic_sample_scipy(ref.astype(np.float64), coords[..., 0], coords[..., 1], coords[..., 2] / 2.0)
+    fin = np.isfinite(want)
+    np.testing.assert_allclose(got[fin], want[fin], rtol=1e-6, atol=1e-4)
+
+
+def test_projection_samples_reference_when_values_absent():
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    coords, _, ref = _projection_case(8)
+    coords[1, 1, 1, 0] = 3.0
+    planes = [2.0]
+    got = C.project_coords_to_fixed_planes_gpu(coords, ref, planes, z_window=1.0, return_numpy=True,
+                                               output_order="zxy")
+    vals = X.cubic_sample_scipy(ref.astype(np.float64), coords[..., 0], coords[..., 1], coords[..., 2]).astype(np.float32)
+    want = X.project_max(vals, coords, planes, ref.shape[0], ref.shape[1], 1, 1.0, False, 0, 0.0)
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-3)

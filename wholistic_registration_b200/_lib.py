@@ -70,6 +70,11 @@ EXPORTS = (
     "wr_bwareafilt3",
     "wr_xres_workspace_size",
     "wr_xres_register",
+    "wr_spline_workspace_size",
+    "wr_spline_sample",
+    "wr_project_workspace_size",
+    "wr_project_planes_max",
+    "wr_project_planes_weighted",
 )
 
 
@@ -210,6 +215,14 @@ def load():
                                                ctypes.POINTER(sz)]
         lib.wr_xres_register.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, vp, P, ctypes.c_float,
                                          vp, vp, vp, vp, vp, sz, vp]
+        i64_, f32_ = ctypes.c_int64, ctypes.c_float
+        lib.wr_spline_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
+        lib.wr_spline_sample.argtypes = [vp, i32, i32, i32, vp, i64_, vp, vp, sz, vp]
+        lib.wr_project_workspace_size.argtypes = [i32, i32, i32, i32, ctypes.POINTER(sz)]
+        lib.wr_project_planes_max.argtypes = [vp, vp, i64_, vp, i32, i32, i32, i32, f32_, i32, i32, f32_, i32, vp,
+                                              vp, sz, vp]
+        lib.wr_project_planes_weighted.argtypes = [vp, vp, i64_, vp, i32, i32, i32, i32, f32_, f32_, i32, f32_, f32_,
+                                                   vp, vp, vp, sz, vp]
         for name in EXPORTS:
             getattr(lib, name).restype = (ctypes.c_char_p if name.endswith("last_error") else ctypes.c_int)
         if lib.wr_abi_version() != 1:

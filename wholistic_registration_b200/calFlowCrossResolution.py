@@ -16,6 +16,14 @@ Every computation runs on the GPU through the sm_100a library
 missing.  NumPy inputs give NumPy outputs; CUDA torch tensors in the same
 (x, y, z) layout give CUDA tensors.
 
+The module also carries the continuous reference ``H``
+(``generate_continuous_H_gpu`` / ``apply_H_to_matrix_gpu``, :463-478,
+1144-1154) and the two fixed-plane projections of mapped samples
+(``project_coords_to_fixed_planes_gpu``, max splat, :480-569 + 878-1141;
+``project_coords_to_fixed_planes_weighted_gpu``, weighted bilinear splat,
+:571-660 + 700-876) with the reference's signatures; they return CUDA torch
+tensors where the reference returns CuPy arrays.
+
 Not built here: the wrong-region correction the reference runs by default
 (``wrong_region_enable=True``: bad-region detection on the CP errors, a trap
 mask in reference space and two re-runs, :2240-2467) and an initial
@@ -35,7 +43,8 @@ import torch
 from . import _lib
 from .registrar import LKParams, _stream_ptr, stats_to_log
 
-__all__ = ["getMotion_v2", "XresRegistrar"]
+__all__ = ["getMotion_v2", "XresRegistrar", "generate_continuous_H_gpu", "apply_H_to_matrix_gpu",
+           "project_coords_to_fixed_planes_gpu", "project_coords_to_fixed_planes_weighted_gpu"]
 
 
 class XresRegistrar:
@@ -201,3 +210,171 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
         return phase.contiguous(), motion.contiguous(), sampled.contiguous()
     return (np.ascontiguousarray(phase.cpu().numpy()), np.ascontiguousarray(motion.cpu().numpy()),
             np.ascontiguousarray(sampled.cpu().numpy()))
+
+
+# ---------------------------------------------------------------------------
+# continuous reference H and fixed-plane projections
+# ---------------------------------------------------------------------------
+
+def _cuda_f32(a, device=None):
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=torch.float32)
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float32))).to(device)
+
+
+def _workspace(nbytes, device):
+    return torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=device)
+
+
+def _aligned(buf):
+    return (buf.data_ptr() + 255) // 256 * 256
+
+
+def spline_sample(vol_zyx: torch.Tensor, coords_xyz: torch.Tensor, stream=None) -> torch.Tensor:
+    """Cubic B-spline (order 3, mode "nearest") of a (z, y, x) float32 CUDA
+    volume at (n, 3) points (x, y, z); (n,) float32 (``wr_spline_sample``)."""
+    lib = _lib.load()
+    vol = vol_zyx.to(torch.float32).contiguous()
+    pts = coords_xyz.to(device=vol.device, dtype=torch.float32).reshape(-1, 3).contiguous()
+    nz, ny, nx = (int(v) for v in vol.shape)
+    need = ctypes.c_size_t(0)
+    _lib.check("wr_spline_workspace_size", lib.wr_spline_workspace_size(nz, ny, nx, ctypes.byref(need)))
+    ws = _workspace(need.value, vol.device)
+    out = torch.empty(pts.shape[0], dtype=torch.float32, device=vol.device)
+    _lib.check("wr_spline_sample", lib.wr_spline_sample(vol.data_ptr(), nz, ny, nx, pts.data_ptr(), pts.shape[0],
+                                                        out.data_ptr(), _aligned(ws), int(need.value),
+                                                        _stream_ptr(stream)))
+    return out
+
+
+def generate_continuous_H_gpu(stack, zRatio):
+    """``H`` of calFlowCrossResolution.py:463-478: a callable mapping
+    (..., 3) physical coordinates (z divided by ``zRatio``) to the cubic
+    spline of ``stack`` (x, y, z), float32."""
+    vol = _cuda_f32(stack).permute(2, 1, 0).contiguous()
+    zr = float(zRatio)
+
+    def H(coords_phys):
+        c = _cuda_f32(coords_phys, vol.device).clone()
+        c[..., 2] = c[..., 2] / zr
+        return spline_sample(vol, c.reshape(-1, 3)).reshape(c.shape[:-1])
+
+    return H
+
+
+def apply_H_to_matrix_gpu(A, H):
+    """calFlowCrossResolution.py:1144-1154: H at every (x, y, z) of A (..., 3)."""
+    return H(A)
+
+
+def _ref_xyz_shape(ref_volume, order):
+    if order == "xyz":
+        X, Y, Z = ref_volume.shape
+    elif order == "zyx":
+        Z, Y, X = ref_volume.shape
+    else:
+        raise ValueError("ref_volume_order should be 'xyz' or 'zyx'.")
+    return int(X), int(Y), int(Z)
+
+
+def _projection_inputs(coords_ref_xyk_xyz, ref_volume, target_z_planes, values_xyk, ref_volume_order,
+                       downsample_xy):
+    coords = _cuda_f32(coords_ref_xyk_xyz)
+    if coords.dim() != 4 or coords.shape[-1] != 3:
+        raise ValueError(f"coords_ref_xyk_xyz should have shape (X,Y,K,3), got {tuple(coords.shape)}")
+    ref = _cuda_f32(ref_volume, coords.device)
+    if ref.dim() != 3:
+        raise ValueError(f"ref_volume should be 3D, got {tuple(ref.shape)}")
+    X, Y, _ = _ref_xyz_shape(ref, ref_volume_order)
+    ds = int(downsample_xy)
+    if ds < 1:
+        raise ValueError("downsample_xy should be >= 1.")
+    target = _cuda_f32(np.atleast_1d(np.asarray(target_z_planes, dtype=np.float32)), coords.device).reshape(-1)
+    pts = coords.reshape(-1, 3).contiguous()
+    if values_xyk is None:
+        vol_zyx = ref.permute(2, 1, 0).contiguous() if ref_volume_order == "xyz" else ref.contiguous()
+        values = spline_sample(vol_zyx, pts)
+    else:
+        values = _cuda_f32(values_xyk, coords.device)
+        if tuple(values.shape) != tuple(coords.shape[:-1]):
+            raise ValueError(f"values_xyk shape {tuple(values.shape)} does not match coords shape "
+                             f"{tuple(coords.shape[:-1])}")
+        values = values.reshape(-1).contiguous()
+    return pts, values, target, X, Y, ds
+
+
+def project_coords_to_fixed_planes_gpu(coords_ref_xyk_xyz, ref_volume=None, target_z_planes=None, values_xyk=None,
+                                       ref_volume_order="xyz", z_window=1.5, downsample_xy=1, fill_value=0.0,
+                                       return_numpy=False, output_order="zyx", xy_splat_mode="subpixel_footprint",
+                                       xy_extra_radius=0):
+    """Max splat of mapped samples onto fixed reference z planes
+    (calFlowCrossResolution.py:878-1141, kernel :480-569)."""
+    if target_z_planes is None:
+        raise ValueError("target_z_planes must be provided.")
+    if ref_volume is None:
+        raise ValueError("ref_volume must be provided to infer reference shape.")
+    if xy_splat_mode == "nearest":
+        nearest, extra = 1, 0
+    elif xy_splat_mode == "subpixel_footprint":
+        nearest, extra = 0, int(xy_extra_radius)
+        if extra < 0:
+            raise ValueError("xy_extra_radius should be >= 0.")
+    else:
+        raise ValueError("xy_splat_mode should be 'nearest' or 'subpixel_footprint'.")
+    if output_order not in ("zyx", "zxy"):
+        raise ValueError("output_order should be 'zyx' or 'zxy'.")
+    pts, values, target, X, Y, ds = _projection_inputs(coords_ref_xyk_xyz, ref_volume, target_z_planes, values_xyk,
+                                                       ref_volume_order, downsample_xy)
+    lib = _lib.load()
+    npl = int(target.numel())
+    xo, yo = (X + ds - 1) // ds, (Y + ds - 1) // ds
+    need = ctypes.c_size_t(0)
+    _lib.check("wr_project_workspace_size", lib.wr_project_workspace_size(npl, X, Y, ds, ctypes.byref(need)))
+    ws = _workspace(need.value, pts.device)
+    out = torch.empty((npl, xo, yo), dtype=torch.float32, device=pts.device)
+    _lib.check("wr_project_planes_max",
+               lib.wr_project_planes_max(values.data_ptr(), pts.data_ptr(), values.numel(), target.data_ptr(), npl, X,
+                                         Y, ds, float(z_window), nearest, extra,
+                                         0.0 if fill_value is None else float(fill_value),
+                                         0 if fill_value is None else 1, out.data_ptr(), _aligned(ws), int(need.value),
+                                         _stream_ptr(None)))
+    if output_order == "zyx":
+        out = out.transpose(1, 2)
+    return out.cpu().numpy() if return_numpy else out
+
+
+def project_coords_to_fixed_planes_weighted_gpu(coords_ref_xyk_xyz, ref_volume, target_z_planes, values_xyk=None,
+                                                ref_volume_order="xyz", z_window=1.5, z_sigma=None,
+                                                z_weight_mode="gaussian", downsample_xy=1, fill_value=0.0,
+                                                return_numpy=False, output_order="zyx", eps=1e-6):
+    """Weighted bilinear splat onto fixed reference z planes
+    (calFlowCrossResolution.py:700-876, kernel :571-660); returns
+    (planes, summed weights)."""
+    modes = {"hard": 0, "triangular": 1, "gaussian": 2}
+    if z_weight_mode not in modes:
+        raise ValueError("z_weight_mode should be 'hard', 'triangular', or 'gaussian'.")
+    if output_order not in ("zyx", "zxy"):
+        raise ValueError("output_order should be 'zyx' or 'zxy'.")
+    pts, values, target, X, Y, ds = _projection_inputs(coords_ref_xyk_xyz, ref_volume, target_z_planes, values_xyk,
+                                                       ref_volume_order, downsample_xy)
+    if z_sigma is None:
+        z_sigma = float(z_window) * 0.5
+    lib = _lib.load()
+    npl = int(target.numel())
+    xo, yo = (X + ds - 1) // ds, (Y + ds - 1) // ds
+    need = ctypes.c_size_t(0)
+    _lib.check("wr_project_workspace_size", lib.wr_project_workspace_size(npl, X, Y, ds, ctypes.byref(need)))
+    ws = _workspace(need.value, pts.device)
+    out = torch.empty((npl, xo, yo), dtype=torch.float32, device=pts.device)
+    wout = torch.empty((npl, xo, yo), dtype=torch.float32, device=pts.device)
+    _lib.check("wr_project_planes_weighted",
+               lib.wr_project_planes_weighted(values.data_ptr(), pts.data_ptr(), values.numel(), target.data_ptr(),
+                                              npl, X, Y, ds, float(z_window), float(z_sigma),
+                                              modes[z_weight_mode], float(fill_value), float(eps), out.data_ptr(),
+                                              wout.data_ptr(), _aligned(ws), int(need.value), _stream_ptr(None)))
+    if output_order == "zyx":
+        out, wout = out.transpose(1, 2), wout.transpose(1, 2)
+    if return_numpy:
+        return out.cpu().numpy(), wout.cpu().numpy()
+    return out, wout

@@ -306,4 +306,160 @@ __global__ void k_xres_finish(const FieldSrc f, float* __restrict__ phase, float
   }
 }
 
+// ---------------------------------------------------------------------------
+// continuous reference H (generate_continuous_H_gpu / apply_H_to_matrix_gpu,
+// utils/calFlowCrossResolution.py:463-478, 1144-1154) and the fixed-plane
+// projections of mapped samples (:480-660, 700-1141)
+// ---------------------------------------------------------------------------
+
+// H at n points (x, y, z) of `coords`: float64 coefficients, float64 sum,
+// rounded to float32 like map_coordinates on a float32 stack.
+__global__ void k_spline_points(const double* __restrict__ C, int px, int py, int pz, const float* __restrict__ coords,
+                                long long n, float* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)spline_sample<double, double>(C, px, py, pz, coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]);
+}
+
+// float <-> unsigned key whose unsigned order is the float order
+__device__ __forceinline__ unsigned float_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// minimum of the finite values (key in mm[0], start 0xffffffff) and whether
+// there is one (mm[1] != 0)
+__global__ void k_finite_min(const float* __restrict__ v, long long n, unsigned* __restrict__ mm) {
+  unsigned kmin = 0xffffffffu, any = 0u;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float f = v[i];
+    if (isfinite(f)) {
+      kmin = min(kmin, float_key(f));
+      any = 1u;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+    any |= __shfl_xor_sync(0xffffffffu, any, o);
+  }
+  if ((threadIdx.x & 31) == 0 && any) {
+    atomicMin(mm, kmin);
+    atomicOr(mm + 1, 1u);
+  }
+}
+
+// shift = max(1 - min, 0) of the finite values, as a float32 computation
+__device__ __forceinline__ float project_shift(const unsigned* mm) {
+  if (!mm[1]) return 0.f;
+  return fmaxf(__fadd_rn(-key_float(mm[0]), 1.f), 0.f);
+}
+
+// Max splat of shifted (non-negative) samples onto fixed z planes: a sample
+// at (x, y, z) reaches plane z0 when |z - z0| <= z_window and writes the XY
+// pixels (rounded x, y) or (floor .. floor + 1 +- extra), each pixel index
+// divided by the down-sampling factor.  Output (nplanes, xout, yout) as
+// unsigned keys, start 0 (below every float).
+__global__ void k_project_max(const float* __restrict__ values, const float* __restrict__ coords, long long n,
+                              const float* __restrict__ target_z, int nplanes, int xref, int yref, int xout, int yout,
+                              float z_window, int ds, int nearest, int extra, const unsigned* __restrict__ mm,
+                              unsigned* __restrict__ out) {
+  const float shift = project_shift(mm);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v0 = values[i];
+    const float x = coords[3 * i], y = coords[3 * i + 1], z = coords[3 * i + 2];
+    const float val = __fadd_rn(v0, shift);
+    if (!isfinite(val) || !isfinite(x) || !isfinite(y) || !isfinite(z)) continue;
+    const unsigned key = float_key(val);
+    int x0, x1, y0, y1;
+    if (nearest) {
+      x0 = x1 = (int)floorf(x + 0.5f);
+      y0 = y1 = (int)floorf(y + 0.5f);
+    } else {
+      const int xf = (int)floorf(x), yf = (int)floorf(y);
+      x0 = xf - extra; x1 = xf + 1 + extra;
+      y0 = yf - extra; y1 = yf + 1 + extra;
+    }
+    for (int p = 0; p < nplanes; ++p) {
+      if (fabsf(z - target_z[p]) > z_window) continue;
+      unsigned* plane = out + (size_t)p * xout * yout;
+      for (int xi = max(x0, 0); xi <= min(x1, xref - 1); ++xi) {
+        const int xo = xi / ds;
+        if (xo >= xout) continue;
+        for (int yi = max(y0, 0); yi <= min(y1, yref - 1); ++yi) {
+          const int yo = yi / ds;
+          if (yo >= yout) continue;
+          atomicMax(plane + (size_t)xo * yout + yo, key);
+        }
+      }
+    }
+  }
+}
+
+// keys -> values: the max minus the shift, or the fill value where nothing
+// landed (has_fill = 0 keeps -inf)
+__global__ void k_project_max_finish(const unsigned* __restrict__ keys, long long n, const unsigned* __restrict__ mm,
+                                     float fill, int has_fill, float* __restrict__ out) {
+  const float shift = project_shift(mm);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned k = keys[i];
+    if (k == 0u) out[i] = has_fill ? fill : -INFINITY;
+    else out[i] = __fsub_rn(key_float(k), shift);
+  }
+}
+
+// Weighted splat: samples with x in [0, xref - 1] and y in [0, yref - 1]
+// reach plane z0 with weight wz(|z - z0|) (mode 0: 1, 1: 1 - dz / (window +
+// 1e-6), 2: exp(-dz^2 / (2 sigma^2 + 1e-6))) for dz <= z_window, and are
+// spread bilinearly over the 2 x 2 output pixels around (x, y) / ds.
+__global__ void k_project_weighted(const float* __restrict__ values, const float* __restrict__ coords, long long n,
+                                   const float* __restrict__ target_z, int nplanes, int xref, int yref, int xout,
+                                   int yout, float z_window, float z_sigma, int ds, int mode, float* __restrict__ sum_v,
+                                   float* __restrict__ sum_w) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v = values[i];
+    const float x = coords[3 * i], y = coords[3 * i + 1], z = coords[3 * i + 2];
+    if (!isfinite(v) || !isfinite(x) || !isfinite(y) || !isfinite(z)) continue;
+    if (x < 0.f || x > (float)(xref - 1) || y < 0.f || y > (float)(yref - 1)) continue;
+    const float xo_f = x / (float)ds, yo_f = y / (float)ds;
+    const int xo0 = (int)floorf(xo_f), yo0 = (int)floorf(yo_f);
+    const float dx = xo_f - (float)xo0, dy = yo_f - (float)yo0;
+    for (int p = 0; p < nplanes; ++p) {
+      const float dz = fabsf(z - target_z[p]);
+      if (dz > z_window) continue;
+      float wz = 1.f;
+      if (mode == 1) {
+        wz = fmaxf(1.f - dz / (z_window + 1e-6f), 0.f);
+      } else if (mode == 2) {
+        const float sg = z_sigma > 0.f ? z_sigma : z_window * 0.5f;
+        wz = expf(-0.5f * dz * dz / (sg * sg + 1e-6f));
+      }
+      if (!(wz > 0.f) || !isfinite(wz)) continue;
+      const size_t base = (size_t)p * xout * yout;
+      for (int ax = 0; ax <= 1; ++ax) {
+        const int xo = xo0 + ax;
+        if (xo < 0 || xo >= xout) continue;
+        const float wx = ax == 0 ? 1.f - dx : dx;
+        for (int ay = 0; ay <= 1; ++ay) {
+          const int yo = yo0 + ay;
+          if (yo < 0 || yo >= yout) continue;
+          const float w = wx * (ay == 0 ? 1.f - dy : dy) * wz;
+          if (!(w > 0.f) || !isfinite(w)) continue;
+          atomicAdd(sum_v + base + (size_t)xo * yout + yo, v * w);
+          atomicAdd(sum_w + base + (size_t)xo * yout + yo, w);
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_project_weighted_finish(const float* __restrict__ sum_v, const float* __restrict__ sum_w, long long n,
+                                          float eps, float fill, float* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float w = sum_w[i];
+    out[i] = w > eps ? sum_v[i] / fmaxf(w, eps) : fill;
+  }
+}
+
 }  // namespace wr
