@@ -329,6 +329,8 @@ def run_ours(args, wl, rank, world, local_rank):
     res["config"]["autotune"] = {"flags": reg.tune_flags, "ms_per_candidate": tune_report} if tune_report else None
     if not args.no_batch:
         res["config"]["batched_small_frames"] = run_batched_small(device)
+    if not args.no_xres:
+        res["config"]["cross_resolution"] = run_cross_resolution(device, args.xres_shape)
 
     # learned warm start + float16 levels (the headline path) on the same frames
     ws = None
@@ -429,6 +431,45 @@ def run_batched_small(device, n=16, reps=3):
         out[name + "_volumes_per_s"] = round(n * reps / (e0.elapsed_time(e1) * 1e-3), 2)
     out["speedup"] = round(out["batched_cuda_graph_volumes_per_s"] / out["one_call_per_frame_volumes_per_s"], 3)
     return out
+
+
+def run_cross_resolution(device, shape="32x1024x1024:128", reps=4):
+    """getMotion_v2 (wrong-region correction off): by default a
+    32x1024x1024 moving stack (z spacing 4) onto a 128x1024x1024 reference
+    (z spacing 1), layer 3, r 16, iter 10, its own stopping rules; the moving
+    stack is every (nzh / nz)-th reference slice shifted by one voxel in x and y."""
+    import torch
+
+    from wholistic_registration_b200 import synthetic
+    from wholistic_registration_b200.calFlowCrossResolution import XresRegistrar
+    from wholistic_registration_b200.registrar import LKParams
+
+    zyx, nzh = shape.split(":")
+    nz, ny, nx = (int(v) for v in zyx.split("x"))
+    nzh = int(nzh)
+    if nzh % nz:
+        raise ValueError("--xres-shape: the reference's z extent must be a multiple of the moving stack's")
+    tmpl, _, _ = synthetic.make_pair((nzh, ny, nx), 77, n_blobs=max(200, 20000 * nzh * ny * nx // (128 << 20)),
+                                     device=device)
+    ref = tmpl.float().contiguous()
+    mov = torch.roll(ref[::nzh // nz], shifts=(1, -1), dims=(1, 2)).contiguous()
+    excl = torch.zeros((nz, ny, nx), dtype=torch.uint8, device=device)
+    p = LKParams(layer=3, iter=10, r=16, zRatio=float(nzh // nz), movRange=5.0, smoothPenalty=0.05, tol=1e-3)
+    reg = XresRegistrar((nz, ny, nx), (nzh, ny, nx), p, 1.0, has_mask_ref=False, device=device)
+    reg.register(mov, ref, mask_mov=excl)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        reg.register(mov, ref, mask_mov=excl)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    log, _ = reg.error_log()
+    return {"shape_mov_zyx": [nz, ny, nx], "shape_ref_zyx": [nzh, ny, nx], "zRatio": float(nzh // nz), "zRatio_HR": 1.0,
+            "layer": 3, "r": 16, "iter": 10, "ms_per_volume": round(ms, 3), "volumes_per_s": round(1e3 / ms, 3),
+            "updates_per_level": {k: len(v["max_diff_motion"]) for k, v in log.items()},
+            "api": "XresRegistrar.register (device-resident stacks)"}
 
 
 def run_warmstart(args, wl, template, excl, frames, params, device, world, weights):
@@ -616,6 +657,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-xres", action="store_true", help="skip the cross-resolution (getMotion_v2) measurement")
+    ap.add_argument("--xres-shape", default="32x1024x1024:128",
+                    help="moving stack ZxYxX and reference z extent of the cross-resolution measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
