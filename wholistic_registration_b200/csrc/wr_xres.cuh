@@ -164,11 +164,6 @@ __global__ void k_spline_anticausal(const double* __restrict__ src, double* __re
   }
 }
 
-__global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
-}
-
 // exclusion bit of a (resized) mask: bit 0 = (value > thresh)
 template <typename T>
 __global__ void k_threshold_bits(const T* __restrict__ in, uint8_t* __restrict__ bits, long long n, double thresh) {
@@ -232,6 +227,46 @@ __device__ __forceinline__ R spline_sample(const T* __restrict__ C, int px, int 
   return acc;
 }
 
+// The float32 coefficients of a level stored as x quads: Q[row][q] holds the
+// four taps (q - 1 .. q + 2, clamped to the row) a sample whose first x tap
+// is q - 1 reads, so one 16-byte load replaces four scalar loads.
+__global__ void k_spline_quads(const double* __restrict__ c, float4* __restrict__ q, int px, long long rows) {
+  const long long n = rows * px;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % px);
+    const double* r = c + (i - x);
+    q[i] = make_float4((float)r[max(x - 1, 0)], (float)r[x], (float)r[min(x + 1, px - 1)], (float)r[min(x + 2, px - 1)]);
+  }
+}
+
+// spline_sample<float, float> on the quad layout
+__device__ __forceinline__ float spline_sample_quads(const float4* __restrict__ Q, int px, int py, int pz, float x,
+                                                     float y, float z) {
+  const SplineAxis ay = spline_axis(y, py), az = spline_axis(z, pz);
+  float c = x;
+  const float lo = -(float)kSplinePad, hi = (float)(px - 1 - kSplinePad);
+  if (!(c >= lo)) c = lo;
+  if (!(c <= hi)) c = hi;
+  const float f = floorf(c);
+  const int qx = (int)f + kSplinePad;   // first tap + 1, in [0, px - 1]
+  float wx[4], wy[4], wz[4];
+  bspline_weights<float>(c - f, wx);
+  bspline_weights<float>(ay.t, wy);
+  bspline_weights<float>(az.t, wz);
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float accy = 0.f;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const float4 v = __ldg(Q + ((size_t)az.i[k] * py + ay.i[b]) * px + qx);
+      accy += wy[b] * (wx[0] * v.x + wx[1] * v.y + wx[2] * v.z + wx[3] * v.w);
+    }
+    acc += wz[k] * accy;
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------
 // fused iteration
 // ---------------------------------------------------------------------------
@@ -240,7 +275,7 @@ struct XresArgs {
   IterArgs a;              // iteration grid: a.ref = moving level, a.mbits bit 0 = moving exclusion
   const float4* g;         // reference level on its grid: (m, Gx, Gy, Gz), G = half central difference
   int nxh, nyh, nzh;       // reference level extent
-  const float* cref;       // padded spline coefficients of the reference level
+  const float4* cref;      // padded spline coefficients of the reference level, x quads
   const double* cmask;     // padded spline coefficients of its 0/1 exclusion mask, or null
   int pxh, pyh, pzh;       // padded extent
   double zr, zrh;          // zRatio / 2^l and zRatio_HR / 2^l: phase z of slice k is k zr / zrh
@@ -252,7 +287,7 @@ struct XresArgs {
 // then the same smoothing, window sums and CP neighbour difference as
 // k_lk_accumulate (utils/calFlowCrossResolution.py:2101-2170).
 template <int MODE, int DIFF0, bool MASK>
-__global__ void __launch_bounds__(kAccThreads, 2) k_xres_accumulate(const __grid_constant__ XresArgs xa) {
+__global__ void __launch_bounds__(kAccThreads, 3) k_xres_accumulate(const __grid_constant__ XresArgs xa) {
   const IterArgs& a = xa.a;
   if (!*(volatile const int*)&a.st->active) return;
   extern __shared__ float4 smem4[];
@@ -282,7 +317,7 @@ __global__ void __launch_bounds__(kAccThreads, 2) k_xres_accumulate(const __grid
 // the motion itself and H(phase) (utils/calFlowCrossResolution.py:2205-2209).
 template <int MODE>
 __global__ void k_xres_finish(const FieldSrc f, float* __restrict__ phase, float* __restrict__ motion,
-                              float* __restrict__ sampled, const float* __restrict__ cref, int pxh, int pyh, int pzh,
+                              float* __restrict__ sampled, const float4* __restrict__ cref, int pxh, int pyh, int pzh,
                               int nx, int ny, int nz, double zr, double zrh) {
   WR_FOR_ROWS(nz * ny, row) {
     const int z = row / ny, y = row - z * ny;
@@ -301,7 +336,7 @@ __global__ void k_xres_finish(const FieldSrc f, float* __restrict__ phase, float
         phase[3 * i + 1] = py;
         phase[3 * i + 2] = pz;
       }
-      if (sampled) sampled[i] = spline_sample<float, float>(cref, pxh, pyh, pzh, px, py, pz);
+      if (sampled) sampled[i] = spline_sample_quads(cref, pxh, pyh, pzh, px, py, pz);
     }
   }
 }
