@@ -30,10 +30,12 @@ extern "C" {
  * (nzh, nyh, nxh).  p->precision must be WR_PREC_F32; p->zRatio is the
  * moving stack's z spacing (option["zRatio"]), zRatio_HR the reference's
  * (option["zRatio_HR"]).  has_mask_ref: a reference exclusion mask will be
- * passed (its spline coefficients need room).
+ * passed (its spline coefficients need room); has_phase_init: an initial
+ * phase will be passed.
  */
 WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nzh, int32_t nyh, int32_t nxh,
-                                  const WrLKParams* p, float zRatio_HR, int32_t has_mask_ref, size_t* bytes);
+                                  const WrLKParams* p, float zRatio_HR, int32_t has_mask_ref, int32_t has_phase_init,
+                                  size_t* bytes);
 
 /*
  * getMotion_v2 without the wrong-region correction.
@@ -43,6 +45,9 @@ WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nz
  *                  uint8 or NULL: option["mask_mov"] / ["mask_ref"], values
  *                  resized per level and excluded where > 0.5
  *   motion_init    (nz, ny, nx, 3) or NULL: option["motion"]
+ *   phase_init     (nz, ny, nx, 3) or NULL: option["phase"], the moving grid's
+ *                  map into the reference (per level resized and divided by
+ *                  the level's scale, :1978-1992); NULL: (x, y, z zRatio / zRatio_HR)
  *   p              layer, iter, r, zRatio, smoothPenalty, movRange, tol,
  *                  forced_updates (replay, -1 = off), flags (launch shape)
  * Outputs (any may be NULL): phase_out and motion_out (nz, ny, nx, 3),
@@ -51,7 +56,8 @@ WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nz
  */
 WR_API int wr_xres_register(const float* mov, int32_t nz, int32_t ny, int32_t nx, const float* ref, int32_t nzh,
                             int32_t nyh, int32_t nxh, const uint8_t* excl_mask_mov, const uint8_t* excl_mask_ref,
-                            const float* motion_init, const WrLKParams* p, float zRatio_HR, float* phase_out,
+                            const float* motion_init, const float* phase_init, const WrLKParams* p,
+                            float zRatio_HR, float* phase_out,
                             float* motion_out, float* ref_sampled_out, WrLKStats* stats, void* workspace,
                             size_t workspace_bytes, void* stream);
 

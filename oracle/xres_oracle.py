@@ -13,7 +13,8 @@ are relative to ``src/wholistic_registration``:
   (cross-resolution) grid
 * ``utils/calFlowCrossResolution.py:2031-2237``  ``optimize_layer_cross_resolution``
 * ``utils/calFlowCrossResolution.py:1904-2028``  phase composition, mask
-  resampling (threshold 0.5), motion / phase initialisation, CP grid, valid mask
+  resampling (threshold 0.5), motion / phase initialisation (``option["phase"]``
+  included), CP grid, valid mask
 * ``utils/calFlowCrossResolution.py:463-478, 1144-1154``  the continuous
   reference ``H``: ``map_coordinates(order=3, mode="nearest")``
 * ``utils/calFlowCrossResolution.py:41-272``  neighbour difference, error,
@@ -184,8 +185,15 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
                 up = imresize(prev[..., d], shape, method="bilinear")
                 motion[..., d] = up * 2 if d < 2 else up
 
-        X, Y, Z = np.indices(shape)
-        phase_cur = np.stack([X, Y, Z * zratio / zratio_hr], axis=-1).astype(np.float32)
+        phase_init = option.get("phase")
+        if phase_init is not None:
+            phase_init = np.asarray(phase_init, dtype=np.float32)
+            phase_cur = np.zeros(shape + (3,), dtype=np.float32)
+            for d in range(3):
+                phase_cur[..., d] = imresize(phase_init[..., d], shape) / (sz[d] / shape[d])
+        else:
+            X, Y, Z = np.indices(shape)
+            phase_cur = np.stack([X, Y, Z * zratio / zratio_hr], axis=-1).astype(np.float32)
         sps = sp * (2 * r + 1) ** 2
         xg = np.arange(r, x - 1, 2 * r + 1)
         yg = np.arange(r, y - 1, 2 * r + 1)

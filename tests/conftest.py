@@ -83,4 +83,6 @@ def load_xres_case(name):
     option = dict(meta)
     option.update({"mask_ref": arrays["mask_ref"].copy(), "mask_mov": arrays["mask_mov"].copy(),
                    "motion": arrays.get("motion_init"), "wrong_region_enable": False})
+    if "phase_init" in arrays:
+        option["phase"] = arrays["phase_init"]
     return arrays, option

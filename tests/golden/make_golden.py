@@ -261,6 +261,7 @@ XRES_CASES = {
     "xr_refwide_r2_l1": ((40, 40, 5), (48, 44, 10), 2.0, 1.0, 2, 1, 8, 1e-3, 0.05, True, False),
     "xr_z1_r3_l1": ((44, 40, 1), (44, 40, 3), 3.0, 1.0, 3, 1, 8, 1e-3, 0.05, False, False),
     "xr_refz1_r2_l0": ((36, 36, 4), (36, 36, 1), 1.0, 4.0, 2, 0, 6, 1e-3, 0.05, True, False),
+    "xr_phase_r3_l1": ((48, 44, 5), (48, 44, 10), 2.0, 1.0, 3, 1, 8, 1e-3, 0.05, False, "phase"),
 }
 
 
@@ -315,18 +316,28 @@ def make_xres_cases(root, out_dir):
             X, Y, Z = np.meshgrid(*[np.arange(n) for n in rs], indexing="ij")
             mref[((X - 0.7 * rs[0]) / (0.2 * rs[0])) ** 2 + ((Y - 0.6 * rs[1]) / (0.25 * rs[1])) ** 2 < 1] = 1
         init = None
-        if use_init:
+        phase0 = None
+        if use_init == "phase":
+            # an initial phase: the default map shifted by a smooth field in x and z
+            X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in ms], indexing="ij")
+            phase0 = np.stack([X + 0.6 * np.sin(Y / 8.0), Y - 0.3, Z * zr / zrh + 0.2 * np.cos(X / 11.0)],
+                              -1).astype(np.float32)
+        elif use_init:
             X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in ms], indexing="ij")
             init = np.stack([0.4 * np.sin(X / 9.0), 0.3 * np.cos(Y / 7.0), 0.1 + 0 * Z], -1).astype(np.float32)
             init += rng.normal(scale=0.05, size=init.shape).astype(np.float32)
         option = {"mask_ref": mref.copy(), "mask_mov": mmov.copy(), "layer": layer, "iter": it, "r": r,
                   "zRatio": zr, "zRatio_HR": zrh, "smoothPenalty": sp, "movRange": 5.0, "tol": tol,
                   "motion": init, "wrong_region_enable": False}
+        if phase0 is not None:
+            option["phase"] = phase0
         phase, motion, sampled = cf.getMotion_v2(mov.copy(), ref.copy(), option)
         rec = {"mov": mov, "ref": ref, "mask_mov": mmov, "mask_ref": mref, "phase": np.asarray(phase, np.float32),
                "motion": np.asarray(motion, np.float32), "ref_sampled": np.asarray(sampled, np.float64)}
         if init is not None:
             rec["motion_init"] = init
+        if phase0 is not None:
+            rec["phase_init"] = phase0
         np.savez_compressed(os.path.join(out_dir, f"xres_{name}.npz"), **rec)
         index[name] = {"layer": layer, "iter": it, "r": r, "zRatio": zr, "zRatio_HR": zrh, "tol": tol,
                        "smoothPenalty": sp, "movRange": 5.0}

@@ -118,10 +118,6 @@ def test_xres_rejects_unbuilt_options():
     opt["wrong_region_enable"] = True
     with pytest.raises(NotImplementedError):
         C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
-    opt = dict(option)
-    opt["phase"] = np.zeros(arrays["mov"].shape + (3,), np.float32)
-    with pytest.raises(NotImplementedError):
-        C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
 
 
 def _projection_case(seed=5):

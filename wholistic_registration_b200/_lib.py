@@ -211,9 +211,9 @@ def load():
         lib.wr_get_mask.argtypes = [ctypes.POINTER(WrVolume), ctypes.c_double, ctypes.c_double, vp, vp, vp, sz, vp]
         lib.wr_bwareafilt3.argtypes = [vp, i32, i32, i32, ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, sz, vp]
         P = ctypes.POINTER(WrLKParams)
-        lib.wr_xres_workspace_size.argtypes = [i32, i32, i32, i32, i32, i32, P, ctypes.c_float, i32,
+        lib.wr_xres_workspace_size.argtypes = [i32, i32, i32, i32, i32, i32, P, ctypes.c_float, i32, i32,
                                                ctypes.POINTER(sz)]
-        lib.wr_xres_register.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, vp, P, ctypes.c_float,
+        lib.wr_xres_register.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, vp, vp, P, ctypes.c_float,
                                          vp, vp, vp, vp, vp, sz, vp]
         i64_, f32_ = ctypes.c_int64, ctypes.c_float
         lib.wr_spline_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]

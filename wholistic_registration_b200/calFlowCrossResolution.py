@@ -26,9 +26,8 @@ tensors where the reference returns CuPy arrays.
 
 Not built here: the wrong-region correction the reference runs by default
 (``wrong_region_enable=True``: bad-region detection on the CP errors, a trap
-mask in reference space and two re-runs, :2240-2467) and an initial
-``option["phase"]``; both raise ``NotImplementedError`` instead of silently
-computing something else.  One optional key extends the options:
+mask in reference space and two re-runs, :2240-2467), which raises
+``NotImplementedError`` instead of silently computing something else.  One optional key extends the options:
 ``forced_updates`` (layer -> number of motion updates, replaying another
 run's iteration counts).
 """
@@ -52,19 +51,21 @@ class XresRegistrar:
     (zh, yh, xh) reference stack on one GPU (``wr_xres_register``)."""
 
     def __init__(self, shape_zyx, ref_shape_zyx, params: LKParams, zRatio_HR: float, has_mask_ref: bool = True,
-                 device=None):
+                 device=None, has_phase_init: bool = False):
         self.lib = _lib.load()
         self.shape = tuple(int(s) for s in shape_zyx)
         self.ref_shape = tuple(int(s) for s in ref_shape_zyx)
         self.params = params
         self.zRatio_HR = float(zRatio_HR)
         self.has_mask_ref = bool(has_mask_ref)
+        self.has_phase_init = bool(has_phase_init)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self._cp = params.to_c()
         nbytes = ctypes.c_size_t(0)
         _lib.check("wr_xres_workspace_size",
                    self.lib.wr_xres_workspace_size(*self.shape, *self.ref_shape, ctypes.byref(self._cp),
-                                                   self.zRatio_HR, int(self.has_mask_ref), ctypes.byref(nbytes)))
+                                                   self.zRatio_HR, int(self.has_mask_ref), int(self.has_phase_init),
+                                                   ctypes.byref(nbytes)))
         self.workspace_bytes = int(nbytes.value)
         self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
         self._ws_ptr = (self.workspace.data_ptr() + 255) // 256 * 256
@@ -81,10 +82,12 @@ class XresRegistrar:
         return t.data_ptr()
 
     def register(self, mov, ref, mask_mov=None, mask_ref=None, motion_init=None, phase_out=None, motion_out=None,
-                 sampled_out=None, stream=None):
+                 sampled_out=None, stream=None, phase_init=None):
         """(phase, motion, sampled) as (z, y, x, 3), (z, y, x, 3), (z, y, x) float32 tensors."""
         if mask_ref is not None and not self.has_mask_ref:
             raise ValueError("this registrar was built without room for a reference mask")
+        if phase_init is not None and not self.has_phase_init:
+            raise ValueError("this registrar was built without room for an initial phase")
         pm = self._check(mov, "mov", self.shape, (torch.float32,))
         pr = self._check(ref, "ref", self.ref_shape, (torch.float32,))
         if mask_mov is not None and mask_mov.dtype == torch.bool:
@@ -94,6 +97,7 @@ class XresRegistrar:
         pmm = self._check(mask_mov, "mask_mov", self.shape, (torch.uint8,))
         pmr = self._check(mask_ref, "mask_ref", self.ref_shape, (torch.uint8,))
         pin = self._check(motion_init, "motion_init", self.shape + (3,), (torch.float32,))
+        pph = self._check(phase_init, "phase_init", self.shape + (3,), (torch.float32,))
         new = lambda shp: torch.empty(shp, dtype=torch.float32, device=self.device)  # noqa: E731
         phase_out = new(self.shape + (3,)) if phase_out is None else phase_out
         motion_out = new(self.shape + (3,)) if motion_out is None else motion_out
@@ -102,7 +106,7 @@ class XresRegistrar:
                              (sampled_out, "sampled_out", self.shape)):
             self._check(t, name, shp, (torch.float32,))
         _lib.check("wr_xres_register",
-                   self.lib.wr_xres_register(pm, *self.shape, pr, *self.ref_shape, pmm, pmr, pin,
+                   self.lib.wr_xres_register(pm, *self.shape, pr, *self.ref_shape, pmm, pmr, pin, pph,
                                              ctypes.byref(self._cp), self.zRatio_HR, phase_out.data_ptr(),
                                              motion_out.data_ptr(), sampled_out.data_ptr(), self.stats_dev.data_ptr(),
                                              self._ws_ptr, self.workspace_bytes, _stream_ptr(stream)))
@@ -168,8 +172,6 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
     if bool(option.get("wrong_region_enable", True)):
         raise NotImplementedError("the wrong-region correction of getMotion_v2 is not built on this path; "
                                   "pass option['wrong_region_enable'] = False")
-    if option.get("phase") is not None:
-        raise NotImplementedError("an initial option['phase'] is not supported on this path")
     as_torch = isinstance(data_mov, torch.Tensor)
     device = data_mov.device if as_torch and data_mov.is_cuda else torch.device("cuda", torch.cuda.current_device())
     mov = _to_device(data_mov, device, torch.float32)
@@ -180,6 +182,8 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
     mask_ref = _mask_to_device(option["mask_ref"], ref_xyz, device)
     init = option.get("motion")
     init_t = None if init is None else _to_device(init, device, torch.float32)
+    phase0 = option.get("phase")
+    phase_t = None if phase0 is None else _to_device(phase0, device, torch.float32)
     params = LKParams(
         layer=int(option["layer"]), iter=int(option["iter"]), r=int(option["r"]),
         zRatio=float(option.get("zRatio", 1.0)), movRange=float(option.get("movRange", 5.0)),
@@ -188,16 +192,17 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
     zr_hr = float(option["zRatio_HR"])
     key = (tuple(mov.shape), tuple(ref.shape), params.layer, params.iter, params.r, params.zRatio, params.movRange,
            params.smoothPenalty, params.tol, tuple(sorted(params.forced_updates.items())), zr_hr,
-           mask_ref is not None, str(device))
+           mask_ref is not None, phase_t is not None, str(device))
     reg = _cache.get(key)
     if reg is None:
         if len(_cache) > 4:
             _cache.clear()
-        reg = XresRegistrar(tuple(mov.shape), tuple(ref.shape), params, zr_hr, mask_ref is not None, device)
+        reg = XresRegistrar(tuple(mov.shape), tuple(ref.shape), params, zr_hr, mask_ref is not None, device,
+                            has_phase_init=phase_t is not None)
         _cache[key] = reg
     global last_registrar
     last_registrar = reg
-    phase, motion, sampled = reg.register(mov, ref, mask_mov, mask_ref, init_t)
+    phase, motion, sampled = reg.register(mov, ref, mask_mov, mask_ref, init_t, phase_init=phase_t)
     if verbose:
         log, err = reg.error_log()
         for name, lv in log.items():

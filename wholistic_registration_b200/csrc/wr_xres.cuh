@@ -279,6 +279,7 @@ struct XresArgs {
   const double* cmask;     // padded spline coefficients of its 0/1 exclusion mask, or null
   int pxh, pyh, pzh;       // padded extent
   double zr, zrh;          // zRatio / 2^l and zRatio_HR / 2^l: phase z of slice k is k zr / zrh
+  const float4* phase0;    // the level's initial phase (x, y, z, -), or null for (x, y, z zr / zrh)
 };
 
 // One launch of the cross-resolution iteration: per voxel the residual
@@ -313,19 +314,32 @@ __global__ void __launch_bounds__(kAccThreads, 3) k_xres_accumulate(const __grid
   }
 }
 
+// (n, 3) interleaved float -> float4 (the finest level's initial phase: an
+// exact copy, as a resize at scale 1 is)
+__global__ void k_pack_xyz(const float* __restrict__ in, float4* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
+}
+
 // Final outputs at the finest level: phase = (x, y, z zr / zrh) + motion,
 // the motion itself and H(phase) (utils/calFlowCrossResolution.py:2205-2209).
 template <int MODE>
 __global__ void k_xres_finish(const FieldSrc f, float* __restrict__ phase, float* __restrict__ motion,
                               float* __restrict__ sampled, const float4* __restrict__ cref, int pxh, int pyh, int pzh,
-                              int nx, int ny, int nz, double zr, double zrh) {
+                              int nx, int ny, int nz, double zr, double zrh, const float4* __restrict__ phase0) {
   WR_FOR_ROWS(nz * ny, row) {
     const int z = row / ny, y = row - z * ny;
     const float fz0 = (float)(((double)z * zr) / zrh);
     WR_FOR_COLS(nx, x) {
       const float3 m = eval_field<MODE>(f, x, y, z);
       const size_t i = ((size_t)z * ny + y) * nx + x;
-      const float px = (float)x + m.x, py = (float)y + m.y, pz = fz0 + m.z;
+      float px = (float)x + m.x, py = (float)y + m.y, pz = fz0 + m.z;
+      if (phase0) {
+        const float4 q = phase0[i];
+        px = q.x + m.x;
+        py = q.y + m.y;
+        pz = q.z + m.z;
+      }
       if (motion) {
         motion[3 * i] = m.x;
         motion[3 * i + 1] = m.y;
