@@ -357,7 +357,7 @@ def run_ours(args, wl, rank, world, local_rank):
         host_warp = [torch.empty(wl["shape"], dtype=torch.float32).pin_memory() for _ in range(2)]
         series = SeriesRegistrar(template, params, mask_ref=excl, mask_mov=excl)
         series.reg.tune_flags = reg.tune_flags
-        ek = max(4, min(args.steps, 16))
+        ek = max(4, args.steps)   # one pass of the pipeline: fill and drain amortised over the timed steps
         seq = [host_frames[i % n_host] for i in range(ek)]
         outs_m = [host_motion[i % 2] for i in range(ek)]
         outs_w = [host_warp[i % 2] for i in range(ek)]
