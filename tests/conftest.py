@@ -86,3 +86,20 @@ def load_xres_case(name):
     if "phase_init" in arrays:
         option["phase"] = arrays["phase_init"]
     return arrays, option
+
+
+def xres_wr_case_names():
+    import glob
+
+    return sorted(os.path.basename(f)[len("xreswr_"):-4] for f in glob.glob(os.path.join(GOLDEN, "xreswr_*.npz")))
+
+
+def load_xres_wr_case(name):
+    """(arrays, option) for a getMotion_v2 case with the wrong-region correction
+    on: the inputs of the xres case, the outputs of the reference's run with
+    the correction."""
+    arrays, option = load_xres_case(name)
+    out = dict(np.load(os.path.join(GOLDEN, f"xreswr_{name}.npz")))
+    arrays.update(out)
+    option["wrong_region_enable"] = True
+    return arrays, option

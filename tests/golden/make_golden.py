@@ -265,6 +265,12 @@ XRES_CASES = {
 }
 
 
+# cases re-run with wrong_region_enable=True (accepted and rejected corrections,
+# a low valid ratio, an empty trap mask)
+XRES_WR_CASES = ("xr_mask_r2_l1", "xr_small_r3_l1", "xr_init_r4_l2", "xr_ragged_r3_l2", "xr_refz1_r2_l0",
+                 "xr_z1_r3_l1", "xr_phase_r3_l1")
+
+
 def xres_pair(mov_shape, ref_shape, zr, zr_hr, seed):
     """Moving and reference stacks of one blob field sampled at z spacings zr
     and zr_hr (physical units per z index), the moving one displaced by a
@@ -344,6 +350,19 @@ def make_xres_cases(root, out_dir):
         print(f"{name}: mov {ms} ref {rs} max |motion| {float(np.abs(motion).max()):.3f}")
     with open(os.path.join(out_dir, "xres_cases.json"), "w") as fh:
         json.dump(index, fh, indent=1, sort_keys=True)
+    # the same inputs with the wrong-region correction on (the reference's default)
+    for name in XRES_WR_CASES:
+        d = dict(np.load(os.path.join(out_dir, f"xres_{name}.npz")))
+        meta = index[name]
+        option = dict(meta)
+        option.update({"mask_ref": d["mask_ref"].copy(), "mask_mov": d["mask_mov"].copy(),
+                       "motion": d.get("motion_init"), "wrong_region_enable": True})
+        if "phase_init" in d:
+            option["phase"] = d["phase_init"]
+        phase, motion, sampled = cf.getMotion_v2(d["mov"].copy(), d["ref"].copy(), option)
+        np.savez_compressed(os.path.join(out_dir, f"xreswr_{name}.npz"), phase=np.asarray(phase, np.float32),
+                            motion=np.asarray(motion, np.float32), ref_sampled=np.asarray(sampled, np.float64))
+        print(f"{name} (wrong-region correction on): max |motion| {float(np.abs(motion).max()):.3f}")
 
 
 def main():

@@ -7,7 +7,8 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_motion_case, load_xres_case, motion_case_names, option_from_case, xres_case_names
+from conftest import (GOLDEN, load_motion_case, load_xres_case, load_xres_wr_case, motion_case_names,
+                      option_from_case, xres_case_names, xres_wr_case_names)
 from oracle import lk_oracle as O
 
 PRIM = os.path.join(GOLDEN, "primitives.npz")
@@ -135,3 +136,16 @@ def test_xres_spline_restatement_matches_scipy():
         got = X.cubic_sample(coef, *pts)
         want = X.cubic_sample_scipy(vol, *pts)
         np.testing.assert_allclose(got, want, rtol=0, atol=tol * np.abs(vol).max())
+
+
+@pytest.mark.parametrize("name", xres_wr_case_names())
+def test_xres_wrong_region_oracle_matches_reference(name):
+    """getMotion_v2 with the wrong-region correction: the restatement
+    reproduces the reference's run (detection, trap mask, re-runs, choice)."""
+    from oracle import xres_oracle as X
+
+    arrays, option = load_xres_wr_case(name)
+    phase, motion, sampled, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], option)
+    np.testing.assert_allclose(motion, arrays["motion"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(phase, arrays["phase"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(sampled, arrays["ref_sampled"], rtol=1e-12, atol=1e-9)
