@@ -4,8 +4,7 @@
  * Replaces the reference entry point (path relative to src/wholistic_registration/)
  *
  *   wr_xres_register   utils/calFlowCrossResolution.py:2470-2663
- *                      getMotion_v2(data_mov, data_ref, option) with
- *                      option["wrong_region_enable"] = False
+ *                      getMotion_v2(data_mov, data_ref, option)
  *
  * The moving stack lives on the iteration grid, the reference stack on its own
  * grid (another z spacing, possibly other x / y extents); the reference is
@@ -26,6 +25,24 @@ extern "C" {
 #endif
 
 /*
+ * getMotion_v2's wrong-region correction (utils/calFlowCrossResolution.py:
+ * 2240-2467, option keys in brackets): after each layer's optimisation, CPs
+ * whose local error is a robust outlier are grouped into regions, their
+ * voxels' phases seed a trap mask in reference space, and the layer is
+ * re-run with the trap excluded and then refined with the original masks;
+ * the refined result is kept when its error is lower.  enable = 0: off.
+ */
+typedef struct WrXresWrongRegion {
+  int32_t enable;              /* ["wrong_region_enable"] */
+  int32_t metric;              /* ["wrong_region_metric"]: 0 "mse", 1 "mae" */
+  float mad_threshold;         /* ["wrong_region_mad_threshold"], 3.0 */
+  int32_t min_component_size;  /* ["wrong_region_min_component_size"], 2 */
+  float expand_radius_xy;      /* ["expand_radius_xy"], 2.0 (divided by 2^layer) */
+  float sigma_grad;            /* ["sigma_grad"], 1.0 */
+  float intensity_k;           /* ["intensity_k"], 2.0 */
+} WrXresWrongRegion;
+
+/*
  * Workspace bytes for a moving stack (nz, ny, nx) and a reference stack
  * (nzh, nyh, nxh).  p->precision must be WR_PREC_F32; p->zRatio is the
  * moving stack's z spacing (option["zRatio"]), zRatio_HR the reference's
@@ -35,10 +52,13 @@ extern "C" {
  */
 WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nzh, int32_t nyh, int32_t nxh,
                                   const WrLKParams* p, float zRatio_HR, int32_t has_mask_ref, int32_t has_phase_init,
-                                  size_t* bytes);
+                                  const WrXresWrongRegion* wr, size_t* bytes);
 
 /*
- * getMotion_v2 without the wrong-region correction.
+ * getMotion_v2; wr NULL or wr->enable = 0 runs it without the wrong-region
+ * correction (option["wrong_region_enable"] = False).  The correction needs
+ * p->iter >= 2 to change anything (with one iteration no pass updates the
+ * motion) and at most 4096 CPs per slice.
  *   mov            (nz, ny, nx) float32 moving stack
  *   ref            (nzh, nyh, nxh) float32 reference stack
  *   excl_mask_mov  (nz, ny, nx) uint8 or NULL; excl_mask_ref (nzh, nyh, nxh)
@@ -57,7 +77,7 @@ WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nz
 WR_API int wr_xres_register(const float* mov, int32_t nz, int32_t ny, int32_t nx, const float* ref, int32_t nzh,
                             int32_t nyh, int32_t nxh, const uint8_t* excl_mask_mov, const uint8_t* excl_mask_ref,
                             const float* motion_init, const float* phase_init, const WrLKParams* p,
-                            float zRatio_HR, float* phase_out,
+                            float zRatio_HR, const WrXresWrongRegion* wr, float* phase_out,
                             float* motion_out, float* ref_sampled_out, WrLKStats* stats, void* workspace,
                             size_t workspace_bytes, void* stream);
 

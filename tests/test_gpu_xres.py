@@ -1,6 +1,6 @@
-"""Cross-resolution registration (getMotion_v2, wrong-region correction off)
-on the GPU against fixtures from the reference's own run and against the
-oracle restatement.
+"""Cross-resolution registration (getMotion_v2, with and without the
+wrong-region correction) on the GPU against fixtures from the reference's
+own runs and against the oracle restatement.
 
 Tolerances: motion and phase within 1e-3 voxel (max abs) wherever the
 reference's own result is stable, the sampled reference within 1e-4 relative
@@ -28,7 +28,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import load_xres_case, xres_case_names
+from conftest import load_xres_case, load_xres_wr_case, xres_case_names, xres_wr_case_names
 
 pytestmark = pytest.mark.gpu
 
@@ -116,8 +116,42 @@ def test_xres_rejects_unbuilt_options():
     arrays, option = load_xres_case("xr_small_r3_l1")
     opt = dict(option)
     opt["wrong_region_enable"] = True
+    opt["wrong_region_exclude_mode"] = "highresidual"
     with pytest.raises(NotImplementedError):
         C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
+    opt["wrong_region_exclude_mode"] = "direct"
+    opt["wrong_region_metric"] = "l2"
+    with pytest.raises(ValueError):
+        C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
+
+
+@pytest.mark.parametrize("name", xres_wr_case_names())
+def test_xres_wrong_region_matches_reference_run(name):
+    """getMotion_v2 with the wrong-region correction (the reference's
+    default): the same bound as without it, the spread measured by the oracle
+    running the correction under the same perturbations (a perturbation that
+    flips a control point's outlier status or the keep / discard choice shows
+    up there as spread).  The device log must hold the updates of every pass
+    the oracle ran (one pass, or three when a trap was built)."""
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    arrays, option = load_xres_wr_case(name)
+    phase, motion, sampled = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(option))
+    _, _, _, log = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option))
+    dev_log, _ = C.last_registrar.error_log()
+    want = _updates_per_level(log)
+    got = {int(k.split("_")[1]): len(v["max_diff_motion"]) for k, v in dev_log.items()}
+    assert got == want, f"updates per level {got} vs reference {want}"
+    spread = _reference_spread(arrays, option, arrays["motion"])
+    bound = 1e-3 + 3.0 * spread
+    err_m = np.abs(motion - arrays["motion"])
+    err_p = np.abs(phase - arrays["phase"])
+    assert (err_m > bound).mean() <= 1e-3, f"motion: max excess {float((err_m - bound).max()):.3g}"
+    assert (err_p > bound).mean() <= 1e-3, f"phase: max excess {float((err_p - bound).max()):.3g}"
+    span = float(np.ptp(arrays["ref_sampled"])) or 1.0
+    own = X.cubic_sample_scipy(arrays["ref"].astype(np.float64), phase[..., 0], phase[..., 1], phase[..., 2])
+    np.testing.assert_allclose(sampled, own, rtol=0, atol=1e-4 * span)
 
 
 def _projection_case(seed=5):

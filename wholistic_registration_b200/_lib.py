@@ -78,6 +78,19 @@ EXPORTS = (
 )
 
 
+class WrXresWrongRegion(ctypes.Structure):
+    """include/wr_xres.h: getMotion_v2's wrong-region correction options."""
+    _fields_ = [
+        ("enable", ctypes.c_int32),
+        ("metric", ctypes.c_int32),
+        ("mad_threshold", ctypes.c_float),
+        ("min_component_size", ctypes.c_int32),
+        ("expand_radius_xy", ctypes.c_float),
+        ("sigma_grad", ctypes.c_float),
+        ("intensity_k", ctypes.c_float),
+    ]
+
+
 class WrVolume(ctypes.Structure):
     _fields_ = [
         ("data", ctypes.c_void_p),
@@ -211,10 +224,11 @@ def load():
         lib.wr_get_mask.argtypes = [ctypes.POINTER(WrVolume), ctypes.c_double, ctypes.c_double, vp, vp, vp, sz, vp]
         lib.wr_bwareafilt3.argtypes = [vp, i32, i32, i32, ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, sz, vp]
         P = ctypes.POINTER(WrLKParams)
-        lib.wr_xres_workspace_size.argtypes = [i32, i32, i32, i32, i32, i32, P, ctypes.c_float, i32, i32,
+        WR = ctypes.POINTER(WrXresWrongRegion)
+        lib.wr_xres_workspace_size.argtypes = [i32, i32, i32, i32, i32, i32, P, ctypes.c_float, i32, i32, WR,
                                                ctypes.POINTER(sz)]
         lib.wr_xres_register.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, vp, vp, P, ctypes.c_float,
-                                         vp, vp, vp, vp, vp, sz, vp]
+                                         WR, vp, vp, vp, vp, vp, sz, vp]
         i64_, f32_ = ctypes.c_int64, ctypes.c_float
         lib.wr_spline_workspace_size.argtypes = [i32, i32, i32, ctypes.POINTER(sz)]
         lib.wr_spline_sample.argtypes = [vp, i32, i32, i32, vp, i64_, vp, vp, sz, vp]

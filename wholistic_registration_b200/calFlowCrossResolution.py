@@ -24,10 +24,11 @@ The module also carries the continuous reference ``H``
 :571-660 + 700-876) with the reference's signatures; they return CUDA torch
 tensors where the reference returns CuPy arrays.
 
-Not built here: the wrong-region correction the reference runs by default
+The wrong-region correction the reference runs by default
 (``wrong_region_enable=True``: bad-region detection on the CP errors, a trap
-mask in reference space and two re-runs, :2240-2467), which raises
-``NotImplementedError`` instead of silently computing something else.  One optional key extends the options:
+mask in reference space and two re-runs, :2240-2467) runs on the device too;
+its ``wrong_region_exclude_mode="highresidual"`` variant is not built and
+raises ``NotImplementedError`` instead of silently computing something else.  One optional key extends the options:
 ``forced_updates`` (layer -> number of motion updates, replaying another
 run's iteration counts).
 """
@@ -51,7 +52,7 @@ class XresRegistrar:
     (zh, yh, xh) reference stack on one GPU (``wr_xres_register``)."""
 
     def __init__(self, shape_zyx, ref_shape_zyx, params: LKParams, zRatio_HR: float, has_mask_ref: bool = True,
-                 device=None, has_phase_init: bool = False):
+                 device=None, has_phase_init: bool = False, wrong_region=None):
         self.lib = _lib.load()
         self.shape = tuple(int(s) for s in shape_zyx)
         self.ref_shape = tuple(int(s) for s in ref_shape_zyx)
@@ -61,15 +62,20 @@ class XresRegistrar:
         self.has_phase_init = bool(has_phase_init)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self._cp = params.to_c()
+        # the wrong-region correction's options (None: off), a WrXresWrongRegion
+        self._wr = wrong_region
         nbytes = ctypes.c_size_t(0)
         _lib.check("wr_xres_workspace_size",
                    self.lib.wr_xres_workspace_size(*self.shape, *self.ref_shape, ctypes.byref(self._cp),
                                                    self.zRatio_HR, int(self.has_mask_ref), int(self.has_phase_init),
-                                                   ctypes.byref(nbytes)))
+                                                   self._wr_ptr(), ctypes.byref(nbytes)))
         self.workspace_bytes = int(nbytes.value)
         self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
         self._ws_ptr = (self.workspace.data_ptr() + 255) // 256 * 256
         self.stats_dev = torch.zeros(ctypes.sizeof(_lib.WrLKStats), dtype=torch.uint8, device=self.device)
+
+    def _wr_ptr(self):
+        return ctypes.byref(self._wr) if self._wr is not None else None
 
     @staticmethod
     def _check(t, name, shape, dtypes):
@@ -107,7 +113,8 @@ class XresRegistrar:
             self._check(t, name, shp, (torch.float32,))
         _lib.check("wr_xres_register",
                    self.lib.wr_xres_register(pm, *self.shape, pr, *self.ref_shape, pmm, pmr, pin, pph,
-                                             ctypes.byref(self._cp), self.zRatio_HR, phase_out.data_ptr(),
+                                             ctypes.byref(self._cp), self.zRatio_HR, self._wr_ptr(),
+                                             phase_out.data_ptr(),
                                              motion_out.data_ptr(), sampled_out.data_ptr(), self.stats_dev.data_ptr(),
                                              self._ws_ptr, self.workspace_bytes, _stream_ptr(stream)))
         return phase_out, motion_out, sampled_out
@@ -169,9 +176,19 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
     Returns (phase_new, motion_current, data_ref_sampled) in the reference's
     (x, y, z[, 3]) layout.
     """
+    wr = None
     if bool(option.get("wrong_region_enable", True)):
-        raise NotImplementedError("the wrong-region correction of getMotion_v2 is not built on this path; "
-                                  "pass option['wrong_region_enable'] = False")
+        metric = str(option.get("wrong_region_metric", "mse")).lower()
+        if metric not in ("mse", "mae"):
+            raise ValueError("metric must be 'mse' or 'mae'")
+        if option.get("wrong_region_exclude_mode", "direct") != "direct":
+            raise NotImplementedError("wrong_region_exclude_mode 'highresidual' is not built on this path; "
+                                      "the default 'direct' is")
+        wr = _lib.WrXresWrongRegion(1, 0 if metric == "mse" else 1,
+                                    float(option.get("wrong_region_mad_threshold", 3.0)),
+                                    int(option.get("wrong_region_min_component_size", 2)),
+                                    float(option.get("expand_radius_xy", 2.0)), float(option.get("sigma_grad", 1.0)),
+                                    float(option.get("intensity_k", 2.0)))
     as_torch = isinstance(data_mov, torch.Tensor)
     device = data_mov.device if as_torch and data_mov.is_cuda else torch.device("cuda", torch.cuda.current_device())
     mov = _to_device(data_mov, device, torch.float32)
@@ -192,13 +209,14 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
     zr_hr = float(option["zRatio_HR"])
     key = (tuple(mov.shape), tuple(ref.shape), params.layer, params.iter, params.r, params.zRatio, params.movRange,
            params.smoothPenalty, params.tol, tuple(sorted(params.forced_updates.items())), zr_hr,
-           mask_ref is not None, phase_t is not None, str(device))
+           mask_ref is not None, phase_t is not None,
+           None if wr is None else tuple(getattr(wr, f) for f, _ in wr._fields_), str(device))
     reg = _cache.get(key)
     if reg is None:
         if len(_cache) > 4:
             _cache.clear()
         reg = XresRegistrar(tuple(mov.shape), tuple(ref.shape), params, zr_hr, mask_ref is not None, device,
-                            has_phase_init=phase_t is not None)
+                            has_phase_init=phase_t is not None, wrong_region=wr)
         _cache[key] = reg
     global last_registrar
     last_registrar = reg

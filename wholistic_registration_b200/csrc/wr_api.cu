@@ -15,8 +15,11 @@
 #include "wr_kernels.cuh"
 #include "wr_plan.h"
 #include "wr_xres.cuh"
+#include "wr_xres_wr.cuh"
 #include "wr_xres.h"
 #include <cmath>
+#include <algorithm>
+#include <cub/cub.cuh>
 
 namespace wr {
 

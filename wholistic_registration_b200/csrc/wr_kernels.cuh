@@ -1299,13 +1299,15 @@ constexpr float kMotionTol = 1e-3f;
 __device__ __forceinline__ void k_post_body(LKState* st, int level, int forced, int defer, float md_tol) {
   if (!st->do_update) return;
   WrLKStats& S = st->stats;
-  const int u = st->n_updates;
-  st->n_updates = u + 1;
-  S.updates[level] = u + 1;
+  // the level's log runs on across passes (the cross-resolution correction
+  // re-runs a level): its slot is the level's update count, not this pass's
+  const int slot = S.updates[level];
+  st->n_updates += 1;
+  S.updates[level] = slot + 1;
   st->do_update = 0;
   if (defer) return;
   const float md = __uint_as_float(st->maxdiff_bits);
-  if (u < WR_MAX_ITERS) S.max_diff_motion[level][u] = (double)md;
+  if (slot < WR_MAX_ITERS) S.max_diff_motion[level][slot] = (double)md;
   if (forced < 0 && md < md_tol) st->active = 0;
   st->maxdiff_bits = 0u;
 }
@@ -1321,7 +1323,8 @@ __global__ void k_post(LKState* st, int level, int forced, int defer, float md_t
 __device__ __forceinline__ void k_first_post_body(LKState* st, int level, int forced, float md_tol) {
   if (!st->active) return;
   const float md = __uint_as_float(st->maxdiff_bits);
-  st->stats.max_diff_motion[level][0] = (double)md;
+  const int slot = st->stats.updates[level] - 1;   // this pass's first update
+  if (slot >= 0 && slot < WR_MAX_ITERS) st->stats.max_diff_motion[level][slot] = (double)md;
   if (forced < 0 && md < md_tol) st->active = 0;
   st->maxdiff_bits = 0u;
 }

@@ -280,6 +280,8 @@ struct XresArgs {
   int pxh, pyh, pzh;       // padded extent
   double zr, zrh;          // zRatio / 2^l and zRatio_HR / 2^l: phase z of slice k is k zr / zrh
   const float4* phase0;    // the level's initial phase (x, y, z, -), or null for (x, y, z zr / zrh)
+  float* it_out;           // non-null: every voxel's It_raw (mov - H(phase)) is stored here,
+  uint8_t* ex_out;         //   and its exclusion flag here (the end-of-pass evaluation)
 };
 
 // One launch of the cross-resolution iteration: per voxel the residual

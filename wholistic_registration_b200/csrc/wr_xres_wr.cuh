@@ -1,0 +1,419 @@
+// Device kernels of getMotion_v2's wrong-region correction
+// (utils/calFlowCrossResolution.py:1190-1900, 2240-2467): the residual and
+// validity of a finished pass, control-point errors, bad-region detection on
+// the CP grid, and the trap mask grown in reference space.
+//
+// Included by wr_api.cu after wr_xres.cuh.
+#pragma once
+
+namespace wr {
+
+// residual = 3x3 box (edge-replicated, in-plane) of It_raw, 0 where excluded;
+// valid = !excluded (utils/calFlowCrossResolution.py:2101-2112)
+__global__ void k_wr_residual(const float* __restrict__ it, const uint8_t* __restrict__ ex, float* __restrict__ res,
+                              int nx, int ny, int nz) {
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    WR_FOR_COLS(nx, x) {
+      const size_t i = (size_t)row * nx + x;
+      if (ex[i]) {
+        res[i] = 0.f;
+        continue;
+      }
+      double s = 0.0;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const float* r = it + ((size_t)z * ny + clampi(y + dy, 0, ny - 1)) * nx;
+        for (int dx = -1; dx <= 1; ++dx) s += (double)r[clampi(x + dx, 0, nx - 1)];
+      }
+      res[i] = (float)(s * (double)(1.f / 9.f));
+    }
+  }
+}
+
+// err_cp = window mean of residual^2 (metric 0) or |residual| (metric 1) at
+// each CP, the window edge-replicated (get_local_error_on_control_points,
+// :1190-1222); one thread per CP.
+__global__ void k_wr_cp_error(const float* __restrict__ res, double* __restrict__ err, int nx, int ny, int nz, int r,
+                              int ncx, int ncy, int metric) {
+  const long long ncp = (long long)ncx * ncy * nz;
+  const int w = 2 * r + 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncp; i += (long long)gridDim.x * blockDim.x) {
+    const int cx = (int)(i % ncx);
+    const long long rest = i / ncx;
+    const int cy = (int)(rest % ncy), z = (int)(rest / ncy);
+    const int x0 = r + cx * w, y0 = r + cy * w;
+    double s = 0.0;
+    for (int dy = -r; dy <= r; ++dy) {
+      const float* row = res + ((size_t)z * ny + clampi(y0 + dy, 0, ny - 1)) * nx;
+      for (int dx = -r; dx <= r; ++dx) {
+        const double v = row[clampi(x0 + dx, 0, nx - 1)];
+        s += metric == 0 ? v * v : fabs(v);
+      }
+    }
+    err[i] = s * (double)(1.f / (float)(w * w));
+  }
+}
+
+// Median of v[0..n) (NumPy: the mean of the two middle values for even n)
+// by a bitonic sort of the block's shared buffer (n <= capacity, a power of
+// two); the buffer is left sorted.
+__device__ double block_median(double* buf, int n, int cap) {
+  for (int i = n + threadIdx.x; i < cap; i += blockDim.x) buf[i] = INFINITY;
+  __syncthreads();
+  for (int k = 2; k <= cap; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+        const int p = i ^ j;
+        if (p > i) {
+          const bool up = (i & k) == 0;
+          const double a = buf[i], b = buf[p];
+          if ((a > b) == up) { buf[i] = b; buf[p] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const double m = (n & 1) ? buf[n / 2] : (buf[n / 2 - 1] + buf[n / 2]) / 2.0;
+  __syncthreads();
+  return m;
+}
+
+constexpr int kWrMaxCp = 4096;   // CPs per slice the detection handles (shared-memory sort)
+
+struct WrBox { int x0, x1, y0, y1, z; };
+
+// One CTA per z slice (build_bad_region_mask_from_cp_error, :1570-1787):
+// robust z-scores of the slice's CP errors (median / MAD over the inner CPs
+// when the grid has more than 144), significant CPs joined 4-connected in the
+// slice, components of at least min_size CPs widened by ceil(1.5 r) voxels
+// to boxes (appended to boxes, count in *nbox).
+__global__ void k_wr_bad_regions(const double* __restrict__ err, int ncx, int ncy, int r, int nx, int ny,
+                                 float mad_threshold, int min_size, WrBox* __restrict__ boxes, int* __restrict__ nbox,
+                                 int max_boxes) {
+  extern __shared__ double wr_sm[];
+  const int z = blockIdx.x;
+  const int n = ncx * ncy;
+  int cap = 1;
+  while (cap < n) cap <<= 1;
+  double* buf = wr_sm;                                              // cap
+  int* lab = reinterpret_cast<int*>(buf + cap);                     // n
+  int* size = lab + n;                                              // n
+  int* bb = size + n;                                               // 4 n: min x, max x, min y, max y
+  __shared__ int changed;
+  const double* e = err + (size_t)z * n;
+  const bool inner = n > 144 && ncx > 2 && ncy > 2;
+  const int sx0 = inner ? 1 : 0, sx1 = inner ? ncx - 1 : ncx, sy0 = inner ? 1 : 0, sy1 = inner ? ncy - 1 : ncy;
+  const int wsub = sx1 - sx0, m = wsub * (sy1 - sy0);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const int a = i % wsub, b = i / wsub;
+    buf[i] = e[(sy0 + b) * ncx + sx0 + a];
+  }
+  __syncthreads();
+  const double med = block_median(buf, m, cap);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const int a = i % wsub, b = i / wsub;
+    buf[i] = fabs(e[(sy0 + b) * ncx + sx0 + a] - med);
+  }
+  __syncthreads();
+  const double mad = block_median(buf, m, cap);
+  const double eps = 1e-12;
+  // labels: index + 1 for significant CPs, 0 otherwise
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int a = i % ncx, b = i / ncx;
+    bool sig = false;
+    if (a >= sx0 && a < sx1 && b >= sy0 && b < sy1 && !(mad < eps))
+      sig = fabs(e[i] - med) / (1.4826 * mad + eps) > (double)mad_threshold;
+    lab[i] = sig ? i + 1 : 0;
+  }
+  __syncthreads();
+  // 4-connected components by minimum-label propagation (at most n rounds)
+  for (int round = 0; round < n; ++round) {
+    if (threadIdx.x == 0) changed = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int l = lab[i];
+      if (!l) continue;
+      const int a = i % ncx, b = i / ncx;
+      int mn = l;
+      if (a > 0 && lab[i - 1]) mn = min(mn, lab[i - 1]);
+      if (a + 1 < ncx && lab[i + 1]) mn = min(mn, lab[i + 1]);
+      if (b > 0 && lab[i - ncx]) mn = min(mn, lab[i - ncx]);
+      if (b + 1 < ncy && lab[i + ncx]) mn = min(mn, lab[i + ncx]);
+      if (mn < l) {
+        atomicMin(&lab[i], mn);
+        changed = 1;
+      }
+    }
+    __syncthreads();
+    if (!changed) break;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    size[i] = 0;
+    bb[4 * i] = 1 << 30; bb[4 * i + 1] = -1; bb[4 * i + 2] = 1 << 30; bb[4 * i + 3] = -1;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int l = lab[i];
+    if (!l) continue;
+    const int root = l - 1, a = i % ncx, b = i / ncx;
+    atomicAdd(&size[root], 1);
+    atomicMin(&bb[4 * root], a); atomicMax(&bb[4 * root + 1], a);
+    atomicMin(&bb[4 * root + 2], b); atomicMax(&bb[4 * root + 3], b);
+  }
+  __syncthreads();
+  const int w = 2 * r + 1, dx = (int)ceil(1.5 * (double)r);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (size[i] < max(min_size, 1)) continue;
+    const int k = atomicAdd(nbox, 1);
+    if (k >= max_boxes) continue;
+    WrBox bx;
+    bx.x0 = max(0, r + bb[4 * i] * w - dx);
+    bx.x1 = min(nx - 1, r + bb[4 * i + 1] * w + dx);
+    bx.y0 = max(0, r + bb[4 * i + 2] * w - dx);
+    bx.y1 = min(ny - 1, r + bb[4 * i + 3] * w + dx);
+    bx.z = z;
+    boxes[k] = bx;
+  }
+}
+
+// bad = inside one of the boxes of the voxel's slice, and valid
+__global__ void k_wr_bad_mask(const WrBox* __restrict__ boxes, const int* __restrict__ nbox, const uint8_t* __restrict__ ex,
+                              uint8_t* __restrict__ bad, int nx, int ny, int nz, int max_boxes) {
+  const int nb = min(*nbox, max_boxes);
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    WR_FOR_COLS(nx, x) {
+      bool in = false;
+      for (int k = 0; k < nb && !in; ++k) {
+        const WrBox b = boxes[k];
+        in = b.z == z && x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1;
+      }
+      const size_t i = (size_t)row * nx + x;
+      bad[i] = (in && !ex[i]) ? 1 : 0;
+    }
+  }
+}
+
+// phase of a finished pass at a voxel of the iteration grid
+template <int MODE>
+__device__ __forceinline__ float3 wr_phase(const FieldSrc& f, const float4* phase0, int x, int y, int z, float fz0,
+                                           size_t i) {
+  const float3 m = eval_field<MODE>(f, x, y, z);
+  if (phase0) {
+    const float4 q = phase0[i];
+    return make_float3(q.x + m.x, q.y + m.y, q.z + m.z);
+  }
+  return make_float3((float)x + m.x, (float)y + m.y, fz0 + m.z);
+}
+
+// Seeds: rint(phase) of the bad voxels inside the reference level.
+// pass 0: bounding box (bbox[0..5] = min x, max x, min y, max y, min z, max z)
+// pass 1: seed[(z - oz) * sy * sx + (y - oy) * sx + (x - ox)] = 1 in the ROI.
+template <int MODE>
+__global__ void k_wr_seeds(const FieldSrc f, const float4* __restrict__ phase0, const uint8_t* __restrict__ bad, int nx,
+                           int ny, int nz, double zr, double zrh, int nxh, int nyh, int nzh, int pass,
+                           int* __restrict__ bbox, uint8_t* __restrict__ seed, int ox, int oy, int oz, int sx, int sy) {
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const float fz0 = (float)(((double)z * zr) / zrh);
+    WR_FOR_COLS(nx, x) {
+      const size_t i = (size_t)row * nx + x;
+      if (!bad[i]) continue;
+      const float3 p = wr_phase<MODE>(f, phase0, x, y, z, fz0, i);
+      const int qx = (int)rintf(p.x), qy = (int)rintf(p.y), qz = (int)rintf(p.z);
+      if (qx < 0 || qx >= nxh || qy < 0 || qy >= nyh || qz < 0 || qz >= nzh) continue;
+      if (pass == 0) {
+        atomicMin(bbox, qx); atomicMax(bbox + 1, qx);
+        atomicMin(bbox + 2, qy); atomicMax(bbox + 3, qy);
+        atomicMin(bbox + 4, qz); atomicMax(bbox + 5, qz);
+      } else {
+        seed[((size_t)(qz - oz) * sy + (qy - oy)) * sx + (qx - ox)] = 1;
+      }
+    }
+  }
+}
+
+// Binary dilation (OR) or erosion (AND) of a (sz, sy, sx) uint8 volume with a
+// symmetric structuring element given as offsets (x, y, z); outside the
+// volume counts as 0 (scipy's border_value 0).  keep (may be null): the
+// output is ANDed with it; changed (may be null) is set when out != prev.
+__global__ void k_wr_morph(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int sx, int sy, int sz,
+                           const int3* __restrict__ off, int noff, int dilate, const uint8_t* __restrict__ keep,
+                           int* __restrict__ changed) {
+  const long long n = (long long)sx * sy * sz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % sx);
+    const long long rest = i / sx;
+    const int y = (int)(rest % sy), z = (int)(rest / sy);
+    bool v = !dilate;
+    for (int k = 0; k < noff; ++k) {
+      const int3 o = off[k];
+      const int qx = x + o.x, qy = y + o.y, qz = z + o.z;
+      const bool inside = qx >= 0 && qx < sx && qy >= 0 && qy < sy && qz >= 0 && qz < sz;
+      const bool b = inside && in[((size_t)qz * sy + qy) * sx + qx];
+      if (dilate && b) { v = true; break; }
+      if (!dilate && !b) { v = false; break; }
+    }
+    if (keep && !keep[i]) v = false;
+    const uint8_t o8 = v ? 1 : 0;
+    if (changed && o8 != in[i]) atomicOr(changed, 1);
+    out[i] = o8;
+  }
+}
+
+// One pass of a separable Gaussian (weights w[0..2 rad]) along axis 0 (x),
+// 1 (y) or 2 (z) of a float32 ROI with mode "reflect" (half-sample
+// symmetric), float64 sum, float32 result (scipy.ndimage.correlate1d).
+__global__ void k_wr_gauss(const float* __restrict__ in, float* __restrict__ out, int sx, int sy, int sz,
+                           const double* __restrict__ wts, int rad, int axis) {
+  const long long n = (long long)sx * sy * sz;
+  const int len = axis == 0 ? sx : axis == 1 ? sy : sz;
+  const long long step = axis == 0 ? 1 : axis == 1 ? sx : (long long)sx * sy;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % sx);
+    const long long rest = i / sx;
+    const int y = (int)(rest % sy), z = (int)(rest / sy);
+    const int c = axis == 0 ? x : axis == 1 ? y : z;
+    const long long base = i - (long long)c * step;
+    double s = 0.0;
+    for (int k = -rad; k <= rad; ++k) {
+      int q = c + k;
+      // reflect about the edges, repeating for offsets longer than the line
+      const int period = 2 * len;
+      q %= period;
+      if (q < 0) q += period;
+      if (q >= len) q = period - 1 - q;
+      s += wts[k + rad] * (double)in[base + (long long)q * step];
+    }
+    out[i] = (float)s;
+  }
+}
+
+// the ROI (x0, y0, z0) + (sx, sy, sz) of a (., ny, nx) float level, contiguous
+__global__ void k_copy_roi(const float* __restrict__ lev, float* __restrict__ out, int nx, int ny, int x0, int y0,
+                           int z0, int sx, int sy, int sz) {
+  const long long n = (long long)sx * sy * sz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % sx);
+    const long long rest = i / sx;
+    const int y = (int)(rest % sy), z = (int)(rest / sy);
+    out[i] = lev[((size_t)(z + z0) * ny + (y + y0)) * nx + (x + x0)];
+  }
+}
+
+// the ROI's values under the seed mask, packed (order irrelevant: they are sorted)
+__global__ void k_wr_gather(const float* __restrict__ v, const uint8_t* __restrict__ m, long long n,
+                            float* __restrict__ out, int* __restrict__ count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (m[i]) out[atomicAdd(count, 1)] = v[i];
+}
+
+// |v - med| in float32 (a float32 array minus a Python float)
+__global__ void k_wr_absdev(const float* __restrict__ v, int n, float med, float* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = fabsf(v[i] - med);
+}
+
+// allowed = (near & |sm - med| <= tol) | seed, all float32 comparisons
+__global__ void k_wr_allowed(const float* __restrict__ sm, const uint8_t* __restrict__ near,
+                             const uint8_t* __restrict__ seed, long long n, float med, float tol,
+                             uint8_t* __restrict__ allowed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    allowed[i] = ((near[i] && fabsf(sm[i] - med) <= tol) || seed[i]) ? 1 : 0;
+}
+
+// corrected = level mask | region pasted at the ROI origin
+__global__ void k_wr_paste(const uint8_t* __restrict__ region, uint8_t* __restrict__ mask, int nxh, int nyh,
+                           int ox, int oy, int oz, int sx, int sy, int sz) {
+  const long long n = (long long)sx * sy * sz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (!region[i]) continue;
+    const int x = (int)(i % sx);
+    const long long rest = i / sx;
+    const int y = (int)(rest % sy), z = (int)(rest / sy);
+    mask[((size_t)(z + oz) * nyh + (y + oy)) * nxh + (x + ox)] = 1;
+  }
+}
+
+// valid voxels under a reference mask spline: !moving-excluded and
+// H_mask(phase) <= 0.5 (compute_valid_mask_on_moving_grid, :2006-2028)
+template <int MODE>
+__global__ void k_wr_count_valid(const FieldSrc f, const float4* __restrict__ phase0, const uint8_t* __restrict__ mbits,
+                                 const double* __restrict__ cmask, int pxh, int pyh, int pzh, int nx, int ny, int nz,
+                                 double zr, double zrh, unsigned long long* __restrict__ count) {
+  unsigned long long c = 0;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const float fz0 = (float)(((double)z * zr) / zrh);
+    WR_FOR_COLS(nx, x) {
+      const size_t i = (size_t)row * nx + x;
+      if (mbits && (mbits[i] & 1)) continue;
+      const float3 p = wr_phase<MODE>(f, phase0, x, y, z, fz0, i);
+      if (!((float)spline_sample<double, double>(cmask, pxh, pyh, pzh, p.x, p.y, p.z) > 0.5f)) ++c;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+__global__ void k_wr_count_u8(const uint8_t* __restrict__ v, long long n, int want, unsigned long long* __restrict__ count) {
+  unsigned long long c = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    c += ((v[i] != 0) == (want != 0)) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+// Error of a finished pass (the final recompute, :2211-2216): mean of the
+// residual squared (errpart: per-tile sums of the eval launch) plus the
+// smoothness penalty of the CP neighbour differences without z scaling.
+__global__ void k_wr_pass_error(const double* __restrict__ errpart, long long nblk, const float4* __restrict__ cp,
+                                int ncx, int ncy, int nz, double sps, double n_vox, double* __restrict__ out) {
+  __shared__ double red[2][256];
+  double e = 0.0, pen = 0.0;
+  for (long long i = threadIdx.x; i < nblk; i += blockDim.x) e += errpart[i];
+  const long long ncp = (long long)ncx * ncy * nz;
+  for (long long i = threadIdx.x; i < ncp; i += blockDim.x) {
+    const int cx = (int)(i % ncx);
+    const long long rest = i / ncx;
+    const int cy = (int)(rest % ncy), z = (int)(rest / ncy);
+    const float4* b = cp + (size_t)z * ncy * ncx;
+    double sx = 0.0, sy = 0.0, szz = 0.0;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (dx == 0 && dy == 0) continue;
+        const float4 v = b[clampi(cy + dy, 0, ncy - 1) * ncx + clampi(cx + dx, 0, ncx - 1)];
+        sx += 0.125 * (double)v.x;
+        sy += 0.125 * (double)v.y;
+        szz += 0.125 * (double)v.z;
+      }
+    const float4 c = b[cy * ncx + cx];
+    const float ndx = (float)(sx - (double)c.x), ndy = (float)(sy - (double)c.y), ndz = (float)(szz - (double)c.z);
+    pen += (double)(ndx * ndx + ndy * ndy + ndz * ndz);
+  }
+  red[0][threadIdx.x] = e;
+  red[1][threadIdx.x] = pen;
+  __syncthreads();
+  for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+    if (threadIdx.x < s2) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s2];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s2];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0][0] / n_vox + red[1][0] * sps / n_vox;
+}
+
+__global__ void k_wr_set_active(LKState* st) { st->active = 1; }
+
+// a re-run of a level: fresh stopping state, the level's log kept
+__global__ void k_wr_pass_begin(LKState* st, int level) {
+  st->active = 1;
+  st->do_update = 0;
+  st->level = level;
+  st->n_updates = 0;
+  st->maxdiff_bits = 0u;
+  st->old_err[0] = st->old_err[1] = st->old_err[2] = INFINITY;
+}
+
+}  // namespace wr

@@ -86,7 +86,8 @@ def stats_to_log(st: _lib.WrLKStats, layers: int) -> tuple[dict, float]:
     """error_log dict in the reference's shape (utils/calFlow3d_Wei_v1.py:329-335)."""
     log = {}
     for layer in range(layers - 1, -1, -1):
-        e, u = st.evals[layer], st.updates[layer]
+        # the device keeps at most WR_MAX_ITERS entries per level
+        e, u = min(st.evals[layer], _lib.MAX_ITERS), min(st.updates[layer], _lib.MAX_ITERS)
         diff = [st.diff_error[layer][i] for i in range(e)]
         pen = [st.penalty_error[layer][i] for i in range(e)]
         log[f"layer_{layer}"] = {
