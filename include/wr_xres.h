@@ -40,6 +40,10 @@ typedef struct WrXresWrongRegion {
   float expand_radius_xy;      /* ["expand_radius_xy"], 2.0 (divided by 2^layer) */
   float sigma_grad;            /* ["sigma_grad"], 1.0 */
   float intensity_k;           /* ["intensity_k"], 2.0 */
+  int32_t exclude_mode;        /* ["wrong_region_exclude_mode"]: 0 "direct", 1 "highresidual" (only the bad
+                                  voxels whose 3x3-smoothed error drop over the pass reaches the quantile below
+                                  seed the trap, :2340-2355) */
+  float quantile_q;            /* ["quantile_threshold_q"], 0.8 */
 } WrXresWrongRegion;
 
 /*

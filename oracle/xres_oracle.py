@@ -155,9 +155,12 @@ def _optimize_layer(mov_l, ref_l, mask_mov_l, mask_ref_f, phase_cur, motion, r, 
         res[~valid] = 0
         return phase, sampled, valid, res
 
+    error_init = None
     for it_idx in range(n_iter):
         old_motion = motion.copy()
         phase_new, ref_sampled, valid, res = evaluate(motion)
+        if it_idx == 0:
+            error_init = res ** 2
         cpm = motion[xg][:, yg]
         nei = get_nei_diff(cpm)
         nei[..., 2] *= zratio_hr
@@ -211,8 +214,10 @@ def _optimize_layer(mov_l, ref_l, mask_mov_l, mask_ref_f, phase_cur, motion, r, 
     phase_new, ref_sampled, valid, res = evaluate(motion)
     nei = get_nei_diff(motion[xg][:, yg])
     diff_e, pen_e = cal_error(res, nei, sps)
+    error_last = res ** 2
     return {"motion": motion, "phase_new": phase_new, "data_ref_sampled": ref_sampled, "residual": res,
-            "valid_mask": valid, "current_error": diff_e + pen_e}
+            "valid_mask": valid, "current_error": diff_e + pen_e,
+            "error_init": error_init if error_init is not None else error_last.copy(), "error_last": error_last}
 
 
 # ----------------------------------------------------------------------------
@@ -284,6 +289,27 @@ def bad_region_mask(err_cp, r, xg, yg, x_size, y_size, mad_threshold=3.0, min_co
         z0, z1 = int(where[:, 2].min()), int(where[:, 2].max())
         bad[x0:x1 + 1, y0:y1 + 1, z0:z1 + 1] = True
     return bad, kept
+
+
+def quantile_threshold(arr, q):
+    """get_quantile_threshold (:1790-1799): the element of rank
+    floor((n - 1) q) of the flattened values (0 for none)."""
+    flat = np.asarray(arr).ravel()
+    if flat.size == 0:
+        return 0.0
+    k = int(np.clip(np.floor((flat.size - 1) * q), 0, flat.size - 1))
+    return np.partition(flat, k)[k]
+
+
+def high_residual_refine(bad, error_init, error_last, q):
+    """The "highresidual" exclusion mode (:2340-2355): inside the bad boxes,
+    keep only the voxels whose 3x3-smoothed error drop (first iteration minus
+    final) reaches the q quantile of the drops in the boxes."""
+    box3 = np.ones((3, 3, 1), dtype=np.float32) / 9
+    dense = ndimage.correlate(error_init - error_last, box3, mode="nearest")
+    dense[~bad] = 0
+    th = quantile_threshold(dense[bad], q) if bad.any() else 0
+    return bad & (dense >= th)
 
 
 def trap_mask(bad_mask, phase_new, ref_l, z_ratio_ref, expand_radius_xy=2.0, sigma_grad=1.0, intensity_k=2.5):
@@ -367,8 +393,11 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
     expand = float(option.get("expand_radius_xy", 2.0))
     sigma_grad = float(option.get("sigma_grad", 1.0))
     intensity_k = float(option.get("intensity_k", 2.0))
-    if wr_enable and (replay_updates is not None or wr_mode != "direct"):
-        raise NotImplementedError("oracle: wrong-region correction supports the 'direct' mode without replay")
+    quantile_q = float(option.get("quantile_threshold_q", 0.8))
+    if wr_enable and replay_updates is not None:
+        raise NotImplementedError("oracle: the wrong-region correction runs without replay")
+    if wr_enable and wr_mode not in ("direct", "highresidual"):
+        raise ValueError(f"unknown wrong_region_exclude_mode {wr_mode!r}")
     dat_mov = np.asarray(dat_mov, dtype=np.float32)
     dat_ref = np.asarray(dat_ref, dtype=np.float32)
     sz, sz_hr = dat_mov.shape, dat_ref.shape
@@ -431,6 +460,8 @@ def get_motion_v2(dat_mov, dat_ref, option, replay_updates=None, window_noise=No
             decision = {"regions": nreg}
             lg["wrong_region"] = decision
             if nreg > 0:
+                if wr_mode == "highresidual":
+                    bad = high_residual_refine(bad, res0["error_init"], res0["error_last"], quantile_q)
                 bad = bad & res0["valid_mask"]
                 trap = trap_mask(bad, res0["phase_new"], ref_l, zratio_hr, expand / (2.0 ** layer), sigma_grad,
                                  intensity_k)

@@ -94,6 +94,23 @@ def xres_wr_case_names():
     return sorted(os.path.basename(f)[len("xreswr_"):-4] for f in glob.glob(os.path.join(GOLDEN, "xreswr_*.npz")))
 
 
+def xres_hr_case_names():
+    import glob
+
+    return sorted(os.path.basename(f)[len("xreshr_"):-4] for f in glob.glob(os.path.join(GOLDEN, "xreshr_*.npz")))
+
+
+def load_xres_hr_case(name):
+    """(arrays, option) for a getMotion_v2 case with the wrong-region
+    correction in its "highresidual" exclusion mode."""
+    arrays, option = load_xres_case(name)
+    out = dict(np.load(os.path.join(GOLDEN, f"xreshr_{name}.npz")))
+    option.update({"wrong_region_enable": True, "wrong_region_exclude_mode": "highresidual",
+                   "quantile_threshold_q": float(out.pop("quantile_q"))})
+    arrays.update(out)
+    return arrays, option
+
+
 def load_xres_wr_case(name):
     """(arrays, option) for a getMotion_v2 case with the wrong-region correction
     on: the inputs of the xres case, the outputs of the reference's run with

@@ -271,6 +271,11 @@ XRES_WR_CASES = ("xr_mask_r2_l1", "xr_small_r3_l1", "xr_init_r4_l2", "xr_ragged_
                  "xr_z1_r3_l1", "xr_phase_r3_l1")
 
 
+# cases re-run with wrong_region_exclude_mode="highresidual" (the trap seeded
+# only by the bad voxels whose error dropped most); q 0.8 is the default
+XRES_HR_CASES = {"xr_mask_r2_l1": 0.8, "xr_small_r3_l1": 0.8, "xr_ragged_r3_l2": 0.5, "xr_phase_r3_l1": 0.8}
+
+
 def xres_pair(mov_shape, ref_shape, zr, zr_hr, seed):
     """Moving and reference stacks of one blob field sampled at z spacings zr
     and zr_hr (physical units per z index), the moving one displaced by a
@@ -363,18 +368,45 @@ def make_xres_cases(root, out_dir):
         np.savez_compressed(os.path.join(out_dir, f"xreswr_{name}.npz"), phase=np.asarray(phase, np.float32),
                             motion=np.asarray(motion, np.float32), ref_sampled=np.asarray(sampled, np.float64))
         print(f"{name} (wrong-region correction on): max |motion| {float(np.abs(motion).max()):.3f}")
+    make_xres_hr_cases(cf, out_dir)
+
+
+def make_xres_hr_cases(cf, out_dir):
+    """xres cases re-run with the "highresidual" exclusion mode."""
+    with open(os.path.join(out_dir, "xres_cases.json")) as fh:
+        index = json.load(fh)
+    for name, q in XRES_HR_CASES.items():
+        d = dict(np.load(os.path.join(out_dir, f"xres_{name}.npz")))
+        option = dict(index[name])
+        option.update({"mask_ref": d["mask_ref"].copy(), "mask_mov": d["mask_mov"].copy(),
+                       "motion": d.get("motion_init"), "wrong_region_enable": True,
+                       "wrong_region_exclude_mode": "highresidual", "quantile_threshold_q": q})
+        if "phase_init" in d:
+            option["phase"] = d["phase_init"]
+        phase, motion, sampled = cf.getMotion_v2(d["mov"].copy(), d["ref"].copy(), option)
+        np.savez_compressed(os.path.join(out_dir, f"xreshr_{name}.npz"), phase=np.asarray(phase, np.float32),
+                            motion=np.asarray(motion, np.float32), ref_sampled=np.asarray(sampled, np.float64),
+                            quantile_q=np.float64(q))
+        print(f"{name} (highresidual exclusion, q {q}): max |motion| {float(np.abs(motion).max()):.3f}")
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres"], default=None)
+    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr"], default=None)
     args = ap.parse_args()
     if args.only in (None, "masks"):
         make_mask_cases(args.ref, HERE)
     if args.only in (None, "xres"):
         make_xres_cases(args.ref, HERE)
-    if args.only in ("masks", "xres"):
+    if args.only == "xreshr":
+        src = os.path.join(args.ref, "src", "wholistic_registration")
+        if "wholistic_registration" not in sys.modules:
+            pkg = types.ModuleType("wholistic_registration")
+            pkg.__path__ = [src]
+            sys.modules["wholistic_registration"] = pkg
+        make_xres_hr_cases(importlib.import_module("wholistic_registration.utils.calFlowCrossResolution"), HERE)
+    if args.only in ("masks", "xres", "xreshr"):
         return
     ref = load_reference(args.ref)
     if args.only in (None, "primitives"):

@@ -28,7 +28,8 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import load_xres_case, load_xres_wr_case, xres_case_names, xres_wr_case_names
+from conftest import (load_xres_case, load_xres_hr_case, load_xres_wr_case, xres_case_names, xres_hr_case_names,
+                      xres_wr_case_names)
 
 pytestmark = pytest.mark.gpu
 
@@ -116,8 +117,8 @@ def test_xres_rejects_unbuilt_options():
     arrays, option = load_xres_case("xr_small_r3_l1")
     opt = dict(option)
     opt["wrong_region_enable"] = True
-    opt["wrong_region_exclude_mode"] = "highresidual"
-    with pytest.raises(NotImplementedError):
+    opt["wrong_region_exclude_mode"] = "lowresidual"
+    with pytest.raises(ValueError):
         C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
     opt["wrong_region_exclude_mode"] = "direct"
     opt["wrong_region_metric"] = "l2"
@@ -125,18 +126,20 @@ def test_xres_rejects_unbuilt_options():
         C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
 
 
-@pytest.mark.parametrize("name", xres_wr_case_names())
-def test_xres_wrong_region_matches_reference_run(name):
+@pytest.mark.parametrize("kind,name", [("direct", n) for n in xres_wr_case_names()] +
+                         [("highresidual", n) for n in xres_hr_case_names()])
+def test_xres_wrong_region_matches_reference_run(kind, name):
     """getMotion_v2 with the wrong-region correction (the reference's
     default): the same bound as without it, the spread measured by the oracle
     running the correction under the same perturbations (a perturbation that
     flips a control point's outlier status or the keep / discard choice shows
     up there as spread).  The device log must hold the updates of every pass
-    the oracle ran (one pass, or three when a trap was built)."""
+    the oracle ran (one pass, or three when a trap was built).  Both exclusion
+    modes: "direct" (the default) and "highresidual"."""
     from oracle import xres_oracle as X
     from wholistic_registration_b200 import calFlowCrossResolution as C
 
-    arrays, option = load_xres_wr_case(name)
+    arrays, option = (load_xres_wr_case if kind == "direct" else load_xres_hr_case)(name)
     phase, motion, sampled = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(option))
     _, _, _, log = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option))
     dev_log, _ = C.last_registrar.error_log()

@@ -88,6 +88,8 @@ class WrXresWrongRegion(ctypes.Structure):
         ("expand_radius_xy", ctypes.c_float),
         ("sigma_grad", ctypes.c_float),
         ("intensity_k", ctypes.c_float),
+        ("exclude_mode", ctypes.c_int32),
+        ("quantile_q", ctypes.c_float),
     ]
 
 

@@ -26,9 +26,8 @@ tensors where the reference returns CuPy arrays.
 
 The wrong-region correction the reference runs by default
 (``wrong_region_enable=True``: bad-region detection on the CP errors, a trap
-mask in reference space and two re-runs, :2240-2467) runs on the device too;
-its ``wrong_region_exclude_mode="highresidual"`` variant is not built and
-raises ``NotImplementedError`` instead of silently computing something else.  One optional key extends the options:
+mask in reference space and two re-runs, :2240-2467) runs on the device too,
+in both exclusion modes ("direct" and "highresidual").  One optional key extends the options:
 ``forced_updates`` (layer -> number of motion updates, replaying another
 run's iteration counts).
 """
@@ -181,14 +180,16 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
         metric = str(option.get("wrong_region_metric", "mse")).lower()
         if metric not in ("mse", "mae"):
             raise ValueError("metric must be 'mse' or 'mae'")
-        if option.get("wrong_region_exclude_mode", "direct") != "direct":
-            raise NotImplementedError("wrong_region_exclude_mode 'highresidual' is not built on this path; "
-                                      "the default 'direct' is")
+        modes = {"direct": 0, "highresidual": 1}
+        mode = option.get("wrong_region_exclude_mode", "direct")
+        if mode not in modes:
+            raise ValueError(f"wrong_region_exclude_mode must be 'direct' or 'highresidual', not {mode!r}")
         wr = _lib.WrXresWrongRegion(1, 0 if metric == "mse" else 1,
                                     float(option.get("wrong_region_mad_threshold", 3.0)),
                                     int(option.get("wrong_region_min_component_size", 2)),
                                     float(option.get("expand_radius_xy", 2.0)), float(option.get("sigma_grad", 1.0)),
-                                    float(option.get("intensity_k", 2.0)))
+                                    float(option.get("intensity_k", 2.0)), modes[mode],
+                                    float(option.get("quantile_threshold_q", 0.8)))
     as_torch = isinstance(data_mov, torch.Tensor)
     device = data_mov.device if as_torch and data_mov.is_cuda else torch.device("cuda", torch.cuda.current_device())
     mov = _to_device(data_mov, device, torch.float32)

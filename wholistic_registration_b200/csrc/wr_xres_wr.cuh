@@ -177,7 +177,8 @@ __global__ void k_wr_bad_regions(const double* __restrict__ err, int ncx, int nc
   }
 }
 
-// bad = inside one of the boxes of the voxel's slice, and valid
+// bad = inside one of the boxes of the voxel's slice, and valid (ex null:
+// the boxes alone)
 __global__ void k_wr_bad_mask(const WrBox* __restrict__ boxes, const int* __restrict__ nbox, const uint8_t* __restrict__ ex,
                               uint8_t* __restrict__ bad, int nx, int ny, int nz, int max_boxes) {
   const int nb = min(*nbox, max_boxes);
@@ -190,9 +191,50 @@ __global__ void k_wr_bad_mask(const WrBox* __restrict__ boxes, const int* __rest
         in = b.z == z && x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1;
       }
       const size_t i = (size_t)row * nx + x;
-      bad[i] = (in && !ex[i]) ? 1 : 0;
+      bad[i] = (in && !(ex && ex[i])) ? 1 : 0;
     }
   }
+}
+
+// "highresidual" exclusion (:2340-2355): dense = 3x3 box (edge-replicated,
+// in-plane) of the error drop res0^2 - res1^2 over the pass (first iteration's
+// residual minus the final one), 0 outside the bad boxes; float64.
+__global__ void k_wr_error_drop(const float* __restrict__ res0, const float* __restrict__ res1,
+                                const uint8_t* __restrict__ bad, double* __restrict__ dense, int nx, int ny, int nz) {
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    WR_FOR_COLS(nx, x) {
+      const size_t i = (size_t)row * nx + x;
+      if (!bad[i]) {
+        dense[i] = 0.0;
+        continue;
+      }
+      double s = 0.0;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const size_t o = ((size_t)z * ny + clampi(y + dy, 0, ny - 1)) * nx;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const size_t j = o + clampi(x + dx, 0, nx - 1);
+          const double a = res0[j], b = res1[j];
+          s += a * a - b * b;
+        }
+      }
+      dense[i] = s * (double)(1.f / 9.f);
+    }
+  }
+}
+
+// the error drops inside the bad boxes, packed (they are sorted next)
+__global__ void k_wr_gather_drop(const double* __restrict__ dense, const uint8_t* __restrict__ bad, long long n,
+                                 double* __restrict__ out, int* __restrict__ count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (bad[i]) out[atomicAdd(count, 1)] = dense[i];
+}
+
+// bad &= dense >= th, and valid
+__global__ void k_wr_keep_high(uint8_t* __restrict__ bad, const double* __restrict__ dense, double th,
+                               const uint8_t* __restrict__ ex, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    bad[i] = (bad[i] && dense[i] >= th && !ex[i]) ? 1 : 0;
 }
 
 // phase of a finished pass at a voxel of the iteration grid
