@@ -331,6 +331,8 @@ def run_ours(args, wl, rank, world, local_rank):
         res["config"]["batched_small_frames"] = run_batched_small(device)
     if not args.no_xres:
         res["config"]["cross_resolution"] = run_cross_resolution(device, args.xres_shape)
+        res["config"]["cross_resolution_wrong_region"] = run_cross_resolution(device, args.xres_shape,
+                                                                              wrong_region=True)
 
     # learned warm start + float16 levels (the headline path) on the same frames
     ws = None
@@ -433,15 +435,17 @@ def run_batched_small(device, n=16, reps=3):
     return out
 
 
-def run_cross_resolution(device, shape="32x1024x1024:128", reps=4):
-    """getMotion_v2 (wrong-region correction off): by default a
-    32x1024x1024 moving stack (z spacing 4) onto a 128x1024x1024 reference
-    (z spacing 1), layer 3, r 16, iter 10, its own stopping rules; the moving
-    stack is every (nzh / nz)-th reference slice shifted by one voxel in x and y."""
+def run_cross_resolution(device, shape="32x1024x1024:128", reps=4, wrong_region=False):
+    """getMotion_v2: by default a 32x1024x1024 moving stack (z spacing 4)
+    onto a 128x1024x1024 reference (z spacing 1), layer 3, r 16, iter 10, its
+    own stopping rules; the moving stack is every (nzh / nz)-th reference
+    slice shifted by one voxel in x and y.  wrong_region: with the
+    wrong-region correction at the reference's default options."""
     import torch
 
     from wholistic_registration_b200 import synthetic
     from wholistic_registration_b200.calFlowCrossResolution import XresRegistrar
+    from wholistic_registration_b200 import _lib
     from wholistic_registration_b200.registrar import LKParams
 
     zyx, nzh = shape.split(":")
@@ -455,7 +459,8 @@ def run_cross_resolution(device, shape="32x1024x1024:128", reps=4):
     mov = torch.roll(ref[::nzh // nz], shifts=(1, -1), dims=(1, 2)).contiguous()
     excl = torch.zeros((nz, ny, nx), dtype=torch.uint8, device=device)
     p = LKParams(layer=3, iter=10, r=16, zRatio=float(nzh // nz), movRange=5.0, smoothPenalty=0.05, tol=1e-3)
-    reg = XresRegistrar((nz, ny, nx), (nzh, ny, nx), p, 1.0, has_mask_ref=False, device=device)
+    wr = _lib.WrXresWrongRegion(1, 0, 3.0, 2, 2.0, 1.0, 2.0, 0, 0.8) if wrong_region else None
+    reg = XresRegistrar((nz, ny, nx), (nzh, ny, nx), p, 1.0, has_mask_ref=False, device=device, wrong_region=wr)
     reg.register(mov, ref, mask_mov=excl)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -469,6 +474,7 @@ def run_cross_resolution(device, shape="32x1024x1024:128", reps=4):
     return {"shape_mov_zyx": [nz, ny, nx], "shape_ref_zyx": [nzh, ny, nx], "zRatio": float(nzh // nz), "zRatio_HR": 1.0,
             "layer": 3, "r": 16, "iter": 10, "ms_per_volume": round(ms, 3), "volumes_per_s": round(1e3 / ms, 3),
             "updates_per_level": {k: len(v["max_diff_motion"]) for k, v in log.items()},
+            "wrong_region_correction": "on (reference defaults, direct mode)" if wrong_region else "off",
             "api": "XresRegistrar.register (device-resident stacks)"}
 
 

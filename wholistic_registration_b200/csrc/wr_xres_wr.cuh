@@ -178,21 +178,15 @@ __global__ void k_wr_bad_regions(const double* __restrict__ err, int ncx, int nc
 }
 
 // bad = inside one of the boxes of the voxel's slice, and valid (ex null:
-// the boxes alone)
-__global__ void k_wr_bad_mask(const WrBox* __restrict__ boxes, const int* __restrict__ nbox, const uint8_t* __restrict__ ex,
-                              uint8_t* __restrict__ bad, int nx, int ny, int nz, int max_boxes) {
-  const int nb = min(*nbox, max_boxes);
-  WR_FOR_ROWS(nz * ny, row) {
-    const int z = row / ny, y = row - z * ny;
-    WR_FOR_COLS(nx, x) {
-      bool in = false;
-      for (int k = 0; k < nb && !in; ++k) {
-        const WrBox b = boxes[k];
-        in = b.z == z && x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1;
-      }
-      const size_t i = (size_t)row * nx + x;
-      bad[i] = (in && !(ex && ex[i])) ? 1 : 0;
-    }
+// the boxes alone); one CTA per box paints its rectangle into a zeroed mask.
+__global__ void k_wr_paint_boxes(const WrBox* __restrict__ boxes, const uint8_t* __restrict__ ex,
+                                 uint8_t* __restrict__ bad, int nx, int ny) {
+  const WrBox b = boxes[blockIdx.x];
+  const int w = b.x1 - b.x0 + 1, h = b.y1 - b.y0 + 1;
+  for (int k = threadIdx.x; k < w * h; k += blockDim.x) {
+    const int y = b.y0 + k / w, x = b.x0 + k % w;
+    const size_t i = ((size_t)b.z * ny + y) * nx + x;
+    bad[i] = (ex && ex[i]) ? 0 : 1;
   }
 }
 
@@ -276,59 +270,91 @@ __global__ void k_wr_seeds(const FieldSrc f, const float4* __restrict__ phase0, 
   }
 }
 
-// Binary dilation (OR) or erosion (AND) of a (sz, sy, sx) uint8 volume with a
-// symmetric structuring element given as offsets (x, y, z); outside the
-// volume counts as 0 (scipy's border_value 0).  keep (may be null): the
-// output is ANDed with it; changed (may be null) is set when out != prev.
-__global__ void k_wr_morph(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int sx, int sy, int sz,
-                           const int3* __restrict__ off, int noff, int dilate, const uint8_t* __restrict__ keep,
-                           int* __restrict__ changed) {
-  const long long n = (long long)sx * sy * sz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % sx);
-    const long long rest = i / sx;
-    const int y = (int)(rest % sy), z = (int)(rest / sy);
-    bool v = !dilate;
-    for (int k = 0; k < noff; ++k) {
-      const int3 o = off[k];
-      const int qx = x + o.x, qy = y + o.y, qz = z + o.z;
-      const bool inside = qx >= 0 && qx < sx && qy >= 0 && qy < sy && qz >= 0 && qz < sz;
-      const bool b = inside && in[((size_t)qz * sy + qy) * sx + qx];
-      if (dilate && b) { v = true; break; }
-      if (!dilate && !b) { v = false; break; }
+// Binary morphology on a (sz, sy, sx) uint8 ROI with a symmetric structuring
+// element given as offsets (x, y, z); outside the ROI counts as 0 (scipy's
+// border_value 0).  Rows (y, z) by blocks, x by threads: no 64-bit division.
+//
+// Dilation by scatter: every set voxel writes 1 at its offsets into a zeroed
+// out (the work is set voxels x offsets; the sets here are sparse seeds and
+// regions grown from them).
+__global__ void k_wr_dilate_scatter(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int sx, int sy, int sz,
+                                    const int3* __restrict__ off, int noff) {
+  WR_FOR_ROWS(sz * sy, row) {
+    const int z = row / sy, y = row - z * sy;
+    WR_FOR_COLS(sx, x) {
+      if (!in[(size_t)row * sx + x]) continue;
+      for (int k = 0; k < noff; ++k) {
+        const int3 o = off[k];
+        const int qx = x + o.x, qy = y + o.y, qz = z + o.z;
+        if (qx >= 0 && qx < sx && qy >= 0 && qy < sy && qz >= 0 && qz < sz) out[((size_t)qz * sy + qy) * sx + qx] = 1;
+      }
     }
-    if (keep && !keep[i]) v = false;
-    const uint8_t o8 = v ? 1 : 0;
-    if (changed && o8 != in[i]) atomicOr(changed, 1);
-    out[i] = o8;
   }
 }
 
+// Erosion: a voxel stays set when every offset lands on a set voxel inside
+// the ROI; the element holds (0, 0, 0), so unset voxels stay unset.
+__global__ void k_wr_erode(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int sx, int sy, int sz,
+                           const int3* __restrict__ off, int noff) {
+  WR_FOR_ROWS(sz * sy, row) {
+    const int z = row / sy, y = row - z * sy;
+    WR_FOR_COLS(sx, x) {
+      const size_t i = (size_t)row * sx + x;
+      bool v = in[i] != 0;
+      for (int k = 0; k < noff && v; ++k) {
+        const int3 o = off[k];
+        const int qx = x + o.x, qy = y + o.y, qz = z + o.z;
+        v = qx >= 0 && qx < sx && qy >= 0 && qy < sy && qz >= 0 && qz < sz && in[((size_t)qz * sy + qy) * sx + qx];
+      }
+      out[i] = v ? 1 : 0;
+    }
+  }
+}
+
+// out &= keep; *changed set when out differs from prev (one growth step)
+__global__ void k_wr_keep(uint8_t* __restrict__ out, const uint8_t* __restrict__ keep, const uint8_t* __restrict__ prev,
+                          long long n, int* __restrict__ changed) {
+  int c = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const uint8_t v = (out[i] && keep[i]) ? 1 : 0;
+    out[i] = v;
+    c |= v != prev[i];
+  }
+  if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(changed, 1);
+}
+
+// scipy's "reflect" (half-sample symmetric) index of q on a line of len,
+// repeating for offsets longer than the line
+__device__ __forceinline__ int reflect_index(int q, int len) {
+  if (q >= 0 && q < len) return q;
+  const int period = 2 * len;
+  q %= period;
+  if (q < 0) q += period;
+  return q >= len ? period - 1 - q : q;
+}
+
 // One pass of a separable Gaussian (weights w[0..2 rad]) along axis 0 (x),
-// 1 (y) or 2 (z) of a float32 ROI with mode "reflect" (half-sample
-// symmetric), float64 sum, float32 result (scipy.ndimage.correlate1d).
+// 1 (y) or 2 (z) of a float32 ROI with mode "reflect", float64 sum, float32
+// result (scipy.ndimage.correlate1d).  Rows (y, z) by blocks, x by threads.
 __global__ void k_wr_gauss(const float* __restrict__ in, float* __restrict__ out, int sx, int sy, int sz,
                            const double* __restrict__ wts, int rad, int axis) {
-  const long long n = (long long)sx * sy * sz;
-  const int len = axis == 0 ? sx : axis == 1 ? sy : sz;
-  const long long step = axis == 0 ? 1 : axis == 1 ? sx : (long long)sx * sy;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % sx);
-    const long long rest = i / sx;
-    const int y = (int)(rest % sy), z = (int)(rest / sy);
-    const int c = axis == 0 ? x : axis == 1 ? y : z;
-    const long long base = i - (long long)c * step;
-    double s = 0.0;
-    for (int k = -rad; k <= rad; ++k) {
-      int q = c + k;
-      // reflect about the edges, repeating for offsets longer than the line
-      const int period = 2 * len;
-      q %= period;
-      if (q < 0) q += period;
-      if (q >= len) q = period - 1 - q;
-      s += wts[k + rad] * (double)in[base + (long long)q * step];
+  WR_FOR_ROWS(sz * sy, row) {
+    const int z = row / sy, y = row - z * sy;
+    WR_FOR_COLS(sx, x) {
+      double s = 0.0;
+      if (axis == 0) {
+        const float* line = in + (size_t)row * sx;
+        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)line[reflect_index(x + k, sx)];
+      } else if (axis == 1) {
+        const float* col = in + (size_t)z * sy * sx + x;
+        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)col[(size_t)reflect_index(y + k, sy) * sx];
+      } else {
+        const float* col = in + (size_t)y * sx + x;
+        const size_t plane = (size_t)sx * sy;
+        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)col[(size_t)reflect_index(z + k, sz) * plane];
+      }
+      out[(size_t)row * sx + x] = (float)s;
     }
-    out[i] = (float)s;
   }
 }
 
