@@ -311,11 +311,22 @@ __global__ void k_wr_erode(const uint8_t* __restrict__ in, uint8_t* __restrict__
   }
 }
 
-// out &= keep; *changed set when out differs from prev (one growth step)
+// out &= keep; *changed set when out differs from prev (one growth step).
+// 16 bytes per thread (the ROI buffers start 256-byte aligned), tail by bytes.
 __global__ void k_wr_keep(uint8_t* __restrict__ out, const uint8_t* __restrict__ keep, const uint8_t* __restrict__ prev,
                           long long n, int* __restrict__ changed) {
   int c = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+  const long long n16 = n >> 4;
+  const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, step = (long long)gridDim.x * blockDim.x;
+  for (long long i = t0; i < n16; i += step) {
+    uint4 o = reinterpret_cast<const uint4*>(out)[i];
+    const uint4 k = reinterpret_cast<const uint4*>(keep)[i];
+    const uint4 p = reinterpret_cast<const uint4*>(prev)[i];
+    o.x &= k.x; o.y &= k.y; o.z &= k.z; o.w &= k.w;   // bytes are 0 / 1: AND is the logical and
+    reinterpret_cast<uint4*>(out)[i] = o;
+    c |= (o.x != p.x) | (o.y != p.y) | (o.z != p.z) | (o.w != p.w);
+  }
+  for (long long i = (n16 << 4) + t0; i < n; i += step) {
     const uint8_t v = (out[i] && keep[i]) ? 1 : 0;
     out[i] = v;
     c |= v != prev[i];
@@ -333,40 +344,80 @@ __device__ __forceinline__ int reflect_index(int q, int len) {
   return q >= len ? period - 1 - q : q;
 }
 
-// One pass of a separable Gaussian (weights w[0..2 rad]) along axis 0 (x),
-// 1 (y) or 2 (z) of a float32 ROI with mode "reflect", float64 sum, float32
-// result (scipy.ndimage.correlate1d).  Rows (y, z) by blocks, x by threads.
-__global__ void k_wr_gauss(const float* __restrict__ in, float* __restrict__ out, int sx, int sy, int sz,
-                           const double* __restrict__ wts, int rad, int axis) {
+// scipy.ndimage.gaussian_filter of the ROI (x0, y0, z0) + (sx, sy, sz) of a
+// (., ny, nx) float32 level, evaluated only where near is set (the only
+// voxels whose smoothed value is read).  It reproduces scipy's three
+// correlate1d passes (x, then y, then z): mode "reflect" at the ROI's faces,
+// float64 sums rounded to float32 after each pass, and correlate1d's order
+// for symmetric weights: the centre term, then the tap pairs from the
+// outermost inwards, (left + right) w, with no fused multiply-add.
+// w points at the centre weight, w[j] = the weight at offsets -j and +j;
+// rad < 0: no smoothing (sigma 0), the crop itself.
+struct GaussRoi {
+  const float* lev;
+  int nx, ny, x0, y0, z0, sx, sy, sz, rad;
+  const double* w;
+};
+
+__device__ __forceinline__ float gauss_x(const GaussRoi& g, int x, int y, int z) {
+  const float* line = g.lev + ((size_t)(z + g.z0) * g.ny + (y + g.y0)) * g.nx + g.x0;
+  double s = __dmul_rn((double)line[x], g.w[0]);
+  for (int j = g.rad; j >= 1; --j)
+    s = __dadd_rn(s, __dmul_rn(__dadd_rn((double)line[reflect_index(x - j, g.sx)],
+                                         (double)line[reflect_index(x + j, g.sx)]), g.w[j]));
+  return (float)s;
+}
+
+__device__ __forceinline__ float gauss_xy(const GaussRoi& g, int x, int y, int z) {
+  double s = __dmul_rn((double)gauss_x(g, x, y, z), g.w[0]);
+  for (int j = g.rad; j >= 1; --j)
+    s = __dadd_rn(s, __dmul_rn(__dadd_rn((double)gauss_x(g, x, reflect_index(y - j, g.sy), z),
+                                         (double)gauss_x(g, x, reflect_index(y + j, g.sy), z)), g.w[j]));
+  return (float)s;
+}
+
+// One full correlate1d pass of the same filter along AXIS (0 x, 1 y, 2 z)
+// over a contiguous (sz, sy, sx) float32 ROI (src_nx / src_ny / offsets:
+// where the input lives; the first pass reads the level, later ones the
+// previous pass), in the order and rounding of gauss_x.
+template <int AXIS>
+__global__ void k_wr_gauss_pass(const float* __restrict__ src, int src_nx, int src_ny, int x0, int y0, int z0,
+                                float* __restrict__ out, int sx, int sy, int sz, const double* __restrict__ w, int rad) {
   WR_FOR_ROWS(sz * sy, row) {
     const int z = row / sy, y = row - z * sy;
+    const float* base = src + ((size_t)(z + z0) * src_ny + (y + y0)) * src_nx + x0;
+    const size_t stride = AXIS == 0 ? 1 : AXIS == 1 ? (size_t)src_nx : (size_t)src_nx * src_ny;
+    const int c = AXIS == 1 ? y : z;
+    const int len = AXIS == 0 ? sx : AXIS == 1 ? sy : sz;
     WR_FOR_COLS(sx, x) {
-      double s = 0.0;
-      if (axis == 0) {
-        const float* line = in + (size_t)row * sx;
-        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)line[reflect_index(x + k, sx)];
-      } else if (axis == 1) {
-        const float* col = in + (size_t)z * sy * sx + x;
-        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)col[(size_t)reflect_index(y + k, sy) * sx];
-      } else {
-        const float* col = in + (size_t)y * sx + x;
-        const size_t plane = (size_t)sx * sy;
-        for (int k = -rad; k <= rad; ++k) s += wts[k + rad] * (double)col[(size_t)reflect_index(z + k, sz) * plane];
-      }
+      const float* p = base + x;
+      const int cc = AXIS == 0 ? x : c;
+      const float* line = p - (size_t)cc * stride;
+      double s = __dmul_rn((double)*p, w[0]);
+      for (int j = rad; j >= 1; --j)
+        s = __dadd_rn(s, __dmul_rn(__dadd_rn((double)line[(size_t)reflect_index(cc - j, len) * stride],
+                                             (double)line[(size_t)reflect_index(cc + j, len) * stride]), w[j]));
       out[(size_t)row * sx + x] = (float)s;
     }
   }
 }
 
-// the ROI (x0, y0, z0) + (sx, sy, sz) of a (., ny, nx) float level, contiguous
-__global__ void k_copy_roi(const float* __restrict__ lev, float* __restrict__ out, int nx, int ny, int x0, int y0,
-                           int z0, int sx, int sy, int sz) {
-  const long long n = (long long)sx * sy * sz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % sx);
-    const long long rest = i / sx;
-    const int y = (int)(rest % sy), z = (int)(rest / sy);
-    out[i] = lev[((size_t)(z + z0) * ny + (y + y0)) * nx + (x + x0)];
+__global__ void k_wr_gauss_near(const GaussRoi g, const uint8_t* __restrict__ near, float* __restrict__ out) {
+  WR_FOR_ROWS(g.sz * g.sy, row) {
+    const int z = row / g.sy, y = row - z * g.sy;
+    WR_FOR_COLS(g.sx, x) {
+      const size_t i = (size_t)row * g.sx + x;
+      if (!near[i]) continue;
+      if (g.rad < 0) {
+        out[i] = g.lev[((size_t)(z + g.z0) * g.ny + (y + g.y0)) * g.nx + g.x0 + x];
+        continue;
+      }
+      double s = __dmul_rn((double)gauss_xy(g, x, y, z), g.w[0]);
+      for (int j = g.rad; j >= 1; --j)
+        s = __dadd_rn(s, __dmul_rn(__dadd_rn((double)gauss_xy(g, x, y, reflect_index(z - j, g.sz)),
+                                             (double)gauss_xy(g, x, y, reflect_index(z + j, g.sz))), g.w[j]));
+      out[i] = (float)s;
+    }
   }
 }
 
