@@ -227,6 +227,76 @@ __device__ __forceinline__ R spline_sample(const T* __restrict__ C, int px, int 
   return acc;
 }
 
+// Brick bounds of a mask's spline coefficients: for each 4x4x4 brick b of
+// the padded volume, (min, max) of the coefficients over [4b, 4b + 6] per
+// axis (the brick and the next one), rounded outward to float.  A sample
+// whose first taps (spline_axis .i[0]) fall in brick b reads only
+// coefficients in that range, and its value is a convex combination of them
+// (the cubic B-spline weights are non-negative and sum to 1): when the
+// range lies below 0.5 - 1e-4 the sample is not above 0.5, when it lies above
+// 0.5 + 1e-4 it is, whatever the rounding of the 64-tap sum (its error is
+// below 1e-14 of the largest coefficient).
+constexpr int kBrick = 4;
+constexpr float kBoundMargin = 1e-4f;
+
+__host__ __device__ inline int brick_count(int np) { return (np + kBrick - 1) / kBrick; }
+
+// stage 1: exact min / max of each brick, rounded outward
+__global__ void k_brick_minmax(const double* __restrict__ C, int px, int py, int pz, float2* __restrict__ out) {
+  const int nbx = brick_count(px), nby = brick_count(py), nbz = brick_count(pz);
+  const long long nb = (long long)nbx * nby * nbz;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb; b += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(b % nbx);
+    const long long rest = b / nbx;
+    const int by = (int)(rest % nby), bz = (int)(rest / nby);
+    double lo = INFINITY, hi = -INFINITY;
+    for (int z = bz * kBrick; z < min(pz, bz * kBrick + kBrick); ++z)
+      for (int y = by * kBrick; y < min(py, by * kBrick + kBrick); ++y) {
+        const double* row = C + ((size_t)z * py + y) * px;
+        for (int x = bx * kBrick; x < min(px, bx * kBrick + kBrick); ++x) {
+          const double v = row[x];
+          lo = fmin(lo, v);
+          hi = fmax(hi, v);
+        }
+      }
+    out[b] = make_float2(__double2float_rd(lo), __double2float_ru(hi));
+  }
+}
+
+// stage 2: each brick's range joined with its successors' along x, y and z
+__global__ void k_brick_dilate(const float2* __restrict__ in, int px, int py, int pz, float2* __restrict__ out) {
+  const int nbx = brick_count(px), nby = brick_count(py), nbz = brick_count(pz);
+  const long long nb = (long long)nbx * nby * nbz;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb; b += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(b % nbx);
+    const long long rest = b / nbx;
+    const int by = (int)(rest % nby), bz = (int)(rest / nby);
+    float lo = INFINITY, hi = -INFINITY;
+    for (int z = bz; z <= min(bz + 1, nbz - 1); ++z)
+      for (int y = by; y <= min(by + 1, nby - 1); ++y)
+        for (int x = bx; x <= min(bx + 1, nbx - 1); ++x) {
+          const float2 v = in[((size_t)z * nby + y) * nbx + x];
+          lo = fminf(lo, v.x);
+          hi = fmaxf(hi, v.y);
+        }
+    out[b] = make_float2(lo, hi);
+  }
+}
+
+// H_mask(x, y, z) > 0.5 evaluated as (float)spline_sample<double> > 0.5f,
+// decided from the brick bounds wherever they settle it
+__device__ __forceinline__ bool mask_above_half(const double* __restrict__ C, const float2* __restrict__ bounds, int px,
+                                                int py, int pz, float x, float y, float z) {
+  if (bounds) {
+    const int bx = spline_axis(x, px).i[0] / kBrick, by = spline_axis(y, py).i[0] / kBrick;
+    const int bz = spline_axis(z, pz).i[0] / kBrick;
+    const float2 b = __ldg(bounds + ((size_t)bz * brick_count(py) + by) * brick_count(px) + bx);
+    if (b.y < 0.5f - kBoundMargin) return false;
+    if (b.x > 0.5f + kBoundMargin) return true;
+  }
+  return (float)spline_sample<double, double>(C, px, py, pz, x, y, z) > 0.5f;
+}
+
 // The float32 coefficients of a level stored as x quads: Q[row][q] holds the
 // four taps (q - 1 .. q + 2, clamped to the row) a sample whose first x tap
 // is q - 1 reads, so one 16-byte load replaces four scalar loads.
@@ -277,6 +347,7 @@ struct XresArgs {
   int nxh, nyh, nzh;       // reference level extent
   const float4* cref;      // padded spline coefficients of the reference level, x quads
   const double* cmask;     // padded spline coefficients of its 0/1 exclusion mask, or null
+  const float2* cbounds;   // their brick bounds (mask_above_half), or null
   int pxh, pyh, pzh;       // padded extent
   double zr, zrh;          // zRatio / 2^l and zRatio_HR / 2^l: phase z of slice k is k zr / zrh
   const float4* phase0;    // the level's initial phase (x, y, z, -), or null for (x, y, z zr / zrh)

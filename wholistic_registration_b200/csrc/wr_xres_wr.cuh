@@ -458,7 +458,8 @@ __global__ void k_wr_paste(const uint8_t* __restrict__ region, uint8_t* __restri
 // H_mask(phase) <= 0.5 (compute_valid_mask_on_moving_grid, :2006-2028)
 template <int MODE>
 __global__ void k_wr_count_valid(const FieldSrc f, const float4* __restrict__ phase0, const uint8_t* __restrict__ mbits,
-                                 const double* __restrict__ cmask, int pxh, int pyh, int pzh, int nx, int ny, int nz,
+                                 const double* __restrict__ cmask, const float2* __restrict__ cbounds, int pxh,
+                                 int pyh, int pzh, int nx, int ny, int nz,
                                  double zr, double zrh, unsigned long long* __restrict__ count) {
   unsigned long long c = 0;
   WR_FOR_ROWS(nz * ny, row) {
@@ -468,7 +469,7 @@ __global__ void k_wr_count_valid(const FieldSrc f, const float4* __restrict__ ph
       const size_t i = (size_t)row * nx + x;
       if (mbits && (mbits[i] & 1)) continue;
       const float3 p = wr_phase<MODE>(f, phase0, x, y, z, fz0, i);
-      if (!((float)spline_sample<double, double>(cmask, pxh, pyh, pzh, p.x, p.y, p.z) > 0.5f)) ++c;
+      if (!mask_above_half(cmask, cbounds, pxh, pyh, pzh, p.x, p.y, p.z)) ++c;
     }
   }
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
