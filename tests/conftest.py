@@ -120,3 +120,11 @@ def load_xres_wr_case(name):
     arrays.update(out)
     option["wrong_region_enable"] = True
     return arrays, option
+
+
+def projection_ref_cases():
+    """(name, arrays) of the fixtures from the reference's own projection
+    kernels (tests/golden/make_projection_golden.py)."""
+    d = dict(np.load(os.path.join(GOLDEN, "projection_ref.npz")))
+    names = sorted({k[: -len("_params")] for k in d if k.endswith("_params")})
+    return [(n, {k[len(n) + 1:]: v for k, v in d.items() if k.startswith(n + "_")}) for n in names]

@@ -229,3 +229,35 @@ def test_projection_samples_reference_when_values_absent():
     vals = X.cubic_sample_scipy(ref.astype(np.float64), coords[..., 0], coords[..., 1], coords[..., 2]).astype(np.float32)
     want = X.project_max(vals, coords, planes, ref.shape[0], ref.shape[1], 1, 1.0, False, 0, 0.0)
     np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-3)
+
+
+def test_projection_matches_reference_kernels():
+    """The device max and weighted splats against the reference's own
+    projection kernels (fixtures from tests/golden/make_projection_golden.py):
+    the max splat bit for bit, the weighted one within float32 atomic
+    accumulation order (2e-6 of the largest output)."""
+    from conftest import projection_ref_cases
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    for name, c in projection_ref_cases():
+        p = c["params"]
+        xr, yr = int(p[0]), int(p[1])
+        ref = np.zeros((xr, yr, 6), np.float32)   # only its (x, y) extent is used when values are given
+        if name.startswith("max"):
+            _, _, zw, near, extra, ds, fill = p
+            got = C.project_coords_to_fixed_planes_gpu(c["coords"], ref, c["planes"], values_xyk=c["values"],
+                                                       z_window=float(zw), downsample_xy=int(ds), fill_value=float(fill),
+                                                       return_numpy=True, output_order="zxy",
+                                                       xy_splat_mode="nearest" if near else "subpixel_footprint",
+                                                       xy_extra_radius=int(extra))
+            np.testing.assert_array_equal(got, c["out"], err_msg=name)
+        else:
+            _, _, zw, zs, wm, ds, fill, eps = p
+            mode = {0: "hard", 1: "triangular", 2: "gaussian"}[int(wm)]
+            out, w = C.project_coords_to_fixed_planes_weighted_gpu(
+                c["coords"], ref, c["planes"], values_xyk=c["values"], z_window=float(zw),
+                z_sigma=None if zs < 0 else float(zs), z_weight_mode=mode, downsample_xy=int(ds),
+                fill_value=float(fill), return_numpy=True, output_order="zxy", eps=float(eps))
+            np.testing.assert_allclose(out, c["out"], rtol=0, atol=2e-6 * float(np.abs(c["out"]).max()),
+                                       err_msg=name)
+            np.testing.assert_allclose(w, c["sum_w"], rtol=0, atol=2e-6 * float(c["sum_w"].max()), err_msg=name)

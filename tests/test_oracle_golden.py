@@ -167,3 +167,30 @@ def test_xres_high_residual_oracle_matches_reference(name):
     # the sampled reference moves by its gradient times that phase ulp
     span = float(np.ptp(arrays["ref_sampled"]))
     np.testing.assert_allclose(sampled, arrays["ref_sampled"], rtol=0, atol=1e-6 * span)
+
+
+def test_projection_oracle_matches_reference_kernels():
+    """The oracle's max and weighted splats against the reference's own
+    projection kernels (compiled from its source, run with its wrappers'
+    steps): the max splat bit for bit, the weighted one within float32
+    atomic-accumulation order (2e-6 of the largest output; the oracle sums in
+    float64)."""
+    from conftest import projection_ref_cases
+    from oracle import xres_oracle as X
+
+    cases = projection_ref_cases()
+    assert len(cases) == 8
+    for name, c in cases:
+        p = c["params"]
+        if name.startswith("max"):
+            xr, yr, zw, near, extra, ds, fill = p
+            got = X.project_max(c["values"], c["coords"], c["planes"], int(xr), int(yr), int(ds), float(zw),
+                                bool(near), int(extra), float(fill))
+            np.testing.assert_array_equal(got, c["out"], err_msg=name)
+        else:
+            xr, yr, zw, zs, wm, ds, fill, eps = p
+            got, w = X.project_weighted(c["values"], c["coords"], c["planes"], int(xr), int(yr), int(ds), float(zw),
+                                        None if zs < 0 else float(zs), int(wm), float(fill), float(eps))
+            np.testing.assert_allclose(got, c["out"], rtol=0, atol=2e-6 * float(np.abs(c["out"]).max()),
+                                       err_msg=name)
+            np.testing.assert_allclose(w, c["sum_w"], rtol=0, atol=2e-6 * float(c["sum_w"].max()), err_msg=name)
