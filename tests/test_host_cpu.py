@@ -73,3 +73,37 @@ def test_division_multiplier_bound():
                              [nmax, nmax - 1, (nmax // d) * d, (nmax // d) * d - 1]])
         ns = ns[(ns >= 0) & (ns <= nmax)].astype(object)
         assert all((int(n) * m) >> 32 == int(n) // d for n in ns), d
+
+
+def test_xres_wrong_region_options_validated():
+    """wr_xres_workspace_size sizes the wrong-region correction's buffers and
+    rejects what the device path cannot run: an unknown exclusion mode, a
+    quantile outside [0, 1], a grid of more than 4096 control points per
+    slice (the per-slice sort lives in shared memory).  Host-only: no GPU."""
+    import ctypes
+
+    from wholistic_registration_b200 import _lib
+    from wholistic_registration_b200.registrar import LKParams
+
+    lib = _lib.load()
+    assert ctypes.sizeof(_lib.WrXresWrongRegion) == 36
+    p = LKParams(layer=1, iter=6, r=3, zRatio=3.0, movRange=5.0, smoothPenalty=0.05, tol=1e-3).to_c()
+
+    def size(wr, shape=(6, 48, 40), ref=(9, 48, 40)):
+        n = ctypes.c_size_t(0)
+        rc = lib.wr_xres_workspace_size(*shape, *ref, ctypes.byref(p), 2.0, 0, 0,
+                                        None if wr is None else ctypes.byref(wr), ctypes.byref(n))
+        return rc, n.value
+
+    def wr(mode=0, q=0.8):
+        return _lib.WrXresWrongRegion(1, 0, 3.0, 2, 2.0, 1.0, 2.0, mode, q)
+
+    rc0, off = size(None)
+    rc1, direct = size(wr())
+    rc2, high = size(wr(1))
+    assert rc0 == rc1 == rc2 == 0 and off < direct < high
+    assert size(_lib.WrXresWrongRegion(0, 0, 3.0, 2, 2.0, 1.0, 2.0, 0, 0.8))[1] == off   # enable = 0: off
+    assert size(wr(2))[0] == 3                       # WR_E_PARAM
+    assert size(wr(1, 1.5))[0] == 3
+    assert size(wr(), (2, 1024, 1024), (2, 1024, 1024))[0] == 2   # WR_E_SHAPE: 146 x 146 CPs per slice
+    assert b"4096 control points" in lib.wr_last_error()
