@@ -62,7 +62,7 @@ WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nz
  * getMotion_v2; wr NULL or wr->enable = 0 runs it without the wrong-region
  * correction (option["wrong_region_enable"] = False).  The correction needs
  * p->iter >= 2 to change anything (with one iteration no pass updates the
- * motion) and at most 4096 CPs per slice.
+ * motion).
  *   mov            (nz, ny, nx) float32 moving stack
  *   ref            (nzh, nyh, nxh) float32 reference stack
  *   excl_mask_mov  (nz, ny, nx) uint8 or NULL; excl_mask_ref (nzh, nyh, nxh)

@@ -261,3 +261,52 @@ def test_projection_matches_reference_kernels():
             np.testing.assert_allclose(out, c["out"], rtol=0, atol=2e-6 * float(np.abs(c["out"]).max()),
                                        err_msg=name)
             np.testing.assert_allclose(w, c["sum_w"], rtol=0, atol=2e-6 * float(c["sum_w"].max()), err_msg=name)
+
+
+def _impulse_pair(mov_shape, ref_shape, zr, zr_hr, seed):
+    """Moving and reference stacks cut at z spacings zr and zr_hr from one
+    blurred random-impulse field (physical z step 0.5), the moving one shifted
+    by a smooth in-plane field and Poisson-noised.  (x, y, z) float32."""
+    from scipy import ndimage
+
+    rng = np.random.default_rng(seed)
+    nzf = int(max(mov_shape[2] * zr, ref_shape[2] * zr_hr) / 0.5) + 8
+    field = np.zeros((mov_shape[0] + 8, mov_shape[1] + 8, nzf), np.float64)
+    k = field.size // 60
+    field.flat[rng.choice(field.size, k, replace=False)] = rng.uniform(2e3, 2e4, k)
+    field = ndimage.gaussian_filter(field, (2.0, 2.0, 3.0)) + 100.0
+
+    def cut(shape, zs, dx=0.0, dy=0.0):
+        X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+        pts = np.stack([X + 4 + dx, Y + 4 + dy, Z * zs / 0.5 + 4])
+        return ndimage.map_coordinates(field, pts, order=1, mode="nearest")
+
+    X, Y = np.meshgrid(np.arange(mov_shape[0]), np.arange(mov_shape[1]), indexing="ij")
+    dx = (1.2 * np.sin(2 * np.pi * Y / 37.0 + 0.3) + 0.5)[..., None]
+    dy = (1.0 * np.cos(2 * np.pi * X / 41.0) - 0.4)[..., None]
+    mov = rng.poisson(cut(mov_shape, zr, dx, dy)).astype(np.float32)
+    ref = rng.poisson(cut(ref_shape, zr_hr)).astype(np.float32)
+    return mov, ref
+
+
+def test_xres_wrong_region_many_control_points():
+    """More control points per slice (80 x 80 at r 1) than the detection's
+    shared-memory working set holds: the per-slice median / MAD and
+    components run on global scratch.  Against the oracle with the spread
+    bound; the oracle must have built a trap (regions found, re-runs done)."""
+    from oracle import xres_oracle as X
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    mov, ref = _impulse_pair((240, 240, 3), (240, 240, 5), 2.0, 1.0, 11)
+    option = {"mask_ref": np.zeros(ref.shape, np.uint8), "mask_mov": np.zeros(mov.shape, np.uint8), "layer": 0,
+              "iter": 6, "r": 1, "zRatio": 2.0, "zRatio_HR": 1.0, "smoothPenalty": 0.05, "movRange": 5.0, "tol": 1e-3,
+              "motion": None, "wrong_region_enable": True}
+    phase_o, motion_o, _, log = X.get_motion_v2(mov, ref, dict(option))
+    assert log["layer_0"]["wrong_region"]["regions"] > 0 and "error2" in log["layer_0"]["wrong_region"]
+    phase, motion, _ = C.getMotion_v2(mov, ref, dict(option))
+    dev_log, _ = C.last_registrar.error_log()
+    assert len(dev_log["layer_0"]["max_diff_motion"]) == len(log["layer_0"]["max_diff_motion"])
+    spread = _reference_spread({"mov": mov, "ref": ref}, option, motion_o)
+    bound = 1e-3 + 3.0 * spread
+    err = np.abs(motion - motion_o)
+    assert (err > bound).mean() <= 1e-3, f"motion: max excess {float((err - bound).max()):.3g}"

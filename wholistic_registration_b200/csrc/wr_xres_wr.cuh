@@ -78,7 +78,18 @@ __device__ double block_median(double* buf, int n, int cap) {
   return m;
 }
 
-constexpr int kWrMaxCp = 4096;   // CPs per slice the detection handles (shared-memory sort)
+// Per-slice working set of the detection: cap float64 sort keys (cap = n
+// rounded up to a power of two) and 6 n ints (labels, sizes, 4 box bounds).
+// Up to kWrSharedBytes it lives in shared memory, beyond in global scratch.
+constexpr int kWrSharedBytes = 200 * 1024;
+__host__ __device__ inline int wr_sort_cap(int n) {
+  int cap = 1;
+  while (cap < n) cap <<= 1;
+  return cap;
+}
+__host__ __device__ inline size_t wr_slice_bytes(int n) {
+  return ((size_t)wr_sort_cap(n) * 8 + (size_t)n * 24 + 255) & ~(size_t)255;
+}
 
 struct WrBox { int x0, x1, y0, y1, z; };
 
@@ -86,16 +97,17 @@ struct WrBox { int x0, x1, y0, y1, z; };
 // robust z-scores of the slice's CP errors (median / MAD over the inner CPs
 // when the grid has more than 144), significant CPs joined 4-connected in the
 // slice, components of at least min_size CPs widened by ceil(1.5 r) voxels
-// to boxes (appended to boxes, count in *nbox).
+// to boxes (appended to boxes, count in *nbox).  gscratch null: the working
+// set in dynamic shared memory; else slice z's at gscratch + z
+// wr_slice_bytes(n) (grids of more control points than shared memory holds).
 __global__ void k_wr_bad_regions(const double* __restrict__ err, int ncx, int ncy, int r, int nx, int ny,
                                  float mad_threshold, int min_size, WrBox* __restrict__ boxes, int* __restrict__ nbox,
-                                 int max_boxes) {
+                                 int max_boxes, char* __restrict__ gscratch) {
   extern __shared__ double wr_sm[];
   const int z = blockIdx.x;
   const int n = ncx * ncy;
-  int cap = 1;
-  while (cap < n) cap <<= 1;
-  double* buf = wr_sm;                                              // cap
+  const int cap = wr_sort_cap(n);
+  double* buf = gscratch ? reinterpret_cast<double*>(gscratch + (size_t)z * wr_slice_bytes(n)) : wr_sm;   // cap
   int* lab = reinterpret_cast<int*>(buf + cap);                     // n
   int* size = lab + n;                                              // n
   int* bb = size + n;                                               // 4 n: min x, max x, min y, max y
