@@ -4,9 +4,9 @@ TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/`` may
 import it.  The product path (``wholistic_registration_b200``) never calls
 into it and fails loudly when its CUDA library is missing.
 
-It restates, in NumPy, the reference's cross-resolution path with the
-wrong-region correction switched off (``wrong_region_enable=False``); paths
-are relative to ``src/wholistic_registration``:
+It restates, in NumPy, the reference's cross-resolution path, with and
+without its wrong-region correction; paths are relative to
+``src/wholistic_registration``:
 
 * ``utils/calFlowCrossResolution.py:2470-2663``  ``getMotion_v2``: pyramid of
   the moving stack on its grid and of the reference stack on its own
@@ -17,6 +17,12 @@ are relative to ``src/wholistic_registration``:
   included), CP grid, valid mask
 * ``utils/calFlowCrossResolution.py:463-478, 1144-1154``  the continuous
   reference ``H``: ``map_coordinates(order=3, mode="nearest")``
+* ``utils/calFlowCrossResolution.py:1190-1900, 2240-2467``  the wrong-region
+  correction: CP errors, outlier regions, the trap mask in reference space,
+  the two re-runs and the keep / discard choice, in both exclusion modes
+  ("direct" and "highresidual"); pinned to eleven runs of the reference
+* ``utils/calFlowCrossResolution.py:480-660, 700-1141``  the two projection
+  splats, pinned to fixtures of the reference's own kernels
 * ``utils/calFlowCrossResolution.py:41-272``  neighbour difference, error,
   gradients, 3x3 solve and CP grid interpolation, the same functions as
   ``calFlow3d_Wei_v1.py`` (restated in ``oracle.lk_oracle``)
