@@ -359,9 +359,12 @@ struct XresArgs {
 // mov - H(phase) with phase = (x, y, z zr / zrh) + motion, the reference's
 // gradient at the phase, exclusion by the moving mask or H_mask(phase) > 0.5,
 // then the same smoothing, window sums and CP neighbour difference as
-// k_lk_accumulate (utils/calFlowCrossResolution.py:2101-2170).
+// k_lk_accumulate (utils/calFlowCrossResolution.py:2101-2170).  Four CTAs
+// per SM (64 registers, some spills to L1): the kernel waits on the latency
+// of its spline gathers, and the fourth CTA hides more of it than the spills
+// cost (32.4 -> 29.8 ms per 32x1024x1024 registration against three CTAs).
 template <int MODE, int DIFF0, bool MASK>
-__global__ void __launch_bounds__(kAccThreads, 3) k_xres_accumulate(const __grid_constant__ XresArgs xa) {
+__global__ void __launch_bounds__(kAccThreads, 4) k_xres_accumulate(const __grid_constant__ XresArgs xa) {
   const IterArgs& a = xa.a;
   if (!*(volatile const int*)&a.st->active) return;
   extern __shared__ float4 smem4[];
