@@ -111,6 +111,25 @@ def load_xres_hr_case(name):
     return arrays, option
 
 
+def xres_opt_case_names():
+    import glob
+
+    return sorted(os.path.basename(f)[len("xresopt_"):-4] for f in glob.glob(os.path.join(GOLDEN, "xresopt_*.npz")))
+
+
+def load_xres_opt_case(name):
+    """(arrays, option) for a getMotion_v2 case with the wrong-region
+    correction at non-default options (stored with the fixture)."""
+    import json
+
+    arrays, option = load_xres_case(name)
+    out = dict(np.load(os.path.join(GOLDEN, f"xresopt_{name}.npz")))
+    option["wrong_region_enable"] = True
+    option.update(json.loads(str(out.pop("options"))))
+    arrays.update(out)
+    return arrays, option
+
+
 def load_xres_wr_case(name):
     """(arrays, option) for a getMotion_v2 case with the wrong-region correction
     on: the inputs of the xres case, the outputs of the reference's run with

@@ -276,6 +276,16 @@ XRES_WR_CASES = ("xr_mask_r2_l1", "xr_small_r3_l1", "xr_init_r4_l2", "xr_ragged_
 XRES_HR_CASES = {"xr_mask_r2_l1": 0.8, "xr_small_r3_l1": 0.8, "xr_ragged_r3_l2": 0.5, "xr_phase_r3_l1": 0.8}
 
 
+# cases re-run with non-default wrong-region options (metric, thresholds,
+# radii, no Gaussian smoothing)
+XRES_OPT_CASES = {
+    "xr_mask_r2_l1": {"wrong_region_metric": "mae", "wrong_region_mad_threshold": 2.5,
+                      "wrong_region_min_component_size": 3, "expand_radius_xy": 3.0, "intensity_k": 1.5},
+    "xr_small_r3_l1": {"sigma_grad": 0.0, "expand_radius_xy": 1.0, "wrong_region_mad_threshold": 2.0},
+    "xr_ragged_r3_l2": {"wrong_region_metric": "mae", "sigma_grad": 1.6, "wrong_region_min_component_size": 1},
+}
+
+
 def xres_pair(mov_shape, ref_shape, zr, zr_hr, seed):
     """Moving and reference stacks of one blob field sampled at z spacings zr
     and zr_hr (physical units per z index), the moving one displaced by a
@@ -369,6 +379,26 @@ def make_xres_cases(root, out_dir):
                             motion=np.asarray(motion, np.float32), ref_sampled=np.asarray(sampled, np.float64))
         print(f"{name} (wrong-region correction on): max |motion| {float(np.abs(motion).max()):.3f}")
     make_xres_hr_cases(cf, out_dir)
+    make_xres_opt_cases(cf, out_dir)
+
+
+def make_xres_opt_cases(cf, out_dir):
+    """xres cases re-run with the wrong-region correction at non-default options."""
+    with open(os.path.join(out_dir, "xres_cases.json")) as fh:
+        index = json.load(fh)
+    for name, extra in XRES_OPT_CASES.items():
+        d = dict(np.load(os.path.join(out_dir, f"xres_{name}.npz")))
+        option = dict(index[name])
+        option.update({"mask_ref": d["mask_ref"].copy(), "mask_mov": d["mask_mov"].copy(),
+                       "motion": d.get("motion_init"), "wrong_region_enable": True})
+        option.update(extra)
+        if "phase_init" in d:
+            option["phase"] = d["phase_init"]
+        phase, motion, sampled = cf.getMotion_v2(d["mov"].copy(), d["ref"].copy(), option)
+        np.savez_compressed(os.path.join(out_dir, f"xresopt_{name}.npz"), phase=np.asarray(phase, np.float32),
+                            motion=np.asarray(motion, np.float32), ref_sampled=np.asarray(sampled, np.float64),
+                            options=np.array(json.dumps(extra, sort_keys=True)))
+        print(f"{name} (wrong-region options {extra}): max |motion| {float(np.abs(motion).max()):.3f}")
 
 
 def make_xres_hr_cases(cf, out_dir):
@@ -393,20 +423,21 @@ def make_xres_hr_cases(cf, out_dir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr"], default=None)
+    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt"], default=None)
     args = ap.parse_args()
     if args.only in (None, "masks"):
         make_mask_cases(args.ref, HERE)
     if args.only in (None, "xres"):
         make_xres_cases(args.ref, HERE)
-    if args.only == "xreshr":
+    if args.only in ("xreshr", "xresopt"):
         src = os.path.join(args.ref, "src", "wholistic_registration")
         if "wholistic_registration" not in sys.modules:
             pkg = types.ModuleType("wholistic_registration")
             pkg.__path__ = [src]
             sys.modules["wholistic_registration"] = pkg
-        make_xres_hr_cases(importlib.import_module("wholistic_registration.utils.calFlowCrossResolution"), HERE)
-    if args.only in ("masks", "xres", "xreshr"):
+        cf = importlib.import_module("wholistic_registration.utils.calFlowCrossResolution")
+        (make_xres_hr_cases if args.only == "xreshr" else make_xres_opt_cases)(cf, HERE)
+    if args.only in ("masks", "xres", "xreshr", "xresopt"):
         return
     ref = load_reference(args.ref)
     if args.only in (None, "primitives"):

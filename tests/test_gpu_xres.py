@@ -28,8 +28,8 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import (load_xres_case, load_xres_hr_case, load_xres_wr_case, xres_case_names, xres_hr_case_names,
-                      xres_wr_case_names)
+from conftest import (load_xres_case, load_xres_hr_case, load_xres_opt_case, load_xres_wr_case, xres_case_names,
+                      xres_hr_case_names, xres_opt_case_names, xres_wr_case_names)
 
 pytestmark = pytest.mark.gpu
 
@@ -127,7 +127,8 @@ def test_xres_rejects_unbuilt_options():
 
 
 @pytest.mark.parametrize("kind,name", [("direct", n) for n in xres_wr_case_names()] +
-                         [("highresidual", n) for n in xres_hr_case_names()])
+                         [("highresidual", n) for n in xres_hr_case_names()] +
+                         [("options", n) for n in xres_opt_case_names()])
 def test_xres_wrong_region_matches_reference_run(kind, name):
     """getMotion_v2 with the wrong-region correction (the reference's
     default): the same bound as without it, the spread measured by the oracle
@@ -135,11 +136,13 @@ def test_xres_wrong_region_matches_reference_run(kind, name):
     flips a control point's outlier status or the keep / discard choice shows
     up there as spread).  The device log must hold the updates of every pass
     the oracle ran (one pass, or three when a trap was built).  Both exclusion
-    modes: "direct" (the default) and "highresidual"."""
+    modes: "direct" (the default) and "highresidual", and non-default options
+    (metric "mae", thresholds, radii, sigma_grad 0 and 1.6)."""
     from oracle import xres_oracle as X
     from wholistic_registration_b200 import calFlowCrossResolution as C
 
-    arrays, option = (load_xres_wr_case if kind == "direct" else load_xres_hr_case)(name)
+    loader = {"direct": load_xres_wr_case, "highresidual": load_xres_hr_case, "options": load_xres_opt_case}[kind]
+    arrays, option = loader(name)
     phase, motion, sampled = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(option))
     _, _, _, log = X.get_motion_v2(arrays["mov"], arrays["ref"], dict(option))
     dev_log, _ = C.last_registrar.error_log()

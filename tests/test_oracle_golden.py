@@ -7,8 +7,9 @@ import os
 import numpy as np
 import pytest
 
-from conftest import (GOLDEN, load_motion_case, load_xres_case, load_xres_hr_case, load_xres_wr_case,
-                      motion_case_names, option_from_case, xres_case_names, xres_hr_case_names, xres_wr_case_names)
+from conftest import (GOLDEN, load_motion_case, load_xres_case, load_xres_hr_case, load_xres_opt_case,
+                      load_xres_wr_case, motion_case_names, option_from_case, xres_case_names, xres_hr_case_names,
+                      xres_opt_case_names, xres_wr_case_names)
 from oracle import lk_oracle as O
 
 PRIM = os.path.join(GOLDEN, "primitives.npz")
@@ -194,3 +195,19 @@ def test_projection_oracle_matches_reference_kernels():
             np.testing.assert_allclose(got, c["out"], rtol=0, atol=2e-6 * float(np.abs(c["out"]).max()),
                                        err_msg=name)
             np.testing.assert_allclose(w, c["sum_w"], rtol=0, atol=2e-6 * float(c["sum_w"].max()), err_msg=name)
+
+
+@pytest.mark.parametrize("name", xres_opt_case_names())
+def test_xres_wrong_region_options_oracle_matches_reference(name):
+    """getMotion_v2 with the wrong-region correction at non-default options
+    (metric "mae", MAD threshold, minimum component size, expand radius,
+    intensity_k, sigma_grad 0 and 1.6): the restatement reproduces the
+    reference's run."""
+    from oracle import xres_oracle as X
+
+    arrays, option = load_xres_opt_case(name)
+    phase, motion, sampled, _ = X.get_motion_v2(arrays["mov"], arrays["ref"], option)
+    np.testing.assert_allclose(motion, arrays["motion"], rtol=0, atol=1e-5)
+    np.testing.assert_allclose(phase, arrays["phase"], rtol=0, atol=1e-5)
+    span = float(np.ptp(arrays["ref_sampled"]))
+    np.testing.assert_allclose(sampled, arrays["ref_sampled"], rtol=0, atol=1e-6 * span)
