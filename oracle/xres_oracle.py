@@ -20,7 +20,8 @@ without its wrong-region correction; paths are relative to
 * ``utils/calFlowCrossResolution.py:1190-1900, 2240-2467``  the wrong-region
   correction: CP errors, outlier regions, the trap mask in reference space,
   the two re-runs and the keep / discard choice, in both exclusion modes
-  ("direct" and "highresidual"); pinned to eleven runs of the reference
+  ("direct" and "highresidual") and at non-default options; pinned to
+  fourteen runs of the reference
 * ``utils/calFlowCrossResolution.py:480-660, 700-1141``  the two projection
   splats, pinned to fixtures of the reference's own kernels
 * ``utils/calFlowCrossResolution.py:41-272``  neighbour difference, error,
