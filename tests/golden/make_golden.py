@@ -7,8 +7,8 @@ Run in a container where the reference checkout is available:
 It imports the reference's NumPy path (``wholistic_registration.utils``) through
 a stub top-level package, because the package ``__init__`` pulls in I/O
 libraries that the hot path does not need.  Outputs are written next to this
-script as compressed ``.npz`` files and committed; the GPU box never reads the
-reference.
+script as compressed ``.npz`` files and committed; the tests read only those
+files, never the reference tree.
 
 Every array is in the reference's internal (x, y, z) layout.
 """
