@@ -55,8 +55,9 @@ typedef struct WrXresWrongRegion {
  * phase will be passed.  With the wrong-region correction (wr->enable) the
  * workspace also holds its buffers: a few bytes per voxel of each grid, and,
  * when a slice has more control points than the detection's shared-memory
- * working set holds (about 6000), 8 B per padded plus 24 B per control
- * point for every slice.
+ * working set holds (about 6000), 8 B times the next power of two above
+ * the slice's control-point count plus 24 B per control point, for every
+ * slice.
  */
 WR_API int wr_xres_workspace_size(int32_t nz, int32_t ny, int32_t nx, int32_t nzh, int32_t nyh, int32_t nxh,
                                   const WrLKParams* p, float zRatio_HR, int32_t has_mask_ref, int32_t has_phase_init,
