@@ -262,6 +262,9 @@ template <int MODE>
 __global__ void k_wr_seeds(const FieldSrc f, const float4* __restrict__ phase0, const uint8_t* __restrict__ bad, int nx,
                            int ny, int nz, double zr, double zrh, int nxh, int nyh, int nzh, int pass,
                            int* __restrict__ bbox, uint8_t* __restrict__ seed, int ox, int oy, int oz, int sx, int sy) {
+  // pass 0: each thread's box, then one set of atomics per warp (every lane
+  // of a row warp reaches the end: the row loop is warp-uniform)
+  int lo_x = INT_MAX, hi_x = INT_MIN, lo_y = INT_MAX, hi_y = INT_MIN, lo_z = INT_MAX, hi_z = INT_MIN;
   WR_FOR_ROWS(nz * ny, row) {
     const int z = row / ny, y = row - z * ny;
     const float fz0 = (float)(((double)z * zr) / zrh);
@@ -272,13 +275,22 @@ __global__ void k_wr_seeds(const FieldSrc f, const float4* __restrict__ phase0, 
       const int qx = (int)rintf(p.x), qy = (int)rintf(p.y), qz = (int)rintf(p.z);
       if (qx < 0 || qx >= nxh || qy < 0 || qy >= nyh || qz < 0 || qz >= nzh) continue;
       if (pass == 0) {
-        atomicMin(bbox, qx); atomicMax(bbox + 1, qx);
-        atomicMin(bbox + 2, qy); atomicMax(bbox + 3, qy);
-        atomicMin(bbox + 4, qz); atomicMax(bbox + 5, qz);
+        lo_x = min(lo_x, qx); hi_x = max(hi_x, qx);
+        lo_y = min(lo_y, qy); hi_y = max(hi_y, qy);
+        lo_z = min(lo_z, qz); hi_z = max(hi_z, qz);
       } else {
         seed[((size_t)(qz - oz) * sy + (qy - oy)) * sx + (qx - ox)] = 1;
       }
     }
+  }
+  if (pass != 0) return;
+  lo_x = __reduce_min_sync(0xffffffffu, lo_x); hi_x = __reduce_max_sync(0xffffffffu, hi_x);
+  lo_y = __reduce_min_sync(0xffffffffu, lo_y); hi_y = __reduce_max_sync(0xffffffffu, hi_y);
+  lo_z = __reduce_min_sync(0xffffffffu, lo_z); hi_z = __reduce_max_sync(0xffffffffu, hi_z);
+  if (threadIdx.x == 0 && hi_x >= 0) {
+    atomicMin(bbox, lo_x); atomicMax(bbox + 1, hi_x);
+    atomicMin(bbox + 2, lo_y); atomicMax(bbox + 3, hi_y);
+    atomicMin(bbox + 4, lo_z); atomicMax(bbox + 5, hi_z);
   }
 }
 
