@@ -382,6 +382,46 @@ def make_xres_cases(root, out_dir):
     make_xres_opt_cases(cf, out_dir)
 
 
+# compute_reference_from_block (utils/reference.py:102-124): (dual_channel, k, function)
+REFBLOCK_CASES = {"single": (False, 0.0, "raw"), "dual_sqrt": (True, 0.5, "sqrt"), "dual_log2": (True, 2.0, "log2"),
+                  "dual_k0": (True, 0.0, "raw")}
+
+
+def make_reference_block_cases(root, out_dir):
+    """A block of 12 uint16 [T, Z, Y, X] frames (a blob volume, per-frame
+    Poisson noise and drift, four frames strongly displaced) and its calcium
+    channel, through the reference's compute_reference_from_block."""
+    src = os.path.join(root, "src", "wholistic_registration")
+    if "wholistic_registration" not in sys.modules:
+        pkg = types.ModuleType("wholistic_registration")
+        pkg.__path__ = [src]
+        sys.modules["wholistic_registration"] = pkg
+    rf = importlib.import_module("wholistic_registration.utils.reference")
+    rng = np.random.default_rng(321)
+    T, Z, Y, X = 12, 5, 40, 36
+    Zg, Yg, Xg = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    cy, cx, amp = rng.uniform(0, Y, 25), rng.uniform(0, X, 25), rng.uniform(200, 900, 25)
+
+    def vol(dy, dx):
+        out = np.full((Z, Y, X), 120.0)
+        for i in range(25):
+            out += amp[i] * np.exp(-((Yg - cy[i] - dy) ** 2 + (Xg - cx[i] - dx) ** 2) / 18.0) * (1 + 0.1 * Zg)
+        return out
+
+    mem = np.stack([rng.poisson(vol(0.3 * t if t < 8 else 6.0, 0.2 * t if t < 8 else -5.0)) for t in range(T)])
+    mem = mem.astype(np.uint16)
+    ca = rng.poisson(np.broadcast_to(vol(0.0, 0.0) * 0.3, (T, Z, Y, X))).astype(np.uint16)
+    rec = {"mem": mem, "ca": ca}
+    for name, (dual, k, fn) in REFBLOCK_CASES.items():
+        config = {"channels": {"k": k, "function": fn, "dual_channel": dual}}
+        ref, idx = rf.compute_reference_from_block(mem.copy(), config, ca.copy() if dual else None)
+        rec[f"{name}_ref"], rec[f"{name}_idx"] = np.asarray(ref, np.float64), np.asarray(idx, np.int64)
+        rec[f"{name}_params"] = np.array([float(dual), k], np.float64)
+        rec[f"{name}_function"] = np.array(fn)
+        print(f"reference block {name}: indices {list(np.asarray(idx))}")
+    np.savez_compressed(os.path.join(out_dir, "reference_block.npz"), **rec)
+
+
 def make_xres_opt_cases(cf, out_dir):
     """xres cases re-run with the wrong-region correction at non-default options."""
     with open(os.path.join(out_dir, "xres_cases.json")) as fh:
@@ -423,12 +463,17 @@ def make_xres_hr_cases(cf, out_dir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt"], default=None)
+    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt", "refblock"],
+                    default=None)
     args = ap.parse_args()
     if args.only in (None, "masks"):
         make_mask_cases(args.ref, HERE)
     if args.only in (None, "xres"):
         make_xres_cases(args.ref, HERE)
+    if args.only in (None, "refblock"):
+        make_reference_block_cases(args.ref, HERE)
+    if args.only == "refblock":
+        return
     if args.only in ("xreshr", "xresopt"):
         src = os.path.join(args.ref, "src", "wholistic_registration")
         if "wholistic_registration" not in sys.modules:

@@ -109,3 +109,27 @@ def test_xres_wrong_region_options_validated():
     rc_big, big_off = size(None, (2, 1024, 1024), (2, 1024, 1024))
     rc_big2, big_on = size(wr(), (2, 1024, 1024), (2, 1024, 1024))
     assert rc_big == rc_big2 == 0 and big_on - big_off > 2 * (146 * 146 * 24)
+
+
+def test_compute_reference_from_block_matches_reference():
+    """compute_reference_from_block (utils/reference.py:102-124) against the
+    reference's own function run on the same block (fixture from
+    tests/golden/make_golden.py): the same frames picked, in order, and the
+    same reference volume (float32 correlation GEMM, float64 means) for a
+    single channel, dual channel with sqrt and log2 transforms, and k = 0.
+    Torch runs on CPU tensors here; the path is plain torch."""
+    import os
+
+    import numpy as np
+    import torch
+
+    from wholistic_registration_b200.registration import compute_reference_from_block
+
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_block.npz")))
+    mem, ca = torch.from_numpy(d["mem"]), torch.from_numpy(d["ca"])
+    for name in ("single", "dual_sqrt", "dual_log2", "dual_k0"):
+        dual, k = d[f"{name}_params"]
+        config = {"channels": {"k": float(k), "function": str(d[f"{name}_function"]), "dual_channel": bool(dual)}}
+        ref, idx = compute_reference_from_block(mem, config, ca if dual else None)
+        np.testing.assert_array_equal(idx, d[f"{name}_idx"], err_msg=name)
+        np.testing.assert_allclose(ref, d[f"{name}_ref"], rtol=1e-12, atol=1e-9, err_msg=name)

@@ -100,6 +100,31 @@ def _mean_of(frames, idx):
     return acc / len(idx)
 
 
+def compute_reference_from_block(mem_block, config, ca_block=None):
+    """utils/reference.py:102-124: the reference of a block of frames.
+
+    The mean of the frames best correlated with the most representative one
+    (pick_initial_reference with min(T // 2, 50) correlations), plus, for
+    dual-channel data with k != 0, the transformed float64 mean of the second
+    channel over the same frames.  mem_block / ca_block: [T, Z, Y, X] or
+    [T, Y, X] NumPy arrays (moved to the current CUDA device, as the
+    reference moves them to its GPU) or tensors (used where they are).
+    Returns (reference, indices) as NumPy arrays, as the reference does."""
+    channels = config["channels"]
+    k, function, dual = channels["k"], channels["function"], channels["dual_channel"]
+    n_corr = min(len(mem_block) // 2, 50)
+    device = mem_block.device if isinstance(mem_block, torch.Tensor) else _device(None)
+    mem = _as_tensor(mem_block, device)
+    mem_ref, indsort = pick_initial_reference(mem, max_corr_frames=n_corr)
+    result = mem_ref
+    if dual and k != 0:
+        if ca_block is None:
+            raise ValueError("ca_block is required for dual-channel data with k != 0")
+        ca_ref = _mean_of(_as_tensor(ca_block, device), indsort)
+        result = mem_ref + transform(ca_ref, k, function)
+    return result.cpu().numpy(), indsort.cpu().numpy()
+
+
 def _mse(a, b) -> float:
     """np.mean((a - b) ** 2) with NumPy's dtype rules: two arrays of one
     unsigned integer type subtract and square with wrap-around (as the
