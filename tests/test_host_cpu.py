@@ -133,3 +133,22 @@ def test_compute_reference_from_block_matches_reference():
         ref, idx = compute_reference_from_block(mem, config, ca if dual else None)
         np.testing.assert_array_equal(idx, d[f"{name}_idx"], err_msg=name)
         np.testing.assert_allclose(ref, d[f"{name}_ref"], rtol=1e-12, atol=1e-9, err_msg=name)
+
+
+def test_get_motion_v2_rejects_unknown_wrong_region_options():
+    """getMotion_v2 validates the wrong-region option keys before it touches
+    a device: an unknown metric or exclusion mode raises ValueError (the
+    reference accepts "mse" / "mae" and "direct" / "highresidual")."""
+    import numpy as np
+    import pytest
+
+    from wholistic_registration_b200 import calFlowCrossResolution as C
+
+    mov = np.zeros((8, 8, 2), np.float32)
+    ref = np.zeros((8, 8, 3), np.float32)
+    base = {"mask_ref": 0, "mask_mov": 0, "layer": 0, "iter": 2, "r": 1, "zRatio": 2.0, "zRatio_HR": 1.0,
+            "smoothPenalty": 0.05}
+    with pytest.raises(ValueError, match="metric"):
+        C.getMotion_v2(mov, ref, dict(base, wrong_region_metric="l2"))
+    with pytest.raises(ValueError, match="exclude_mode"):
+        C.getMotion_v2(mov, ref, dict(base, wrong_region_exclude_mode="lowresidual"))
