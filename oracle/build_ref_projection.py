@@ -37,9 +37,12 @@ def extract(ref_root: str) -> str:
     return "\n".join(parts)
 
 
-def build(ref_root: str = "/root/reference") -> str | None:
-    """Compile the library; None when the reference tree is absent."""
-    if not os.path.exists(os.path.join(ref_root, SRC_REL)):
+def build(ref_root: str | None = None) -> str | None:
+    """Compile the library; None when the reference tree is absent.
+
+    ref_root: the reference checkout (default: $WR_REFERENCE_ROOT)."""
+    ref_root = ref_root or os.environ.get("WR_REFERENCE_ROOT")
+    if not ref_root or not os.path.exists(os.path.join(ref_root, SRC_REL)):
         return None
     os.makedirs(OUT, exist_ok=True)
     with open(os.path.join(OUT, "ref_projection_kernels.cu"), "w") as fh:
@@ -52,4 +55,4 @@ def build(ref_root: str = "/root/reference") -> str | None:
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else None))

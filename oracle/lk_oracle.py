@@ -1,6 +1,6 @@
 """CPU oracle for the pyramid patch-wise Lucas-Kanade registration path.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``,
+TEST INFRASTRUCTURE ONLY.  This module checks the product: only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import
 it.  The product path (``wholistic_registration_b200``) never calls into it and
 fails loudly when its CUDA library is missing.

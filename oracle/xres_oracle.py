@@ -1,6 +1,6 @@
 """CPU oracle for the cross-resolution registration ``getMotion_v2``.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/`` may
+TEST INFRASTRUCTURE ONLY.  This module checks the product: only ``tests/`` may
 import it.  The product path (``wholistic_registration_b200``) never calls
 into it and fails loudly when its CUDA library is missing.
 

@@ -2,7 +2,8 @@
 
 Run in a container where the reference checkout is available:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
+    (or set WR_REFERENCE_ROOT)
 
 It imports the reference's NumPy path (``wholistic_registration.utils``) through
 a stub top-level package, because the package ``__init__`` pulls in I/O
@@ -28,6 +29,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from wholistic_registration_b200 import synthetic  # noqa: E402
+
+sys.path.insert(0, HERE)
+from bench_cases import BENCH_CASES, BENCH_ITER, BENCH_R, BENCH_RAW_PENALTY, bench_inputs  # noqa: E402
 
 
 def load_reference(root):
@@ -112,6 +116,39 @@ def make_motion_cases(ref, out_dir):
         print(f"{name}: shape {shape} error {err:.6f} evals/level {counts}")
     with open(os.path.join(out_dir, "motion_cases.json"), "w") as fh:
         json.dump(index, fh, indent=1, sort_keys=True)
+
+
+def make_bench_case(ref, out_dir, name):
+    import time
+
+    cf3 = ref["calFlow3d_Wei_v1"]
+    prep = ref["preprocess"]
+    zyx, seed, nb, md, layer, cov, stride = BENCH_CASES[name]
+    tmpl, mov, excl, digest = bench_inputs(name)
+    factor = prep.getSmPnltNormFctr(tmpl.astype(np.float64), {"mask_ref": excl})
+    option = {
+        "mask_ref": excl.copy(), "mask_mov": excl.copy(), "layer": layer, "iter": BENCH_ITER, "r": BENCH_R,
+        "zRatio": 1.0, "movRange": 5.0, "motion": None, "smoothPenalty": float(factor * BENCH_RAW_PENALTY),
+        "tol": 1e-3, "save_ite": 100,
+    }
+    t0 = time.time()
+    motion, err, _, log = cf3.getMotion(mov.copy(), tmpl.copy(), option)
+    t1 = time.time()
+    warped = cf3.correctMotion(mov.astype(np.float32), motion)
+    rec = {
+        "sha256": np.asarray(digest), "stride": np.int64(stride),
+        "motion_sub": np.ascontiguousarray(motion[::stride, ::stride].astype(np.float32)),
+        "warped_sub": np.ascontiguousarray(warped[::stride, ::stride].astype(np.float32)),
+        "warped_norm": np.float64(np.linalg.norm(warped.astype(np.float64))),
+        "current_error": np.float64(err), "penalty_factor": np.float64(factor),
+        "smooth_penalty": np.float64(factor * BENCH_RAW_PENALTY), "reference_seconds": np.float64(t1 - t0),
+    }
+    for lk, lv in log.items():
+        for key in ("diffError", "penaltyError", "currentError", "max_diff_motion"):
+            rec[f"{lk}/{key}"] = np.asarray(lv[key], dtype=np.float64)
+    np.savez_compressed(os.path.join(out_dir, f"bench_{name}.npz"), **rec)
+    counts = [len(v["currentError"]) for v in log.values()]
+    print(f"{name}: {t1 - t0:.0f} s, error {err:.6f}, evals/level {counts}", flush=True)
 
 
 def make_primitive_cases(ref, out_dir):
@@ -419,6 +456,15 @@ def make_reference_block_cases(root, out_dir):
         rec[f"{name}_params"] = np.array([float(dual), k], np.float64)
         rec[f"{name}_function"] = np.array(fn)
         print(f"reference block {name}: indices {list(np.asarray(idx))}")
+    # float32 frames (non-integer values): the reference's mean keeps float32
+    mem32 = (mem.astype(np.float32) * np.float32(0.37)).astype(np.float32)
+    ca32 = (ca.astype(np.float32) * np.float32(1.13)).astype(np.float32)
+    rec["mem_f32"], rec["ca_f32"] = mem32, ca32
+    for name, (dual, k, fn) in REFBLOCK_CASES.items():
+        config = {"channels": {"k": k, "function": fn, "dual_channel": dual}}
+        ref, idx = rf.compute_reference_from_block(mem32.copy(), config, ca32.copy() if dual else None)
+        rec[f"f32_{name}_ref"], rec[f"f32_{name}_idx"] = np.asarray(ref), np.asarray(idx, np.int64)
+        print(f"reference block f32 {name}: dtype {np.asarray(ref).dtype}, indices {list(np.asarray(idx))}")
     np.savez_compressed(os.path.join(out_dir, "reference_block.npz"), **rec)
 
 
@@ -462,10 +508,19 @@ def make_xres_hr_cases(cf, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt", "refblock"],
-                    default=None)
+    ap.add_argument("--ref", default=os.environ.get("WR_REFERENCE_ROOT"),
+                    help="root of the reference checkout (default: $WR_REFERENCE_ROOT)")
+    ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt", "refblock",
+                                       "bench"], default=None)
+    ap.add_argument("--case", default=None, help="with --only bench: one case of BENCH_CASES")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("the reference root is required (--ref or WR_REFERENCE_ROOT)")
+    if args.only == "bench":
+        ref = load_reference(args.ref)
+        for name in ([args.case] if args.case else BENCH_CASES):
+            make_bench_case(ref, HERE, name)
+        return
     if args.only in (None, "masks"):
         make_mask_cases(args.ref, HERE)
     if args.only in (None, "xres"):

@@ -133,15 +133,30 @@ def test_compute_reference_from_block_matches_reference():
         ref, idx = compute_reference_from_block(mem, config, ca if dual else None)
         np.testing.assert_array_equal(idx, d[f"{name}_idx"], err_msg=name)
         np.testing.assert_allclose(ref, d[f"{name}_ref"], rtol=1e-12, atol=1e-9, err_msg=name)
+    # float32 frames: the reference's mean (and its transform) stays float32
+    mem32, ca32 = torch.from_numpy(d["mem_f32"]), torch.from_numpy(d["ca_f32"])
+    for name in ("single", "dual_sqrt", "dual_log2", "dual_k0"):
+        dual, k = d[f"{name}_params"]
+        config = {"channels": {"k": float(k), "function": str(d[f"{name}_function"]), "dual_channel": bool(dual)}}
+        ref, idx = compute_reference_from_block(mem32, config, ca32 if dual else None)
+        want = d[f"f32_{name}_ref"]
+        assert ref.dtype == want.dtype == np.float32, (name, ref.dtype)
+        np.testing.assert_array_equal(idx, d[f"f32_{name}_idx"], err_msg=name)
+        # float32 sums in the same order; log2 / sqrt within a few float32 ulps
+        np.testing.assert_allclose(ref, want, rtol=1e-6, atol=0, err_msg=name)
 
 
-def test_get_motion_v2_rejects_unknown_wrong_region_options():
-    """getMotion_v2 validates the wrong-region option keys before it touches
-    a device: an unknown metric or exclusion mode raises ValueError (the
-    reference accepts "mse" / "mae" and "direct" / "highresidual")."""
+def test_get_motion_v2_wrong_region_options(monkeypatch):
+    """getMotion_v2 reads the wrong-region option keys as the reference does,
+    before it touches a device: an unknown metric raises ValueError
+    (utils/calFlowCrossResolution.py accepts "mse" / "mae"), and the exclusion
+    mode is "highresidual" only for that exact string; every other value
+    (None, "Direct", "lowresidual") takes the direct exclusion, as the
+    reference's equality test at utils/calFlowCrossResolution.py:2340 does."""
     import numpy as np
     import pytest
 
+    from wholistic_registration_b200 import _lib
     from wholistic_registration_b200 import calFlowCrossResolution as C
 
     mov = np.zeros((8, 8, 2), np.float32)
@@ -150,5 +165,18 @@ def test_get_motion_v2_rejects_unknown_wrong_region_options():
             "smoothPenalty": 0.05}
     with pytest.raises(ValueError, match="metric"):
         C.getMotion_v2(mov, ref, dict(base, wrong_region_metric="l2"))
-    with pytest.raises(ValueError, match="exclude_mode"):
-        C.getMotion_v2(mov, ref, dict(base, wrong_region_exclude_mode="lowresidual"))
+
+    class Captured(Exception):
+        pass
+
+    seen = []
+
+    def fake(*args):
+        seen.append(args[7])   # exclusion mode: 0 direct, 1 high residual
+        raise Captured
+
+    monkeypatch.setattr(_lib, "WrXresWrongRegion", fake)
+    for mode, want in (("highresidual", 1), ("direct", 0), ("Direct", 0), (None, 0), ("lowresidual", 0)):
+        with pytest.raises(Captured):
+            C.getMotion_v2(mov, ref, dict(base, wrong_region_exclude_mode=mode))
+        assert seen[-1] == want, (mode, seen[-1])

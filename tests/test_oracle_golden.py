@@ -83,6 +83,32 @@ def test_get_motion_matches_reference(name):
     np.testing.assert_allclose(warped, arrays["warped"], rtol=1e-6, atol=0)
 
 
+@pytest.mark.parametrize("name", ["c0slab_8x256x256_l2", "c1slab_4x512x512_l3"])
+def test_oracle_matches_reference_at_benchmarked_configuration(name):
+    """r = 16 (33 x 33 patches), 70 % ellipsoid mask, 3 and 4 levels: the
+    oracle reproduces the reference's run (the two smaller benchmarked-
+    configuration fixtures; the GPU tests use all four)."""
+    import sys
+
+    sys.path.insert(0, GOLDEN)
+    from bench_cases import BENCH_CASES, bench_inputs, bench_option
+
+    d = dict(np.load(os.path.join(GOLDEN, f"bench_{name}.npz")))
+    tmpl, mov, excl, digest = bench_inputs(name)
+    assert digest == str(d["sha256"])
+    layer = BENCH_CASES[name][4]
+    option = bench_option(name, float(d["smooth_penalty"]))
+    option["mask_ref"], option["mask_mov"] = excl.copy(), excl.copy()
+    motion, err, _, log = O.get_motion(mov, tmpl, option)
+    for l in range(layer + 1):
+        key = f"layer_{l}"
+        assert len(log[key]["currentError"]) == len(d[f"{key}/currentError"]), key
+        np.testing.assert_allclose(log[key]["currentError"], d[f"{key}/currentError"], rtol=1e-6)
+    s = int(d["stride"])
+    assert np.abs(motion[::s, ::s] - d["motion_sub"]).max() < 1e-4
+    np.testing.assert_allclose(err, float(d["current_error"]), rtol=1e-6)
+
+
 def test_penalty_factor():
     arrays, meta = load_motion_case("mask_r3_l1_z2")
     f = O.smooth_penalty_norm_factor(arrays["ref"].astype(np.float64), arrays["mask_ref"])

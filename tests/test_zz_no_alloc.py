@@ -53,6 +53,29 @@ def test_no_alloc_penalty_factor_matches_allocating_entry_point():
         np.testing.assert_allclose(b, a, rtol=1e-12)
 
 
+@pytest.mark.parametrize("shape", [(20, 1024, 1024), (128, 1024, 1024)])
+def test_no_alloc_penalty_factor_large_volumes(shape):
+    """Volumes whose partial sums fill more than 1024 slots of the static
+    array (20 x 1024 x 1024: 1280 slots) and exactly all of it
+    (128 x 1024 x 1024 = 134,217,728 voxels: 8192 slots), against the
+    allocating entry point, two calls in a row."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from wholistic_registration_b200 import _lib
+
+    lib = _lib.load()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(11)
+    ref = (torch.rand(shape, generator=gen, device="cuda") * 60000).to(torch.int32).to(torch.uint16)
+    mask = (torch.rand(shape, generator=gen, device="cuda") > 0.7).to(torch.uint8)
+    for m in (mask, None):
+        a, b = _call_both(lib, _lib, ref, m)
+        assert np.isfinite(a) and a > 0
+        np.testing.assert_allclose(b, a, rtol=1e-12)
+    del ref, mask
+    torch.cuda.empty_cache()
+
+
 def test_no_alloc_rejects_volumes_beyond_its_scratch():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")

@@ -180,15 +180,14 @@ def getMotion_v2(data_mov, data_ref, option, verbose=False):
         metric = str(option.get("wrong_region_metric", "mse")).lower()
         if metric not in ("mse", "mae"):
             raise ValueError("metric must be 'mse' or 'mae'")
-        modes = {"direct": 0, "highresidual": 1}
-        mode = option.get("wrong_region_exclude_mode", "direct")
-        if mode not in modes:
-            raise ValueError(f"wrong_region_exclude_mode must be 'direct' or 'highresidual', not {mode!r}")
+        # utils/calFlowCrossResolution.py:2340 tests only for "highresidual";
+        # every other value (None, "Direct", ...) takes the direct exclusion
+        exclude_high = option.get("wrong_region_exclude_mode", "direct") == "highresidual"
         wr = _lib.WrXresWrongRegion(1, 0 if metric == "mse" else 1,
                                     float(option.get("wrong_region_mad_threshold", 3.0)),
                                     int(option.get("wrong_region_min_component_size", 2)),
                                     float(option.get("expand_radius_xy", 2.0)), float(option.get("sigma_grad", 1.0)),
-                                    float(option.get("intensity_k", 2.0)), modes[mode],
+                                    float(option.get("intensity_k", 2.0)), 1 if exclude_high else 0,
                                     float(option.get("quantile_threshold_q", 0.8)))
     as_torch = isinstance(data_mov, torch.Tensor)
     device = data_mov.device if as_torch and data_mov.is_cuda else torch.device("cuda", torch.cuda.current_device())

@@ -91,13 +91,19 @@ def pick_initial_reference(frames: torch.Tensor, max_corr_frames: int = 20, spat
 
 
 def _mean_of(frames, idx):
-    """float64 mean of frames[idx] over the first axis, added in index
-    order as NumPy's axis-0 mean does (one frame converted at a time)."""
+    """Mean of frames[idx] over the first axis with NumPy's dtype rules, the
+    frames added in index order as NumPy's axis-0 mean adds them: float32
+    (and float16, through a float32 sum) frames keep their type, every other
+    type is averaged in float64."""
+    if frames.dtype in (torch.float32, torch.float16):
+        acc_t, out_t = torch.float32, frames.dtype
+    else:
+        acc_t, out_t = torch.float64, torch.float64
     acc = None
     for i in idx.tolist():
-        f = frames[int(i)].to(torch.float64)
+        f = frames[int(i)].to(acc_t)
         acc = f if acc is None else acc + f
-    return acc / len(idx)
+    return (acc / len(idx)).to(out_t)
 
 
 def compute_reference_from_block(mem_block, config, ca_block=None):
