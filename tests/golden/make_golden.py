@@ -468,6 +468,103 @@ def make_reference_block_cases(root, out_dir):
     np.savez_compressed(os.path.join(out_dir, "reference_block.npz"), **rec)
 
 
+# Per-batch wrappers (utils/registration.py:41-189 and :192-352) run through
+# the reference itself.  name: (wrapper, config overrides, given reference,
+# dual channel, motion_init)
+WRAPPER_CASES = {
+    "w3d_auto": ("3d", {}, False, False, False),
+    "w3d_dual_sqrt": ("3d", {"channels": {"dual_channel": True, "k": 0.5, "function": "sqrt"}}, False, True, False),
+    "w3d_given_init": ("3d", {"reference": {"pick_reference_auto": False}}, True, False, True),
+    "w2d_auto": ("2d", {}, False, False, False),
+    "w2d_dual_log2": ("2d", {"channels": {"dual_channel": True, "k": 2.0, "function": "log2"}}, False, True, False),
+}
+
+
+def wrapper_config(overrides):
+    """The config dict of a wrapper case (the reference reads it as TOML)."""
+    cfg = {
+        "reference": {"pick_reference_auto": True, "chunk_size": 2},
+        "channels": {"dual_channel": False, "k": 0.0, "function": "raw"},
+        "mask": {"maskRange": [5, 5000], "thresFactor": 3.0},
+        "pyramid": {"r": 3, "layer": 1, "iter": 6, "smoothPenalty": 0.08, "tolerance": 1e-3},
+        "MetaData": {"zRatio": 2.0},
+    }
+    for sec, kv in overrides.items():
+        cfg[sec] = dict(cfg[sec], **kv)
+    return cfg
+
+
+def wrapper_inputs(kind, seed):
+    """(membrane, calcium, reference, motion_init): uint16 [T, Z, Y, X] (3d)
+    or [T, Y, X] (2d) frames of a blob volume under small smooth shifts, with
+    a few bright outlier spots for the masks, and the calcium channel."""
+    rng = np.random.default_rng(seed)
+    zyx = (6, 56, 64) if kind == "3d" else (1, 60, 68)
+    T = 3
+    tmpl, _, _ = synthetic.make_pair(zyx, seed, n_blobs=160, max_disp=(1.0, 1.0, 0.3), noise=False)
+    base = tmpl.numpy().astype(np.float64)
+    mem, ca = [], []
+    for t in range(T):
+        _, mov, _ = synthetic.make_pair(zyx, seed + 10 + t, max_disp=(2.0, 2.0, 0.5 if kind == "3d" else 0.0),
+                                        template=torch_from(base), noise=False)
+        v = mov.numpy().astype(np.float64)
+        spots = rng.integers(0, np.array(zyx), size=(3, 3))
+        for z, y, x in spots:
+            v[z, max(0, y - 1):y + 2, max(0, x - 1):x + 2] += 20000.0
+        mem.append(rng.poisson(v))
+        ca.append(rng.poisson(0.3 * v + 50.0))
+    mem = np.clip(np.asarray(mem), 0, 65535).astype(np.uint16)
+    ca = np.clip(np.asarray(ca), 0, 65535).astype(np.uint16)
+    ref = mem.astype(np.float64).mean(axis=0)
+    init = rng.normal(scale=0.3, size=zyx + (3,)).astype(np.float32)
+    if kind == "2d":
+        mem, ca, ref, init = mem[:, 0], ca[:, 0], ref[0], init[0, :, :, :]
+    return mem, ca, ref, init
+
+
+def torch_from(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32))
+
+
+def make_wrapper_cases(root, out_dir):
+    import tempfile
+
+    import toml
+
+    try:
+        import skimage  # noqa: F401
+    except ImportError:
+        sys.modules.update(_skimage_standin())
+    load_reference(root)
+    reg = importlib.import_module("wholistic_registration.utils.registration")
+    rec = {}
+    for i, (name, (kind, over, given, dual, use_init)) in enumerate(WRAPPER_CASES.items()):
+        cfg = wrapper_config(over)
+        mem, ca, ref, init = wrapper_inputs(kind, 500 + i)
+        with tempfile.NamedTemporaryFile("w", suffix=".toml", delete=False) as fh:
+            toml.dump(cfg, fh)
+            path = fh.name
+        fn = reg.wbi_registration_3d if kind == "3d" else reg.wbi_registration_2d
+        out = fn(mem.copy(), path, reference_image=ref.copy() if given else None,
+                 motion_init=(init.copy() if use_init else None), verbose=False,
+                 moving_Ca_image=ca.copy() if dual else None)
+        os.unlink(path)
+        mem_out, ca_out, dat_ref, errors, motion_out = out
+        rec[f"{name}/mem"], rec[f"{name}/ca"], rec[f"{name}/ref"], rec[f"{name}/init"] = mem, ca, ref, init
+        rec[f"{name}/mem_out"] = np.asarray(mem_out, np.float32)
+        rec[f"{name}/ca_out"] = np.asarray(ca_out, np.float32)
+        rec[f"{name}/dat_ref"] = np.asarray(dat_ref)
+        rec[f"{name}/motion_out"] = np.asarray(motion_out, np.float32)
+        rec[f"{name}/initial_error"] = np.array([e["initial_error"] for e in errors], np.float64)
+        rec[f"{name}/eventual_error"] = np.array([e["eventual_error"] for e in errors], np.float64)
+        rec[f"{name}/config"] = np.array(json.dumps(cfg))
+        print(f"{name}: motion {np.asarray(motion_out).shape}, max |m| {np.abs(motion_out).max():.3f}, "
+              f"errors {[round(float(e['eventual_error']), 3) for e in errors]}", flush=True)
+    np.savez_compressed(os.path.join(out_dir, "wrappers.npz"), **rec)
+
+
 def make_xres_opt_cases(cf, out_dir):
     """xres cases re-run with the wrong-region correction at non-default options."""
     with open(os.path.join(out_dir, "xres_cases.json")) as fh:
@@ -511,11 +608,14 @@ def main():
     ap.add_argument("--ref", default=os.environ.get("WR_REFERENCE_ROOT"),
                     help="root of the reference checkout (default: $WR_REFERENCE_ROOT)")
     ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt", "refblock",
-                                       "bench"], default=None)
+                                       "bench", "wrappers"], default=None)
     ap.add_argument("--case", default=None, help="with --only bench: one case of BENCH_CASES")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference root is required (--ref or WR_REFERENCE_ROOT)")
+    if args.only == "wrappers":
+        make_wrapper_cases(args.ref, HERE)
+        return
     if args.only == "bench":
         ref = load_reference(args.ref)
         for name in ([args.case] if args.case else BENCH_CASES):

@@ -111,15 +111,20 @@ def test_xres_torch_inputs_stay_on_device():
     np.testing.assert_allclose(motion.cpu().numpy(), arrays["motion"], rtol=0, atol=1e-3)
 
 
-def test_xres_rejects_unbuilt_options():
+def test_xres_wrong_region_option_handling():
+    """An unknown metric raises ValueError; an exclusion mode other than
+    "highresidual" runs the direct exclusion, as the reference's equality test
+    (utils/calFlowCrossResolution.py:2340) does: same motion as "direct"."""
     from wholistic_registration_b200 import calFlowCrossResolution as C
 
     arrays, option = load_xres_case("xr_small_r3_l1")
     opt = dict(option)
     opt["wrong_region_enable"] = True
+    opt["wrong_region_exclude_mode"] = "direct"
+    _, direct, _ = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(opt))
     opt["wrong_region_exclude_mode"] = "lowresidual"
-    with pytest.raises(ValueError):
-        C.getMotion_v2(arrays["mov"], arrays["ref"], opt)
+    _, other, _ = C.getMotion_v2(arrays["mov"], arrays["ref"], dict(opt))
+    np.testing.assert_array_equal(other, direct)
     opt["wrong_region_exclude_mode"] = "direct"
     opt["wrong_region_metric"] = "l2"
     with pytest.raises(ValueError):
