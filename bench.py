@@ -329,6 +329,7 @@ def run_ours(args, wl, rank, world, local_rank):
     res["config"]["autotune"] = {"flags": reg.tune_flags, "ms_per_candidate": tune_report} if tune_report else None
     if not args.no_batch:
         res["config"]["batched_small_frames"] = run_batched_small(device)
+        res["config"]["uneven_batch"] = run_uneven_batch(device)
     if not args.no_xres:
         res["config"]["cross_resolution"] = run_cross_resolution(device, args.xres_shape)
         res["config"]["cross_resolution_wrong_region"] = run_cross_resolution(device, args.xres_shape,
@@ -432,6 +433,82 @@ def run_batched_small(device, n=16, reps=3):
         torch.cuda.synchronize()
         out[name + "_volumes_per_s"] = round(n * reps / (e0.elapsed_time(e1) * 1e-3), 2)
     out["speedup"] = round(out["batched_cuda_graph_volumes_per_s"] / out["one_call_per_frame_volumes_per_s"], 3)
+    return out
+
+
+def run_uneven_batch(device, reps=3, seed=777):
+    """Uneven batch: 48 volume pairs, 16 each at 32x256x256, 64x512x512 and
+    96x768x1024 (config-0 blob density and sinusoid fields), each with its
+    own random ellipsoid exclusion mask (40-90 % coverage) and patch radius
+    r in 4..16 (patches 9x9 .. 33x33), as many levels (up to 4) as the radius
+    leaves a CP on the coarsest, 10 iterations.  Timed: registering each
+    volume with its own parameters one call after another (registrars built
+    beforehand, one per shape and radius) against one per-frame-parameter
+    batched call (wr_lk_register_batch_each) replayed from a CUDA graph."""
+    import numpy as np
+    import torch
+
+    from wholistic_registration_b200 import LKParams, LKRegistrar, penalty_factor, synthetic
+    from wholistic_registration_b200.batch import BatchRegistrar
+
+    rng = np.random.default_rng(seed)
+    shapes = [(32, 256, 256)] * 16 + [(64, 512, 512)] * 16 + [(96, 768, 1024)] * 16
+    radii = [4, 6, 8, 10, 12, 14, 16]
+    movs, refs, masks, plist = [], [], [], []
+    for k, shape in enumerate(shapes):
+        nb = max(200, int(2000 * np.prod(shape) / (64 * 256 * 256)))
+        tmpl, mov, _ = synthetic.make_pair(shape, seed + k, n_blobs=nb, max_disp=(4.0, 4.0, 1.5), device=device)
+        cov = float(rng.uniform(0.4, 0.9))
+        excl = (~synthetic.ellipsoid_inclusion(shape, cov, device=device)).to(torch.uint8).contiguous()
+        r = int(radii[k % len(radii)])
+        layer = 0
+        while layer < 3 and min(shape[1], shape[2]) // 2 ** (layer + 1) >= 2 * r + 1:
+            layer += 1
+        factor = float(penalty_factor(tmpl.float().contiguous(), excl))
+        plist.append(LKParams(layer=layer, iter=10, r=r, zRatio=1.0, movRange=5.0, smoothPenalty=0.08 * factor,
+                              tol=1e-3))
+        movs.append(mov.contiguous())
+        refs.append(tmpl.contiguous())
+        masks.append(excl)
+        del tmpl, mov
+    torch.cuda.synchronize()
+    regs = {}
+    for shape, p in zip(shapes, plist):
+        key = (shape, p.r, p.layer)
+        if key not in regs:
+            regs[key] = (LKRegistrar(shape, p, device), torch.empty(shape + (3,), dtype=torch.float32, device=device))
+
+    def one_by_one():
+        for k, (shape, p) in enumerate(zip(shapes, plist)):
+            reg, out = regs[(shape, p.r, p.layer)]
+            reg.set_params(p)
+            reg.register(movs[k], refs[k], masks[k], masks[k], out=out)
+
+    br = BatchRegistrar(shapes, plist, device, graph=True)
+    br.register(movs, refs, masks, masks)
+
+    def batched():
+        br.register(movs, refs, masks, masks)
+
+    nvox = float(sum(np.prod(s) for s in shapes))
+    out = {"volumes": len(shapes), "shapes_zyx": [[32, 256, 256], [64, 512, 512], [96, 768, 1024]],
+           "radii": sorted({p.r for p in plist}), "layers": sorted({p.layer for p in plist}),
+           "mask_coverage": "uniform 0.4-0.9 per volume"}
+    for name, fn in (("one_call_per_volume", one_by_one), ("batched_cuda_graph", batched)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3 / reps
+        out[name + "_volumes_per_s"] = round(len(shapes) / sec, 2)
+        out[name + "_gvox_per_s"] = round(nvox / sec * 1e-9, 3)
+    out["speedup"] = round(out["batched_cuda_graph_volumes_per_s"] / out["one_call_per_volume_volumes_per_s"], 3)
+    del br, regs, movs, refs, masks
+    torch.cuda.empty_cache()
     return out
 
 

@@ -46,7 +46,7 @@ extern "C" {
 #define WR_ABI_VERSION 1
 #define WR_MAX_LEVELS 8
 #define WR_MAX_ITERS 64
-#define WR_MAX_BATCH 32
+#define WR_MAX_BATCH 64
 
 /* element types of input volumes */
 enum {
@@ -216,6 +216,22 @@ WR_API int wr_lk_batch_workspace_size(const WrLKItem* items, int32_t n, const Wr
  */
 WR_API int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, void* workspace,
                                 size_t workspace_bytes, void* stream);
+
+/*
+ * wr_lk_register_batch with one parameter set per frame (params[i] for
+ * items[i]), the reference's batch loop (utils/registration.py:299-346) run
+ * over volumes that each carry their own option dict: patch radius r, layer,
+ * iter, zRatio, movRange, smoothPenalty, tol and forced_updates may differ
+ * between frames; precision and the launch-shape flags (WR_LK_TILE_ORDER_X,
+ * WR_LK_CTAS_PER_SM_*) must agree.  Level l (0 = finest) of every frame that
+ * has it runs together, one persistent launch of the fused iteration kernel
+ * per LK iteration and field kind; each frame's results equal those of a
+ * wr_lk_register call on it with its own parameters.
+ */
+WR_API int wr_lk_batch_each_workspace_size(const WrLKItem* items, const WrLKParams* params, int32_t n,
+                                           size_t* bytes);
+WR_API int wr_lk_register_batch_each(const WrLKItem* items, const WrLKParams* params, int32_t n, void* workspace,
+                                     size_t workspace_bytes, void* stream);
 
 /*
  * getMotion followed by correctMotion of the same moving volume, the step the

@@ -114,7 +114,11 @@ def test_batch_argument_errors():
     from wholistic_registration_b200.batch import BatchRegistrar
 
     with pytest.raises(ValueError):
-        BatchRegistrar([(8, 64, 64)] * 33, _params())
+        BatchRegistrar([(8, 64, 64)] * 65, _params())
+    with pytest.raises(ValueError):
+        BatchRegistrar(SHAPES, [_params()] * 2)          # one parameter set per frame, or one for all
+    with pytest.raises(RuntimeError, match="precision"):
+        BatchRegistrar(SHAPES, [_params(), _params(precision=1), _params()])
     br = BatchRegistrar(SHAPES, _params())
     frames = _frames(70)
     with pytest.raises(ValueError):
@@ -160,3 +164,57 @@ def test_autotune_picks_and_caches(tmp_path, monkeypatch):
     assert (tmp_path / "autotune.json").exists()
     again = {}
     assert reg.autotune(report=again) == flags and again == report
+
+
+@pytest.mark.parametrize("init", [False, True])
+def test_batch_with_parameters_per_frame(init):
+    """Each frame with its own option dict (wr_lk_register_batch_each): patch
+    radius, levels, iterations, zRatio and penalty differ between frames, so
+    frames with fewer levels join the batch at their own top level; every
+    frame's motion, warped volume and evaluations equal its call alone."""
+    _need()
+    from wholistic_registration_b200 import LKRegistrar
+    from wholistic_registration_b200.batch import BatchRegistrar
+
+    shapes = [(8, 96, 80), (6, 70, 66), (8, 64, 64), (5, 120, 96), (7, 80, 90)]
+    frames = _frames(60, shapes)
+    plist = [_params(r=4, layer=2), _params(r=3, layer=1, iter=6, zRatio=2.0),
+             _params(r=2, layer=0, iter=4, smoothPenalty=50.0), _params(r=8, layer=2, tol=1e-4),
+             _params(r=5, layer=1, iter=8, movRange=2.0)]
+    inits = [torch.full(tuple(t.shape) + (3,), 0.3, dtype=torch.float32, device="cuda") for t, _, _ in frames] \
+        if init else None
+    br = BatchRegistrar(shapes, plist, warp=True, init=init)
+    motions, warps = br.register([f[1] for f in frames], [f[0] for f in frames], [f[2] for f in frames],
+                                 [f[2] for f in frames], inits=inits)
+    st = br.stats()
+    for i, ((t, m, e), p) in enumerate(zip(frames, plist)):
+        reg = LKRegistrar(tuple(t.shape), p)
+        w = torch.empty(t.shape, dtype=torch.float32, device="cuda")
+        alone = reg.register(m, t, e, e, motion_init=inits[i] if init else None, warped_out=w).clone()
+        torch.testing.assert_close(motions[i], alone, rtol=0, atol=0)
+        torch.testing.assert_close(warps[i], w, rtol=0, atol=0)
+        s = reg.stats()
+        assert [st[i].evals[l] for l in range(p.layer + 1)] == [s.evals[l] for l in range(p.layer + 1)]
+
+
+def test_batch_holds_64_frames():
+    """The batch cap is 64 frames (WR_MAX_BATCH); 48 small frames with their
+    own radii in one call equal their calls alone."""
+    _need()
+    from wholistic_registration_b200 import LKRegistrar
+    from wholistic_registration_b200 import _lib
+    from wholistic_registration_b200.batch import BatchRegistrar
+
+    assert _lib.MAX_BATCH == 64
+    shapes = [(4, 48 + 4 * (k % 5), 40 + 4 * (k % 7)) for k in range(48)]
+    frames = _frames(80, shapes)
+    plist = [_params(r=2 + k % 4, layer=1, iter=5) for k in range(48)]
+    br = BatchRegistrar(shapes, plist)
+    motions = br.register([f[1] for f in frames], [f[0] for f in frames], [f[2] for f in frames],
+                          [f[2] for f in frames])
+    for i in (0, 17, 33, 47):
+        t, m, e = frames[i]
+        alone = LKRegistrar(tuple(t.shape), plist[i]).register(m, t, e, e)
+        torch.testing.assert_close(motions[i], alone, rtol=0, atol=0)
+    with pytest.raises(ValueError):
+        BatchRegistrar([(4, 48, 40)] * 65, plist[0])

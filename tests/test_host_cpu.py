@@ -36,8 +36,8 @@ def test_flag_bits_match_header():
     h = open(os.path.join(root, "include", "wr_b200.h")).read()
     assert re.search(r"WR_LK_TILE_ORDER_X = 1 << 8", h)
     assert re.search(r"WR_LK_CTAS_PER_SM_SHIFT = 12", h)
-    assert re.search(r"#define WR_MAX_BATCH 32", h)
-    assert _lib.WR_LK_TILE_ORDER_X == 1 << 8 and _lib.WR_LK_CTAS_PER_SM(3) == 3 << 12 and _lib.MAX_BATCH == 32
+    assert re.search(r"#define WR_MAX_BATCH 64", h)
+    assert _lib.WR_LK_TILE_ORDER_X == 1 << 8 and _lib.WR_LK_CTAS_PER_SM(3) == 3 << 12 and _lib.MAX_BATCH == 64
 
 
 def test_wrapper_host_helpers(tmp_path):

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "_wr_b200.so")
 
 MAX_LEVELS = 8
 MAX_ITERS = 64
-MAX_BATCH = 32
+MAX_BATCH = 64
 
 WR_U8, WR_U16, WR_F32 = 1, 2, 3
 WR_PREC_F32, WR_PREC_F16, WR_PREC_BF16 = 0, 1, 2
@@ -46,6 +46,8 @@ EXPORTS = (
     "wr_lk_register_warp",
     "wr_lk_batch_workspace_size",
     "wr_lk_register_batch",
+    "wr_lk_batch_each_workspace_size",
+    "wr_lk_register_batch_each",
     "wr_warp_trilinear",
     "wr_penalty_factor",
     "wr_penalty_factor_noalloc",
@@ -199,6 +201,10 @@ def load():
         lib.wr_lk_batch_workspace_size.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams),
                                                    ctypes.POINTER(sz)]
         lib.wr_lk_register_batch.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams), vp, sz, vp]
+        lib.wr_lk_batch_each_workspace_size.argtypes = [ctypes.POINTER(WrLKItem), ctypes.POINTER(WrLKParams), i32,
+                                                        ctypes.POINTER(sz)]
+        lib.wr_lk_register_batch_each.argtypes = [ctypes.POINTER(WrLKItem), ctypes.POINTER(WrLKParams), i32, vp, sz,
+                                                  vp]
         lib.wr_lk_register_warp.argtypes = (lib.wr_lk_register.argtypes[:7] + [vp] + lib.wr_lk_register.argtypes[7:]
                                             + [ctypes.POINTER(WrProfile)])
         lib.wr_warp_trilinear.argtypes = [ctypes.POINTER(WrVolume), vp, vp, vp]

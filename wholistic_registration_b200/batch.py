@@ -2,12 +2,14 @@
 
 The reference registers the frames of a batch one after another with the same
 option dict (``utils/registration.py:299-346``).  ``BatchRegistrar`` runs up
-to 32 of them together through ``wr_lk_register_batch``: every pyramid level
+to 64 of them together through ``wr_lk_register_batch_each``: every pyramid level
 advances all frames with one persistent launch of the fused iteration kernel
 per LK iteration (and one launch each of the decision, solve and bookkeeping
 kernels), each frame keeping its own stopping state, so each frame's motion
 equals a ``LKRegistrar.register`` call on it alone.  Frames may have
-different shapes.  Small volumes, which leave most of the GPU idle when
+different shapes and, with a list of ``LKParams`` (one per frame), their own
+patch radius, levels, iterations and penalties; they share the storage
+precision.  Small volumes, which leave most of the GPU idle when
 registered one by one, gain the most.
 
 ``graph=True`` captures the whole batched call into a CUDA graph on the
@@ -37,11 +39,14 @@ class BatchRegistrar:
             raise ValueError(f"a batch holds 1..{_lib.MAX_BATCH} frames")
         if dtype not in _DTYPES:
             raise ValueError(f"dtype {dtype} not supported (uint8, uint16, float32)")
-        self.params = params
+        plist = list(params) if isinstance(params, (list, tuple)) else [params] * self.n
+        if len(plist) != self.n:
+            raise ValueError(f"params: one LKParams for the batch or one per frame ({self.n})")
+        self.params = plist
         self.dtype = dtype
         self.has_mmov, self.has_mref, self.has_init, self.has_warp = bool(mask_mov), bool(mask_ref), bool(init), bool(warp)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        self._cp = params.to_c()
+        self._cps = (_lib.WrLKParams * self.n)(*[q.to_c() for q in plist])
         self._items = (_lib.WrLKItem * self.n)()
         one = ctypes.c_void_p(1)   # placeholder pointers: the size query reads shapes and presence only
         for i, s in enumerate(self.shapes):
@@ -52,8 +57,8 @@ class BatchRegistrar:
             it.excl_mask_ref = one if self.has_mref else None
             it.motion_init = one if self.has_init else None
         nbytes = ctypes.c_size_t(0)
-        _lib.check("wr_lk_batch_workspace_size",
-                   self.lib.wr_lk_batch_workspace_size(self._items, self.n, ctypes.byref(self._cp), ctypes.byref(nbytes)))
+        _lib.check("wr_lk_batch_each_workspace_size",
+                   self.lib.wr_lk_batch_each_workspace_size(self._items, self._cps, self.n, ctypes.byref(nbytes)))
         self.workspace_bytes = int(nbytes.value)
         self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
         self._ws_ptr = (self.workspace.data_ptr() + 255) // 256 * 256
@@ -108,10 +113,11 @@ class BatchRegistrar:
             it.motion_out = self.motion[i].data_ptr()
             it.warped_out = self.warped[i].data_ptr() if self.warped else None
             it.stats = self.stats_dev[i].data_ptr()
-        self._cp.flags = flags
-        _lib.check("wr_lk_register_batch",
-                   self.lib.wr_lk_register_batch(self._items, self.n, ctypes.byref(self._cp), self._ws_ptr,
-                                                 self.workspace_bytes, stream))
+        for i in range(self.n):
+            self._cps[i].flags = flags
+        _lib.check("wr_lk_register_batch_each",
+                   self.lib.wr_lk_register_batch_each(self._items, self._cps, self.n, self._ws_ptr,
+                                                      self.workspace_bytes, stream))
 
     # -- API -------------------------------------------------------------------------------------------------------
     def register(self, movs, refs, masks_mov=None, masks_ref=None, inits=None, reuse_reference=False):

@@ -723,67 +723,106 @@ static void launch_batch(int mode, int diff0, const BatchIter& b, long long ntil
   }
 }
 
+// Frames may differ in shape, patch radius, number of levels, iterations and
+// every other solver parameter except the precision and the launch-shape
+// flags.  Level l (0 = finest) of every frame that has it runs together; an
+// iteration launch holds the frames with that many iterations left, grouped
+// by the kernel variant their field needs (a frame's first level starts from
+// its initial field while frames with more levels up-sample theirs).
 template <typename T, int PREC>
-static int run_batch(const Plan* plans, const size_t* offs, const WrLKItem* items, int n, const WrLKParams* p,
+static int run_batch(const Plan* plans, const size_t* offs, const WrLKItem* items, int n, const WrLKParams* params,
                      void* workspace, cudaStream_t s) {
   void* ws[kMaxBatch];
+  int max_levels = 0, max_iter = 0;
   for (int i = 0; i < n; ++i) {
     ws[i] = static_cast<char*>(workspace) + offs[i];
-    prepare_frame<T, PREC>(plans[i], p, (const T*)items[i].mov.data, (const T*)items[i].ref.data,
+    prepare_frame<T, PREC>(plans[i], &params[i], (const T*)items[i].mov.data, (const T*)items[i].ref.data,
                            items[i].excl_mask_mov, items[i].excl_mask_ref, items[i].motion_init, ws[i], s);
+    max_levels = std::max(max_levels, plans[i].levels);
+    max_iter = std::max(max_iter, plans[i].iter);
   }
   const bool has_init = items[0].motion_init != nullptr;
   const bool has_mmov = items[0].excl_mask_mov != nullptr;
   const bool mask = has_mmov || items[0].excl_mask_ref != nullptr;
-  const Plan& P0 = plans[0];
-  const double sps = p->smoothPenalty * (double)((2 * P0.r + 1) * (2 * P0.r + 1));
-  const float sps_f = (float)sps;
-  BatchIter b;
+  const int flags = params[0].flags;
+  const int order = (flags & WR_LK_TILE_ORDER_X) ? 1 : 0;
+  static thread_local BatchIter b;
   BatchDecide bd;
   BatchUpdate bu;
   BatchState bs;
-  memset(&b, 0, sizeof(b));
-  memset(&bd, 0, sizeof(bd));
-  memset(&bu, 0, sizeof(bu));
-  memset(&bs, 0, sizeof(bs));
-  b.n = bd.n = bu.n = bs.n = n;
-  b.order = (p->flags & WR_LK_TILE_ORDER_X) ? 1 : 0;
-  for (int l = P0.levels - 1; l >= 0; --l) {
-    int mode0 = FIELD_ZERO;
+  for (int l = max_levels - 1; l >= 0; --l) {
+    IterArgs args[kMaxBatch];
     FieldSrc f0[kMaxBatch];
-    long long max_ncp = 1;
-    b.tile_start[0] = 0;
-    for (int i = 0; i < n; ++i) {
-      const LevelPlan& L = plans[i].lv[l];
-      b.item[i] = begin_level(plans[i], l, ws[i], has_init, mask, has_mmov, &mode0, s);
-      f0[i] = b.item[i].field0;
-      b.tile_start[i + 1] = b.tile_start[i] + (int)L.nblk;
-      bd.st[i] = bu.st[i] = bs.st[i] = b.item[i].st;
-      bd.errpart[i] = b.item[i].errpart;
-      bd.penpart[i] = b.item[i].penpart;
-      bd.nblk[i] = L.nblk;
-      bd.n_vox[i] = (double)L.n;
-      bu.cp[i] = at_off<float4>(ws[i], L.cp);
-      bu.sums[i] = b.item[i].sums;
-      bu.ncp[i] = L.ncp;
-      if (L.ncp > max_ncp) max_ncp = L.ncp;
-    }
-    const long long ntiles = b.tile_start[n];
-    const int forced = p->forced_updates[l];
-    const double zratio_d = P0.lv[l].zratio_d;
-    const dim3 ugrid((unsigned)((max_ncp + kThreads - 1) / kThreads), (unsigned)n);
-    for (int it = 0; it < P0.iter; ++it) {
-      const int mode = it == 0 ? mode0 : FIELD_CP;
-      const int diff0 = it == 1 ? mode0 : kNoDiff;
-      for (int i = 0; i < n; ++i) b.item[i].field = it == 0 ? f0[i] : field_src(plans[i], l, FIELD_CP, ws[i]);
-      launch_batch<PREC>(mode, diff0, b, ntiles, accumulate_smem(P0.w, diff0 == FIELD_UP), mask, p->flags, s);
-      if (diff0 != kNoDiff) k_first_post_batch<<<1, 32, 0, s>>>(bs, l, forced);
-      k_decide_batch<<<n, 1024, 0, s>>>(bd, sps, l, it, P0.iter, p->tol, forced);
-      if (PREC == WR_PREC_F32)
-        k_update_batch<false><<<ugrid, kThreads, 0, s>>>(bu, sps, sps_f, (double)p->movRange, zratio_d);
-      else
-        k_update_batch<true><<<ugrid, kThreads, 0, s>>>(bu, sps, sps_f, (double)p->movRange, zratio_d);
-      k_post_batch<<<1, 32, 0, s>>>(bs, l, forced, it == 0 ? 1 : 0);
+    int mode0[kMaxBatch];
+    for (int i = 0; i < n; ++i)
+      if (l < plans[i].levels) {
+        args[i] = begin_level(plans[i], l, ws[i], has_init, mask, has_mmov, &mode0[i], s);
+        f0[i] = args[i].field0;
+      }
+    for (int it = 0; it < max_iter; ++it) {
+      int act[kMaxBatch], na = 0;
+      for (int i = 0; i < n; ++i)
+        if (l < plans[i].levels && it < plans[i].iter) act[na++] = i;
+      if (na == 0) break;
+      // the fused iteration, one launch per (field mode, first-difference mode) group
+      bool done[kMaxBatch] = {};
+      for (int g = 0; g < na; ++g) {
+        if (done[g]) continue;
+        const int i0 = act[g];
+        const int mode = it == 0 ? mode0[i0] : FIELD_CP;
+        const int diff0 = it == 1 ? mode0[i0] : kNoDiff;
+        memset(&b, 0, sizeof(b));
+        b.order = order;
+        size_t smem = 0;
+        int m = 0;
+        b.tile_start[0] = 0;
+        for (int h = g; h < na; ++h) {
+          const int i = act[h];
+          if (done[h] || (it == 0 ? mode0[i] : FIELD_CP) != mode || (it == 1 ? mode0[i] : kNoDiff) != diff0) continue;
+          done[h] = true;
+          b.item[m] = args[i];
+          b.item[m].field = it == 0 ? f0[i] : field_src(plans[i], l, FIELD_CP, ws[i]);
+          b.tile_start[m + 1] = b.tile_start[m] + (int)plans[i].lv[l].nblk;
+          smem = std::max(smem, accumulate_smem(plans[i].w, diff0 == FIELD_UP));
+          ++m;
+        }
+        b.n = m;
+        launch_batch<PREC>(mode, diff0, b, b.tile_start[m], smem, mask, flags, s);
+      }
+      memset(&bd, 0, sizeof(bd));
+      memset(&bu, 0, sizeof(bu));
+      memset(&bs, 0, sizeof(bs));
+      bd.n = bu.n = bs.n = na;
+      long long max_ncp = 1;
+      for (int k = 0; k < na; ++k) {
+        const int i = act[k];
+        const Plan& P = plans[i];
+        const LevelPlan& L = P.lv[l];
+        const double sps = params[i].smoothPenalty * (double)((2 * P.r + 1) * (2 * P.r + 1));
+        bd.st[k] = bu.st[k] = bs.st[k] = args[i].st;
+        bd.errpart[k] = args[i].errpart;
+        bd.penpart[k] = args[i].penpart;
+        bd.nblk[k] = L.nblk;
+        bd.n_vox[k] = (double)L.n;
+        bd.sps[k] = sps;
+        bd.tol[k] = params[i].tol;
+        bd.iter[k] = P.iter;
+        bd.forced[k] = bs.forced[k] = params[i].forced_updates[l];
+        bu.cp[k] = at_off<float4>(ws[i], L.cp);
+        bu.sums[k] = args[i].sums;
+        bu.ncp[k] = L.ncp;
+        bu.sps[k] = sps;
+        bu.sps_f[k] = (float)sps;
+        bu.mov_range[k] = (double)params[i].movRange;
+        bu.zratio_d[k] = L.zratio_d;
+        max_ncp = std::max(max_ncp, L.ncp);
+      }
+      const dim3 ugrid((unsigned)((max_ncp + kThreads - 1) / kThreads), (unsigned)na);
+      if (it == 1) k_first_post_batch<<<1, kMaxBatch, 0, s>>>(bs, l);
+      k_decide_batch<<<na, 1024, 0, s>>>(bd, l, it);
+      if (PREC == WR_PREC_F32) k_update_batch<false><<<ugrid, kThreads, 0, s>>>(bu);
+      else k_update_batch<true><<<ugrid, kThreads, 0, s>>>(bu);
+      k_post_batch<<<1, kMaxBatch, 0, s>>>(bs, l, it == 0 ? 1 : 0);
     }
   }
   for (int i = 0; i < n; ++i)
@@ -877,11 +916,12 @@ int wr_lk_workspace_size(int32_t nz, int32_t ny, int32_t nx, const WrLKParams* p
 
 // Plans and workspace offsets of a batch (validates the items; with
 // sizes_only the data and output pointers are not looked at).
-static int batch_plans(const WrLKItem* items, int32_t n, const WrLKParams* p, Plan* plans, size_t* offs,
+static int batch_plans(const WrLKItem* items, int32_t n, const WrLKParams* params, Plan* plans, size_t* offs,
                        size_t* total, bool sizes_only) {
-  if (!items || !p) return fail(WR_E_NULL, "items or params is NULL");
+  if (!items || !params) return fail(WR_E_NULL, "items or params is NULL");
   if (n < 1 || n > WR_MAX_BATCH) return fail(WR_E_PARAM, "batch size must be 1..WR_MAX_BATCH");
   size_t cur = 0;
+  const int launch_bits = WR_LK_TILE_ORDER_X | WR_LK_CTAS_PER_SM_MASK;
   for (int i = 0; i < n; ++i) {
     const WrLKItem& it = items[i];
     int rc;
@@ -903,8 +943,10 @@ static int batch_plans(const WrLKItem* items, int32_t n, const WrLKParams* p, Pl
         (it.excl_mask_ref != nullptr) != (items[0].excl_mask_ref != nullptr) ||
         (it.motion_init != nullptr) != (items[0].motion_init != nullptr))
       return fail(WR_E_PARAM, "the frames of a batch must agree on which masks and initial fields are given");
+    if (params[i].precision != params[0].precision || (params[i].flags & launch_bits) != (params[0].flags & launch_bits))
+      return fail(WR_E_PARAM, "the frames of a batch must agree on the precision and the launch-shape flags");
     const char* why;
-    rc = make_plan(it.mov.nz, it.mov.ny, it.mov.nx, p, true, true, true, &plans[i], &why);
+    rc = make_plan(it.mov.nz, it.mov.ny, it.mov.nx, &params[i], true, true, true, &plans[i], &why);
     if (rc) return fail(rc, why);
     offs[i] = cur;
     cur = align_up(cur + plans[i].total);
@@ -913,18 +955,18 @@ static int batch_plans(const WrLKItem* items, int32_t n, const WrLKParams* p, Pl
   return WR_OK;
 }
 
-int wr_lk_batch_workspace_size(const WrLKItem* items, int32_t n, const WrLKParams* p, size_t* bytes) {
+int wr_lk_batch_each_workspace_size(const WrLKItem* items, const WrLKParams* params, int32_t n, size_t* bytes) {
   if (!bytes) return fail(WR_E_NULL, "bytes is NULL");
   static thread_local Plan plans[WR_MAX_BATCH];
   size_t offs[WR_MAX_BATCH];
-  return batch_plans(items, n, p, plans, offs, bytes, true);
+  return batch_plans(items, n, params, plans, offs, bytes, true);
 }
 
-int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, void* workspace,
-                         size_t workspace_bytes, void* stream) {
+int wr_lk_register_batch_each(const WrLKItem* items, const WrLKParams* params, int32_t n, void* workspace,
+                              size_t workspace_bytes, void* stream) {
   static thread_local Plan plans[WR_MAX_BATCH];
   size_t offs[WR_MAX_BATCH], total = 0;
-  int rc = batch_plans(items, n, p, plans, offs, &total, false);
+  int rc = batch_plans(items, n, params, plans, offs, &total, false);
   if (rc) return rc;
   if (!workspace) return fail(WR_E_NULL, "workspace is NULL");
   if (reinterpret_cast<uintptr_t>(workspace) % 256) return fail(WR_E_WORKSPACE, "workspace must be 256-byte aligned");
@@ -933,16 +975,37 @@ int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, 
   const int dtype = items[0].mov.dtype;
 #define WR_BATCH_DISPATCH(PRECV)                                                                        \
   switch (dtype) {                                                                                      \
-    case WR_U16: return run_batch<uint16_t, PRECV>(plans, offs, items, n, p, workspace, s);             \
-    case WR_U8: return run_batch<uint8_t, PRECV>(plans, offs, items, n, p, workspace, s);               \
-    default: return run_batch<float, PRECV>(plans, offs, items, n, p, workspace, s);                     \
+    case WR_U16: return run_batch<uint16_t, PRECV>(plans, offs, items, n, params, workspace, s);        \
+    case WR_U8: return run_batch<uint8_t, PRECV>(plans, offs, items, n, params, workspace, s);          \
+    default: return run_batch<float, PRECV>(plans, offs, items, n, params, workspace, s);                \
   }
-  switch (p->precision) {
+  switch (params[0].precision) {
     case WR_PREC_F16: WR_BATCH_DISPATCH(WR_PREC_F16)
     case WR_PREC_BF16: WR_BATCH_DISPATCH(WR_PREC_BF16)
     default: WR_BATCH_DISPATCH(WR_PREC_F32)
   }
 #undef WR_BATCH_DISPATCH
+}
+
+// one parameter set for every frame: the per-frame form with n copies
+static int replicate_params(const WrLKParams* p, int32_t n, WrLKParams* out) {
+  if (!p) return fail(WR_E_NULL, "params is NULL");
+  if (n < 1 || n > WR_MAX_BATCH) return fail(WR_E_PARAM, "batch size must be 1..WR_MAX_BATCH");
+  for (int i = 0; i < n; ++i) out[i] = *p;
+  return WR_OK;
+}
+
+int wr_lk_batch_workspace_size(const WrLKItem* items, int32_t n, const WrLKParams* p, size_t* bytes) {
+  WrLKParams ps[WR_MAX_BATCH];
+  int rc = replicate_params(p, n, ps);
+  return rc ? rc : wr_lk_batch_each_workspace_size(items, ps, n, bytes);
+}
+
+int wr_lk_register_batch(const WrLKItem* items, int32_t n, const WrLKParams* p, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  WrLKParams ps[WR_MAX_BATCH];
+  int rc = replicate_params(p, n, ps);
+  return rc ? rc : wr_lk_register_batch_each(items, ps, n, workspace, workspace_bytes, stream);
 }
 
 int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,

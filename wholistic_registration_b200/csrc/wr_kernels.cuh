@@ -1358,32 +1358,35 @@ template <int MODE, int DIFF0, bool MASK, int PREC>
 __global__ void __launch_bounds__(kAccThreads, 4) k_lk_accumulate_batch(const __grid_constant__ BatchIter b) {
   typedef Store<PREC> S;
   extern __shared__ float4 smem4[];
-  const AccSmem sm(smem4, b.item[0].w);   // one patch radius for the batch
-  float4* gsm = sm.gsm;
-  float* it_raw = sm.it_raw;
-  const TileField tf = sm.tf;
-  int* flags = sm.flags;
-  float* red = sm.red;
-  const TileField tf0 = sm.tf0;
-  int* flags0 = sm.flags0;
   float dmax = 0.f;
   int cur = 0;
   for (int k = blockIdx.x; k < b.tile_start[b.n]; k += gridDim.x) {
     int i = cur;
     while (k >= b.tile_start[i + 1]) ++i;
     if (i != cur) {
-      if (DIFF0 != kNoDiff) flush_max(dmax, b.item[cur].st, sm.red);
+      // the start of shared memory is free between tiles (the tail's barrier)
+      if (DIFF0 != kNoDiff) flush_max(dmax, b.item[cur].st, reinterpret_cast<float*>(smem4));
       cur = i;
     }
     const IterArgs& a = b.item[i];
     if (!*(volatile const int*)&a.st->active) continue;
     const int nx = a.mov.nx, ny = a.mov.ny, nz = a.mov.nz;
     const int w = a.w;
+    // frames may differ in patch width: the carve-up follows the tile's frame
+    // (the launch's dynamic shared memory covers the widest)
+    const AccSmem sm(smem4, w);
+    float4* gsm = sm.gsm;
+    float* it_raw = sm.it_raw;
+    const TileField tf = sm.tf;
+    int* flags = sm.flags;
+    float* red = sm.red;
+    const TileField tf0 = sm.tf0;
+    int* flags0 = sm.flags0;
     const int ncx = a.cpv.ncx, ncy = a.cpv.ncy;
     const int tile = tile_of(k - b.tile_start[i], b.order, nz, a.ntx, a.nty);
 #include "wr_acc_tile.inc"
   }
-  if (DIFF0 != kNoDiff) flush_max(dmax, b.item[cur].st, sm.red);
+  if (DIFF0 != kNoDiff) flush_max(dmax, b.item[cur].st, reinterpret_cast<float*>(smem4));
 }
 
 struct BatchDecide {
@@ -1393,13 +1396,17 @@ struct BatchDecide {
   const double* penpart[kMaxBatch];
   long long nblk[kMaxBatch];
   double n_vox[kMaxBatch];
+  double sps[kMaxBatch];        // smoothPenalty x (2r + 1)^2 of each frame
+  double tol[kMaxBatch];
+  int iter[kMaxBatch];
+  int forced[kMaxBatch];
 };
 
 // one block per frame
-__global__ void k_decide_batch(const __grid_constant__ BatchDecide b, double sps, int level, int it, int iter,
-                               double tol, int forced) {
+__global__ void k_decide_batch(const __grid_constant__ BatchDecide b, int level, int it) {
   const int i = blockIdx.x;
-  decide_body(b.st[i], b.errpart[i], b.penpart[i], b.nblk[i], b.n_vox[i], sps, level, it, iter, tol, forced);
+  decide_body(b.st[i], b.errpart[i], b.penpart[i], b.nblk[i], b.n_vox[i], b.sps[i], level, it, b.iter[i], b.tol[i],
+              b.forced[i]);
 }
 
 struct BatchUpdate {
@@ -1408,29 +1415,33 @@ struct BatchUpdate {
   float4* cp[kMaxBatch];
   const float* sums[kMaxBatch];
   long long ncp[kMaxBatch];
+  double sps[kMaxBatch];
+  float sps_f[kMaxBatch];
+  double mov_range[kMaxBatch];
+  double zratio_d[kMaxBatch];   // the level's zRatio of each frame
 };
 
 // blockIdx.y = frame
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads) k_update_batch(const __grid_constant__ BatchUpdate b, double sps,
-                                                          float sps_f, double mov_range, double zratio_d) {
+__global__ void __launch_bounds__(kThreads) k_update_batch(const __grid_constant__ BatchUpdate b) {
   const int f = blockIdx.y;
-  update_body<MIXED>(b.st[f], b.cp[f], b.sums[f], b.ncp[f], blockIdx.x * (long long)blockDim.x + threadIdx.x, sps,
-                     sps_f, mov_range, zratio_d);
+  update_body<MIXED>(b.st[f], b.cp[f], b.sums[f], b.ncp[f], blockIdx.x * (long long)blockDim.x + threadIdx.x, b.sps[f],
+                     b.sps_f[f], b.mov_range[f], b.zratio_d[f]);
 }
 
 struct BatchState {
   int n;
   LKState* st[kMaxBatch];
+  int forced[kMaxBatch];
 };
 
 // one thread per frame
-__global__ void k_post_batch(const __grid_constant__ BatchState b, int level, int forced, int defer) {
-  if (threadIdx.x < b.n) k_post_body(b.st[threadIdx.x], level, forced, defer, kMotionTol);
+__global__ void k_post_batch(const __grid_constant__ BatchState b, int level, int defer) {
+  if (threadIdx.x < b.n) k_post_body(b.st[threadIdx.x], level, b.forced[threadIdx.x], defer, kMotionTol);
 }
 
-__global__ void k_first_post_batch(const __grid_constant__ BatchState b, int level, int forced) {
-  if (threadIdx.x < b.n) k_first_post_body(b.st[threadIdx.x], level, forced, kMotionTol);
+__global__ void k_first_post_batch(const __grid_constant__ BatchState b, int level) {
+  if (threadIdx.x < b.n) k_first_post_body(b.st[threadIdx.x], level, b.forced[threadIdx.x], kMotionTol);
 }
 
 __global__ void k_level_begin(LKState* st, int level, int first) {

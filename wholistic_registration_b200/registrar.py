@@ -121,6 +121,18 @@ class LKRegistrar:
         # launch-shape bits of WrLKParams.flags (tile order, CTAs per SM); results do not depend on them
         self.tune_flags = 0
 
+    def set_params(self, params: LKParams) -> None:
+        """Use other solver parameters from the next call on; the workspace
+        must still suffice (ValueError otherwise), which it does for the same
+        patch radius and number of levels."""
+        cp = params.to_c()
+        nbytes = ctypes.c_size_t(0)
+        _lib.check("wr_lk_workspace_size",
+                   self.lib.wr_lk_workspace_size(*self.shape, ctypes.byref(cp), ctypes.byref(nbytes)))
+        if int(nbytes.value) > self.workspace_bytes:
+            raise ValueError("these parameters need a larger workspace than this registrar holds")
+        self.params, self._cp = params, cp
+
     def autotune(self, dtype=torch.uint16, mask=True, use_cache=True, report=None) -> int:
         """Pick the fused kernel's launch shape for this registrar's shape and
         parameters (``autotune.tune``, cached) and use it from now on."""
