@@ -40,6 +40,12 @@ typedef struct {
 /* Message of the last failed network call on this thread. */
 WR_API const char* wr_net_last_error(void);
 
+/* The convolutions run on the tcgen05 tensor cores with TMEM accumulators and
+   bounded waits: *flag = 1 when a launch on the current device gave up
+   waiting for its tensor-core work since the last call (the flag is then
+   cleared).  Synchronises the device. */
+WR_API int wr_net_tc_error(int* flag);
+
 /* y = act(conv(x) + bias): bf16 output [n][o][cout], or float32 when y32 != NULL. */
 WR_API int wr_net_conv3d_fwd(const WrConvGeom* g, const void* x1, const void* x2, const void* w_bf16,
                              const float* bias, void* y, float* y32, void* stream);

@@ -49,6 +49,9 @@ CASES = [
     (1, (7, 9, 11), 2, 32, 0, 0, 48, 1),
     (2, (6, 10, 12), 1, 32, 16, 1, 16, 1),
     (1, (5, 8, 6), 1, 16, 0, 0, 3, 0),
+    # several 128-row tiles, the widest operands (112 input, 64 output channels)
+    (1, (8, 16, 16), 1, 64, 48, 1, 48, 1),
+    (1, (8, 16, 18), 2, 64, 0, 0, 64, 1),
 ]
 
 
@@ -133,3 +136,7 @@ def test_conv_forward_and_gradients(case):
                     ref_g1[:, z // 2, yy // 2, x // 2] += up_part[:, z, yy, x]
         _close(g2.cpu().numpy(), ref_g2)
         _close(g1.cpu().numpy(), ref_g1)
+    # the tensor-core convolutions finished without a wait running out
+    flag = ctypes.c_int(-1)
+    _l.check("wr_net_tc_error", lib.wr_net_tc_error(ctypes.byref(flag)))
+    assert flag.value == 0

@@ -54,6 +54,7 @@ EXPORTS = (
     "wr_penalty_factor_scratch",
     "wr_resize_table",
     "wr_net_last_error",
+    "wr_net_tc_error",
     "wr_net_conv3d_fwd",
     "wr_net_conv3d_dgrad",
     "wr_net_conv3d_wgrad",

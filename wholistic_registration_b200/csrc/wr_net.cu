@@ -18,10 +18,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 
 #include "wr_b200.h"
 #include "wr_net.h"
+#include "wr_net_tc.cuh"
 
 namespace wrnet {
 
@@ -65,326 +67,9 @@ __device__ __forceinline__ long long vox(int n, int z, int y, int x, int Z, int 
   return (((long long)n * Z + z) * Y + y) * X + x;
 }
 
-// ---------------------------------------------------------------------------
-// forward: CTA = 4 warps x 32 output voxels, all output channels (<= 64)
-// ---------------------------------------------------------------------------
-
 constexpr int kWarps = 4;
-constexpr int kMT = 2;     // m16 tiles per warp
 
-template <int NT>
-__global__ void __launch_bounds__(kWarps * 32) k_conv_fwd(Conv c, const __nv_bfloat16* __restrict__ x1,
-                                                          const __nv_bfloat16* __restrict__ x2,
-                                                          const __nv_bfloat16* __restrict__ w,
-                                                          const float* __restrict__ bias,
-                                                          __nv_bfloat16* __restrict__ y, float* __restrict__ y32) {
-  extern __shared__ __nv_bfloat16 wsm[];   // [cout_p][cin] of the current tap
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
-  const long long base = ((long long)blockIdx.x * kWarps + warp) * (16 * kMT);
-  // the four output rows this thread feeds into A fragments
-  long long row[kMT][2];
-  int rz[kMT][2], ry[kMT][2], rx[kMT][2], rn[kMT][2];
-  bool rv[kMT][2];
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int h = 0; h < 2; ++h) {
-      long long q = base + mt * 16 + g + 8 * h;
-      rv[mt][h] = q < nvox;
-      row[mt][h] = q;
-      long long qq = rv[mt][h] ? q : 0;
-      rx[mt][h] = (int)(qq % c.ox); qq /= c.ox;
-      ry[mt][h] = (int)(qq % c.oy); qq /= c.oy;
-      rz[mt][h] = (int)(qq % c.oz); rn[mt][h] = (int)(qq / c.oz);
-    }
-  float acc[kMT][NT][4];
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int nt = 0; nt < NT; ++nt)
-      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
-  const int chunks = c.cin / 16;
-  for (int tap = 0; tap < 27; ++tap) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < c.cout_p * c.cin / 2; i += blockDim.x)
-      reinterpret_cast<uint32_t*>(wsm)[i] = reinterpret_cast<const uint32_t*>(w + (size_t)tap * c.cout_p * c.cin)[i];
-    __syncthreads();
-    const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
-    // source voxel of each row for this tap (fine grid) and validity
-    long long p2[kMT][2], p1[kMT][2];
-    bool pv[kMT][2];
-    for (int mt = 0; mt < kMT; ++mt)
-      for (int h = 0; h < 2; ++h) {
-        const int z = c.stride * rz[mt][h] + kz, yy = c.stride * ry[mt][h] + ky, xx = c.stride * rx[mt][h] + kx;
-        pv[mt][h] = rv[mt][h] && z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix;
-        p2[mt][h] = pv[mt][h] ? vox(rn[mt][h], z, yy, xx, c.iz, c.iy, c.ix) : 0;
-        const int hz = (c.iz + 1) / 2, hy = (c.iy + 1) / 2, hx = (c.ix + 1) / 2;
-        p1[mt][h] = pv[mt][h] ? (c.up1 ? vox(rn[mt][h], z >> 1, yy >> 1, xx >> 1, hz, hy, hx) : p2[mt][h]) : 0;
-      }
-    for (int ch = 0; ch < chunks; ++ch) {
-      const int c0 = ch * 16;
-      const bool from1 = c0 < c.c1;
-      const __nv_bfloat16* src = from1 ? x1 : x2;
-      const int cs = from1 ? c.c1 : c.c2;
-      const int cc = from1 ? c0 : c0 - c.c1;
-      uint32_t a[kMT][4];
-      for (int mt = 0; mt < kMT; ++mt)
-        for (int h = 0; h < 2; ++h) {
-          uint32_t lo = 0u, hi = 0u;
-          if (pv[mt][h]) {
-            const long long pix = from1 ? p1[mt][h] : p2[mt][h];
-            const uint32_t* sp = reinterpret_cast<const uint32_t*>(src + pix * cs + cc);
-            lo = __ldg(sp + t);
-            hi = __ldg(sp + 4 + t);
-          }
-          a[mt][h] = lo;       // a0 (row g) / a1 (row g+8)
-          a[mt][2 + h] = hi;   // a2 / a3 (channels +8)
-        }
-      for (int nt = 0; nt < NT; ++nt) {
-        const uint32_t* wp = reinterpret_cast<const uint32_t*>(wsm + (size_t)(nt * 8 + g) * c.cin + c0);
-        const uint32_t b0 = wp[t], b1 = wp[4 + t];
-        for (int mt = 0; mt < kMT; ++mt) mma_bf16(acc[mt][nt], a[mt], b0, b1);
-      }
-    }
-  }
-  // epilogue: bias, activation, store
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int h = 0; h < 2; ++h) {
-      if (!rv[mt][h]) continue;
-      const long long q = row[mt][h];
-      for (int nt = 0; nt < NT; ++nt) {
-        const int co = nt * 8 + 2 * t;
-        float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-        if (co < c.cout) v0 += bias[co];
-        if (co + 1 < c.cout) v1 += bias[co + 1];
-        if (c.act) {
-          v0 = v0 > 0.f ? v0 : 0.1f * v0;
-          v1 = v1 > 0.f ? v1 : 0.1f * v1;
-        }
-        if (y32) {
-          if (co < c.cout) y32[q * c.cout + co] = v0;
-          if (co + 1 < c.cout) y32[q * c.cout + co + 1] = v1;
-        } else if (co < c.cout) {
-          *reinterpret_cast<__nv_bfloat162*>(y + q * c.cout + co) = __floats2bfloat162_rn(v0, v1);
-        }
-      }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// forward, stride 1, shared-memory tiled: the CTA's 4x4x8 output voxels read
-// a 6x6x10 input tile staged once in shared memory (both sources, source 1
-// replicated onto the fine grid when it is upsampled); A and B fragments come
-// from ldmatrix.  Voxel rows are padded to an odd number of 16-byte chunks so
-// the 8 rows of each ldmatrix land in distinct banks.
-// ---------------------------------------------------------------------------
-
-constexpr int kTZ = 4, kTY = 4, kTX = 8;                 // output tile (128 voxels, one z plane per warp)
-constexpr int kHZ = kTZ + 2, kHY = kTY + 2, kHX = kTX + 2;
-constexpr int kHalo = kHZ * kHY * kHX;                   // 360 input voxels
-
-__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
-  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
-}
-
-__host__ __device__ inline int tile_row_elems(int cin) { return cin + 8; }
-
-template <int NT>
-__global__ void __launch_bounds__(kWarps * 32) k_conv_fwd_tiled(Conv c, const __nv_bfloat16* __restrict__ x1,
-                                                                const __nv_bfloat16* __restrict__ x2,
-                                                                const __nv_bfloat16* __restrict__ w,
-                                                                const float* __restrict__ bias,
-                                                                __nv_bfloat16* __restrict__ y, float* __restrict__ y32) {
-  extern __shared__ __align__(16) __nv_bfloat16 sm[];
-  const int rs = tile_row_elems(c.cin);               // elements per voxel row
-  __nv_bfloat16* tile = sm;                            // [kHalo][rs]
-  __nv_bfloat16* wsm = sm + kHalo * rs;                // [cout_p][rs]
-  const int tiles_x = (c.ox + kTX - 1) / kTX, tiles_y = (c.oy + kTY - 1) / kTY, tiles_z = (c.oz + kTZ - 1) / kTZ;
-  int b = blockIdx.x;
-  const int bx = b % tiles_x; b /= tiles_x;
-  const int by = b % tiles_y; b /= tiles_y;
-  const int bz = b % tiles_z;
-  const int n = b / tiles_z;
-  const int ox0 = bx * kTX, oy0 = by * kTY, oz0 = bz * kTZ;
-  const int hz = (c.iz + 1) / 2, hy = (c.iy + 1) / 2, hx = (c.ix + 1) / 2;
-  // stage the input tile: 16-byte chunks of every halo voxel
-  const int cpr = c.cin / 8;
-  for (int i = threadIdx.x; i < kHalo * cpr; i += blockDim.x) {
-    const int v = i / cpr, ch = i - v * cpr;
-    const int lx = v % kHX, ly = (v / kHX) % kHY, lz = v / (kHX * kHY);
-    const int z = oz0 - 1 + lz, yy = oy0 - 1 + ly, xx = ox0 - 1 + lx;
-    uint4 val = make_uint4(0u, 0u, 0u, 0u);
-    if (z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix) {
-      const int c0 = ch * 8;
-      if (c0 < c.c1) {
-        const long long p = c.up1 ? vox(n, z >> 1, yy >> 1, xx >> 1, hz, hy, hx) : vox(n, z, yy, xx, c.iz, c.iy, c.ix);
-        val = __ldg(reinterpret_cast<const uint4*>(x1 + p * c.c1 + c0));
-      } else {
-        val = __ldg(reinterpret_cast<const uint4*>(x2 + vox(n, z, yy, xx, c.iz, c.iy, c.ix) * c.c2 + (c0 - c.c1)));
-      }
-    }
-    *reinterpret_cast<uint4*>(tile + v * rs + ch * 8) = val;
-  }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  float acc[2][NT][4];
-  for (int mt = 0; mt < 2; ++mt)
-    for (int nt = 0; nt < NT; ++nt)
-      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
-  // ldmatrix row this lane addresses: matrix j = lane / 8, row r = lane % 8
-  const int j = lane >> 3, r = lane & 7;
-  const int chunks = c.cin / 16;
-  for (int tap = 0; tap < 27; ++tap) {
-    __syncthreads();
-    const int cp = c.cin / 8;
-    for (int i = threadIdx.x; i < c.cout_p * cp; i += blockDim.x) {
-      const int co = i / cp, ch = i - co * cp;
-      *reinterpret_cast<uint4*>(wsm + co * rs + ch * 8) =
-          __ldg(reinterpret_cast<const uint4*>(w + ((size_t)tap * c.cout_p + co) * c.cin + ch * 8));
-    }
-    __syncthreads();
-    const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
-    // output voxel of this lane's ldmatrix row in m-tile mt: (warp, ty, tx)
-    const __nv_bfloat16* arow[2];
-    for (int mt = 0; mt < 2; ++mt) {
-      const int m = mt * 16 + r + 8 * (j & 1);
-      const int ty = m >> 3, tx = m & 7;
-      arow[mt] = tile + (((warp + kz) * kHY + ty + ky) * kHX + tx + kx) * rs + 8 * (j >> 1);
-    }
-    for (int ch = 0; ch < chunks; ++ch) {
-      uint32_t a[2][4];
-      ldsm_x4(a[0], arow[0] + ch * 16);
-      ldsm_x4(a[1], arow[1] + ch * 16);
-#pragma unroll
-      for (int np = 0; np < NT / 2; ++np) {
-        // two n8 tiles: matrices (co 0-7, k lo), (co 0-7, k hi), (co 8-15, k lo), (co 8-15, k hi)
-        uint32_t bm[4];
-        ldsm_x4(bm, wsm + (np * 16 + r + 8 * (j >> 1)) * rs + ch * 16 + 8 * (j & 1));
-        mma_bf16(acc[0][2 * np], a[0], bm[0], bm[1]);
-        mma_bf16(acc[1][2 * np], a[1], bm[0], bm[1]);
-        mma_bf16(acc[0][2 * np + 1], a[0], bm[2], bm[3]);
-        mma_bf16(acc[1][2 * np + 1], a[1], bm[2], bm[3]);
-      }
-    }
-  }
-  for (int mt = 0; mt < 2; ++mt)
-    for (int h = 0; h < 2; ++h) {
-      const int m = mt * 16 + g + 8 * h;
-      const int oz = oz0 + warp, oy = oy0 + (m >> 3), ox = ox0 + (m & 7);
-      if (oz >= c.oz || oy >= c.oy || ox >= c.ox) continue;
-      const long long q = vox(n, oz, oy, ox, c.oz, c.oy, c.ox);
-      for (int nt = 0; nt < NT; ++nt) {
-        const int co = nt * 8 + 2 * t;
-        float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-        if (co < c.cout) v0 += bias[co];
-        if (co + 1 < c.cout) v1 += bias[co + 1];
-        if (c.act) {
-          v0 = v0 > 0.f ? v0 : 0.1f * v0;
-          v1 = v1 > 0.f ? v1 : 0.1f * v1;
-        }
-        if (y32) {
-          if (co < c.cout) y32[q * c.cout + co] = v0;
-          if (co + 1 < c.cout) y32[q * c.cout + co + 1] = v1;
-        } else if (co < c.cout) {
-          *reinterpret_cast<__nv_bfloat162*>(y + q * c.cout + co) = __floats2bfloat162_rn(v0, v1);
-        }
-      }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// data gradient: GEMM over input voxels p (fine grid of the virtual input),
-// k = (tap, co); weights transposed to wt[tap][ci][co_p]
-// ---------------------------------------------------------------------------
-
-template <int NT>
-__global__ void __launch_bounds__(kWarps * 32) k_conv_dgrad(Conv c, const __nv_bfloat16* __restrict__ dy,
-                                                            const __nv_bfloat16* __restrict__ wt,
-                                                            float* __restrict__ dx) {
-  extern __shared__ __nv_bfloat16 wsm[];   // [cin][cout_p] of the current tap
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
-  const long long base = ((long long)blockIdx.x * kWarps + warp) * (16 * kMT);
-  const int ncol = c.cin;   // output columns of this GEMM
-  const int col0 = blockIdx.y * NT * 8;
-  long long row[kMT][2];
-  int rz[kMT][2], ry[kMT][2], rx[kMT][2], rn[kMT][2];
-  bool rv[kMT][2];
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int h = 0; h < 2; ++h) {
-      long long p = base + mt * 16 + g + 8 * h;
-      rv[mt][h] = p < nvox;
-      row[mt][h] = p;
-      long long pp = rv[mt][h] ? p : 0;
-      rx[mt][h] = (int)(pp % c.ix); pp /= c.ix;
-      ry[mt][h] = (int)(pp % c.iy); pp /= c.iy;
-      rz[mt][h] = (int)(pp % c.iz); rn[mt][h] = (int)(pp / c.iz);
-    }
-  float acc[kMT][NT][4];
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int nt = 0; nt < NT; ++nt)
-      for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
-  const int chunks = c.cout_p / 16;
-  for (int tap = 0; tap < 27; ++tap) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < c.cin * c.cout_p / 2; i += blockDim.x)
-      reinterpret_cast<uint32_t*>(wsm)[i] = reinterpret_cast<const uint32_t*>(wt + (size_t)tap * c.cin * c.cout_p)[i];
-    __syncthreads();
-    const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
-    long long q[kMT][2];
-    bool qv[kMT][2];
-    for (int mt = 0; mt < kMT; ++mt)
-      for (int h = 0; h < 2; ++h) {
-        // output voxel reading this input voxel through the tap: p = s*q + k
-        const int az = rz[mt][h] - kz, ay = ry[mt][h] - ky, ax = rx[mt][h] - kx;
-        bool ok = rv[mt][h] && az >= 0 && ay >= 0 && ax >= 0;
-        int oz = az, oy = ay, ox = ax;
-        if (c.stride == 2) {
-          ok = ok && !(az & 1) && !(ay & 1) && !(ax & 1);
-          oz = az >> 1; oy = ay >> 1; ox = ax >> 1;
-        }
-        ok = ok && oz < c.oz && oy < c.oy && ox < c.ox;
-        qv[mt][h] = ok;
-        q[mt][h] = ok ? vox(rn[mt][h], oz, oy, ox, c.oz, c.oy, c.ox) : 0;
-      }
-    for (int ch = 0; ch < chunks; ++ch) {
-      const int c0 = ch * 16;
-      uint32_t a[kMT][4];
-      for (int mt = 0; mt < kMT; ++mt)
-        for (int h = 0; h < 2; ++h) {
-          uint32_t lo = 0u, hi = 0u;
-          if (qv[mt][h]) {
-            const uint32_t* sp = reinterpret_cast<const uint32_t*>(dy + q[mt][h] * c.cout_p + c0);
-            lo = __ldg(sp + t);
-            hi = __ldg(sp + 4 + t);
-          }
-          a[mt][h] = lo;
-          a[mt][2 + h] = hi;
-        }
-      for (int nt = 0; nt < NT; ++nt) {
-        const int ci = col0 + nt * 8 + g;
-        uint32_t b0 = 0u, b1 = 0u;
-        if (ci < ncol) {
-          const uint32_t* wp = reinterpret_cast<const uint32_t*>(wsm + (size_t)ci * c.cout_p + c0);
-          b0 = wp[t];
-          b1 = wp[4 + t];
-        }
-        for (int mt = 0; mt < kMT; ++mt) mma_bf16(acc[mt][nt], a[mt], b0, b1);
-      }
-    }
-  }
-  for (int mt = 0; mt < kMT; ++mt)
-    for (int h = 0; h < 2; ++h) {
-      if (!rv[mt][h]) continue;
-      const long long p = row[mt][h];
-      for (int nt = 0; nt < NT; ++nt) {
-        const int ci = col0 + nt * 8 + 2 * t;
-        if (ci < ncol) dx[p * ncol + ci] = acc[mt][nt][2 * h];
-        if (ci + 1 < ncol) dx[p * ncol + ci + 1] = acc[mt][nt][2 * h + 1];
-      }
-    }
-}
+#include "wr_net_tc_conv.inc"
 
 // ---------------------------------------------------------------------------
 // weight gradient: per (tap, chunk of output voxels) a [cout_p x cin] partial,
@@ -759,21 +444,34 @@ static int check(const WrConvGeom* g, Conv* c) {
   return WR_OK;
 }
 
-template <int NT>
-static void launch_fwd(const Conv& c, const void* x1, const void* x2, const void* w, const float* b, void* y, float* y32,
-                       cudaStream_t s) {
-  if (c.stride == 1) {
-    const int tiles = ((c.ox + kTX - 1) / kTX) * ((c.oy + kTY - 1) / kTY) * ((c.oz + kTZ - 1) / kTZ) * c.n;
-    const size_t smem = (size_t)(kHalo + c.cout_p) * tile_row_elems(c.cin) * 2;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_conv_fwd_tiled<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_conv_fwd_tiled<NT><<<tiles, kWarps * 32, smem, s>>>(c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2,
-                                                          (const __nv_bfloat16*)w, b, (__nv_bfloat16*)y, y32);
-    return;
+// flag the tcgen05 kernels set when a wait runs out (one per device)
+static __device__ int g_tc_err;
+
+static int* tc_err_ptr() {
+  static std::mutex mu;
+  static int* ptr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_tc_err) != cudaSuccess) return nullptr;
+    ptr[dev] = static_cast<int*>(p);
   }
-  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
-  const int blocks = (int)((nvox + kWarps * 16 * kMT - 1) / (kWarps * 16 * kMT));
-  k_conv_fwd<NT><<<blocks, kWarps * 32, (size_t)c.cout_p * c.cin * 2, s>>>(
-      c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2, (const __nv_bfloat16*)w, b, (__nv_bfloat16*)y, y32);
+  return ptr[dev];
+}
+
+template <int MODE, int NT>
+static int launch_tc(const Conv& c, long long rows, int kc, const void* x1, const void* x2, const void* w,
+                     const float* b, void* y, float* y32, float* dx, cudaStream_t s) {
+  int* err = tc_err_ptr();
+  if (!err) return fail(WR_E_PARAM, "no CUDA device for the tensor-core convolution");
+  const size_t smem = tc_smem_bytes(kc, 16 * NT);
+  cudaFuncSetAttribute(k_conv_tc<MODE, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned blocks = (unsigned)((rows + kTcRows - 1) / kTcRows);
+  k_conv_tc<MODE, NT><<<blocks, kTcThreads, smem, s>>>(c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2,
+                                                       (const __nv_bfloat16*)w, b, (__nv_bfloat16*)y, y32, dx, err);
+  return WR_OK;
 }
 
 }  // namespace wrnet
@@ -784,6 +482,18 @@ extern "C" {
 
 const char* wr_net_last_error(void) { return g_err.c_str(); }
 
+int wr_net_tc_error(int* flag) {
+  if (!flag) return fail(WR_E_NULL, "flag is NULL");
+  int* p = tc_err_ptr();
+  if (!p) return fail(WR_E_PARAM, "no CUDA device");
+  int v = 0;
+  cudaError_t e = cudaMemcpy(&v, p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(int));
+  if (e != cudaSuccess) return cuda_status("wr_net_tc_error");
+  *flag = v;
+  return WR_OK;
+}
+
 int wr_net_conv3d_fwd(const WrConvGeom* geom, const void* x1, const void* x2, const void* w, const float* bias,
                       void* y, float* y32, void* stream) {
   Conv c;
@@ -791,12 +501,14 @@ int wr_net_conv3d_fwd(const WrConvGeom* geom, const void* x1, const void* x2, co
   if (rc) return rc;
   if (!x1 || !w || !bias || (!y && !y32) || (c.c2 && !x2)) return fail(WR_E_NULL, "a required pointer is NULL");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  switch (c.cout_p / 8) {
-    case 2: launch_fwd<2>(c, x1, x2, w, bias, y, y32, s); break;
-    case 4: launch_fwd<4>(c, x1, x2, w, bias, y, y32, s); break;
-    case 6: launch_fwd<6>(c, x1, x2, w, bias, y, y32, s); break;
-    default: launch_fwd<8>(c, x1, x2, w, bias, y, y32, s); break;
+  const long long rows = (long long)c.n * c.oz * c.oy * c.ox;
+  switch (c.cout_p / 16) {
+    case 1: rc = launch_tc<kTcFwd, 1>(c, rows, c.cin, x1, x2, w, bias, y, y32, nullptr, s); break;
+    case 2: rc = launch_tc<kTcFwd, 2>(c, rows, c.cin, x1, x2, w, bias, y, y32, nullptr, s); break;
+    case 3: rc = launch_tc<kTcFwd, 3>(c, rows, c.cin, x1, x2, w, bias, y, y32, nullptr, s); break;
+    default: rc = launch_tc<kTcFwd, 4>(c, rows, c.cin, x1, x2, w, bias, y, y32, nullptr, s); break;
   }
+  if (rc) return rc;
   return cuda_status("wr_net_conv3d_fwd");
 }
 
@@ -806,11 +518,17 @@ int wr_net_conv3d_dgrad(const WrConvGeom* geom, const void* dy, const void* wt, 
   if (rc) return rc;
   if (!dy || !wt || !dxv) return fail(WR_E_NULL, "a required pointer is NULL");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const long long nvox = (long long)c.n * c.iz * c.iy * c.ix;
-  constexpr int NT = 4;   // 32 input channels per CTA column
-  dim3 grid((unsigned)((nvox + kWarps * 16 * kMT - 1) / (kWarps * 16 * kMT)), (unsigned)((c.cin + NT * 8 - 1) / (NT * 8)));
-  k_conv_dgrad<NT><<<grid, kWarps * 32, (size_t)c.cin * c.cout_p * 2, s>>>(c, (const __nv_bfloat16*)dy,
-                                                                           (const __nv_bfloat16*)wt, dxv);
+  const long long rows = (long long)c.n * c.iz * c.iy * c.ix;
+  switch (c.cin / 16) {
+    case 1: rc = launch_tc<kTcDgrad, 1>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    case 2: rc = launch_tc<kTcDgrad, 2>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    case 3: rc = launch_tc<kTcDgrad, 3>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    case 4: rc = launch_tc<kTcDgrad, 4>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    case 5: rc = launch_tc<kTcDgrad, 5>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    case 6: rc = launch_tc<kTcDgrad, 6>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+    default: rc = launch_tc<kTcDgrad, 7>(c, rows, c.cout_p, dy, nullptr, wt, nullptr, nullptr, nullptr, dxv, s); break;
+  }
+  if (rc) return rc;
   return cuda_status("wr_net_conv3d_dgrad");
 }
 
