@@ -209,7 +209,7 @@ def test_register_and_warp_in_one_call_matches_two_calls(shape, layer):
     torch.testing.assert_close(warped_fused, warped, rtol=0, atol=0)
 
 
-@pytest.mark.parametrize("precision,rms_tol", [(1, 0.02), (2, 0.1)])
+@pytest.mark.parametrize("precision,rms_tol", [(1, 2.5e-3), (2, 1.5e-2)])   # about twice the B200 errors
 def test_mixed_precision_error_against_fp64_oracle(precision, rms_tol):
     """Levels and gradients stored in float16 (1) or bfloat16 (2), sums and
     solves in float32: flow error against the float64 oracle of the method."""

@@ -115,6 +115,8 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
   P.r = p->r; P.w = 2 * p->r + 1; P.iter = p->iter;
   P.has_mref = has_mref; P.has_mmov = has_mmov; P.has_init = has_init;
   P.dense_all = p->iter == 1;
+  for (int l = 0; l < P.levels; ++l) P.dense_out[l] = P.dense_all || p->forced_updates[l] == 0;
+  for (int l = 0; l < P.levels; ++l) P.dense_in[l] = P.dense_out[l] || (l + 1 < P.levels && P.dense_out[l + 1]);
   P.precision = p->precision;
   Alloc A;
   size_t tmp_a = 0, tmp_b = 0;
@@ -154,7 +156,7 @@ int make_plan(int nz, int ny, int nx, const WrLKParams* p, bool has_mref, bool h
     L.sums = A.take((size_t)L.ncp * 12 * 4);
     L.errpart = A.take((size_t)L.nblk * 8);
     L.penpart = A.take((size_t)L.nblk * 8);
-    L.dense = (P.dense_all || l == P.levels - 1) ? A.take((size_t)L.n * 16) : 0;
+    L.dense = (P.dense_in[l] || l == P.levels - 1) ? A.take((size_t)L.n * 16) : 0;
     L.tx_w = A.take((size_t)L.nx * L.tx_taps * 8);
     L.tx_i = A.take((size_t)L.nx * L.tx_taps * 4);
     L.ty_w = A.take((size_t)L.ny * L.ty_taps * 8);
@@ -388,7 +390,7 @@ static FieldSrc field_src(const Plan& P, int l, int mode, void* ws) {
   if (l + 1 < P.levels) {
     const LevelPlan& C = P.lv[l + 1];
     f.up.src = cp_view(P, C, ws);
-    f.up.src_dense = P.dense_all ? at_off<float4>(ws, C.dense) : nullptr;
+    f.up.src_dense = P.dense_out[l + 1] ? at_off<float4>(ws, C.dense) : nullptr;
     f.up.src_nx = C.nx;
     f.up.src_ny = C.ny;
     f.up.wx = at_off<float>(ws, L.ux_w);
@@ -541,7 +543,7 @@ static int count_launches(const Plan& P, bool has_mmov, bool has_mref, bool has_
   if (has_init) n += (P.levels == 1 ? 3 : 6) + 1;
   for (int l = P.levels - 1; l >= 0; --l) {
     n += 1;                                                    // level begin
-    if (P.dense_all && !(l == P.levels - 1 && has_init)) n += 1; // dense field
+    if (P.dense_in[l] && !(l == P.levels - 1 && has_init)) n += 1; // dense field
     n += 1;                                                    // cp init
     n += 4 * P.iter + (P.iter >= 2 ? 1 : 0);                   // iterations + first-update check
   }
@@ -577,8 +579,9 @@ static IterArgs begin_level(const Plan& P, int l, void* ws, bool has_init, bool 
   const bool coarsest = l == P.levels - 1;
   k_level_begin<<<1, 1, 0, s>>>(st, l, coarsest ? 1 : 0);
   int m0 = coarsest ? (has_init ? FIELD_DENSE : FIELD_ZERO) : FIELD_UP;
-  if (P.dense_all) {
-    // no update can happen at any level: carry dense fields down the pyramid
+  if (P.dense_in[l] && !(coarsest && has_init)) {
+    // a level without update keeps its dense initial field (and the next
+    // finer level starts from that field, materialised)
     FieldSrc f = field_src(P, l, m0, ws);
     float4* dense = at_off<float4>(ws, L.dense);
     const int g = row_grid((long long)L.nz * L.ny);
@@ -621,7 +624,7 @@ static void finish_frame(const Plan& P, void* ws, const T* mov, float* out, floa
                          cudaStream_t s) {
   const LevelPlan& L0 = P.lv[0];
   const int g0 = row_grid((long long)L0.nz * L0.ny);
-  const int mode_out = P.dense_all ? FIELD_DENSE : FIELD_CP;
+  const int mode_out = P.dense_out[0] ? FIELD_DENSE : FIELD_CP;
   const FieldSrc f = field_src(P, 0, mode_out, ws);
   if (warped) {
     // the full-resolution motion and mov warped by it, in one pass

@@ -107,6 +107,12 @@ template <> struct Store<WR_PREC_BF16> {
   static __device__ __forceinline__ V1 pack1(float v) { return __float2bfloat16_rn(v); }
 };
 
+// float16 storage holds half of each value: a half2 result as float2, doubled
+__device__ __forceinline__ float2 half2_scaled(__half2 h) {
+  const float2 f = __half22float2(h);
+  return make_float2(2.f * f.x, 2.f * f.y);
+}
+
 // ---------------------------------------------------------------------------
 // resize tables (utils/imresize.py:60-82)
 // ---------------------------------------------------------------------------

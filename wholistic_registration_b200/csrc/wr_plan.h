@@ -54,6 +54,11 @@ struct Plan {
   int levels;          // layer + 1, index = layer
   int r, w, iter;
   bool has_mref, has_mmov, has_init, dense_all;
+  // dense_out[l]: level l makes no update (iter == 1, or a replay of zero
+  // updates), so its field stays the dense initial field; dense_in[l]: level l
+  // starts from a dense field in its own buffer (it is dense_out, or the
+  // coarser level is, whose dense field the up-sampling must read)
+  bool dense_out[WR_MAX_LEVELS], dense_in[WR_MAX_LEVELS];
   int precision;
   LevelPlan lv[WR_MAX_LEVELS];
   size_t tmp_a, tmp_a_bytes, tmp_b, tmp_b_bytes;
