@@ -388,7 +388,116 @@ class WarmStartRegistrar:
         return motion
 
 
+SWEEP_REFINE = ((0, 2), (0, 4), (0, 10), (1, 2), (1, 4), (1, 6), (2, 4), (2, 6), (2, 10), (3, 4))
+SWEEP_STARTS = ("zero", "network", "truth", "plain")
+
+
+def sweep(shape=(128, 1024, 1024), frames=3, refine=SWEEP_REFINE, starts=SWEEP_STARTS, net=None, seed=500,
+          precision=_lib.WR_PREC_F32, device=None):
+    """What a warm start can buy: short refinements (levels ``layer`` .. 0,
+    ``iter`` iterations) started from the zero field, the network's
+    prediction, the true synthetic deformation (the best any predictor could
+    give) and the plain pyramid's own result, against the plain pyramid
+    (layer 3, r 16, iter 10) on config-1-like frames (20k blobs per
+    128 x 1024 x 1024, fields up to 8 / 8 / 3 voxels, 70 % ellipsoid mask).
+
+    Returns (rows, plain_ms): per (start, layer, iter) the flow RMS from the
+    plain field over all voxels and inside the mask, its max, and the
+    milliseconds per frame (CUDA events; the network's prediction included),
+    and the plain pyramid's milliseconds per frame."""
+    from . import penalty_factor, synthetic
+
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(seed)
+    blobs = max(200, int(20000 * np.prod(shape) / (128 * 1024 * 1024)))
+    clean = synthetic.render_blobs(shape, blobs, rng, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    tmpl_f = torch.poisson(clean, generator=gen)
+    del clean
+    tmpl = tmpl_f.clamp(0, 65535).round().to(torch.int32).to(torch.uint16).contiguous()
+    excl = (~synthetic.ellipsoid_inclusion(shape, 0.7, device=device)).to(torch.uint8).contiguous()
+    inside = excl == 0
+    pen = 0.08 * float(penalty_factor(tmpl, excl))
+    movs, truths = [], []
+    for t in range(frames):
+        _, mov, field = synthetic.make_pair(shape, seed + 1 + t, max_disp=(8.0, 8.0, 3.0), device=device,
+                                            template=tmpl_f)
+        movs.append(mov.contiguous())
+        truths.append(field.contiguous())
+    del tmpl_f
+    if net is None and "network" in starts:
+        net = WarmStartNet(device)
+        net.load()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    base = dict(r=16, zRatio=1.0, movRange=5.0, smoothPenalty=pen, tol=1e-3)
+    plain = LKRegistrar(shape, LKParams(layer=3, iter=10, precision=_lib.WR_PREC_F32, **base), device)
+    plain.register(movs[0], tmpl, excl, excl)                       # warm-up
+    plain_m, plain_ms = [], []
+    for mov in movs:
+        m, ms = timed(lambda: plain.register(mov, tmpl, excl, excl, reuse_reference=True).clone())
+        plain_m.append(m)
+        plain_ms.append(ms)
+    del plain
+    torch.cuda.empty_cache()
+    init = torch.empty(shape + (3,), dtype=torch.float32, device=device)
+    rows = []
+    for layer, iters in refine:
+        reg = LKRegistrar(shape, LKParams(layer=layer, iter=iters, precision=precision, **base), device)
+        reg.register(movs[0], tmpl, excl, excl, motion_init=plain_m[0])   # warm-up, builds the template levels
+        for start in starts:
+            rms, rms_in, mx, ms = [], [], [], []
+            for k, mov in enumerate(movs):
+                def run():
+                    if start == "network":
+                        net.predict(tmpl, mov, out=init)
+                    elif start == "truth":
+                        init.copy_(truths[k])
+                    elif start == "plain":
+                        init.copy_(plain_m[k])
+                    else:
+                        init.zero_()
+                    return reg.register(mov, tmpl, excl, excl, motion_init=init, reuse_reference=True)
+                m, t_ms = timed(run)
+                d = (m - plain_m[k]).float()
+                rms.append(float(d.square().mean().sqrt()))
+                rms_in.append(float(d[inside].square().mean().sqrt()))
+                mx.append(float(d.abs().max()))
+                ms.append(t_ms)
+            rows.append({"start": start, "layer": layer, "iter": iters, "rms": float(np.mean(rms)),
+                         "rms_inside": float(np.mean(rms_in)), "max": float(np.max(mx)),
+                         "ms_per_frame": float(np.median(ms))})
+        del reg
+        torch.cuda.empty_cache()
+    return rows, float(np.median(plain_ms))
+
+
 def main(argv=None):
+    import argparse
+    import sys
+
+    argv = sys.argv[1:] if argv is None else argv
+    if argv[:1] == ["sweep"]:
+        ap = argparse.ArgumentParser(description="what a warm start can buy (see sweep())")
+        ap.add_argument("--shape", default="128x1024x1024")
+        ap.add_argument("--frames", type=int, default=3)
+        args = ap.parse_args(argv[1:])
+        shape = tuple(int(v) for v in args.shape.split("x"))
+        rows, plain_ms = sweep(shape, args.frames)
+        print(f"plain pyramid (layer 3, 10 iterations): {plain_ms:.2f} ms per frame")
+        print("start     layer iter   RMS all  RMS mask      max   ms/frame  speed-up")
+        for r in rows:
+            print(f"{r['start']:8s}  {r['layer']:5d} {r['iter']:4d}  {r['rms']:8.4f}  {r['rms_inside']:8.4f}  "
+                  f"{r['max']:7.3f}  {r['ms_per_frame']:9.2f}  {plain_ms / r['ms_per_frame']:8.2f}")
+        return
     import argparse
 
     ap = argparse.ArgumentParser(description="train the warm-start network on synthetic pairs")
