@@ -5,8 +5,8 @@
 // warm-start channel, option["motion"] (utils/calFlow3d_Wei_v1.py:362-377).
 //
 // Tensors are channels-last bfloat16: [n][z][y][x][c], channel counts padded
-// to multiples of 16.  A convolution is an implicit GEMM on BF16 tensor cores
-// (mma.sync m16n8k16, float32 accumulate):
+// to multiples of 16.  A convolution is an implicit GEMM on the tcgen05 BF16
+// tensor cores, float32 accumulators in tensor memory (wr_net_tc_conv.inc):
 //   forward  y[q][co] = act(b[co] + sum_{tap,ci} x[p(q,tap)][ci] w[tap][co][ci])
 //   data     dx[p][ci] = sum_{tap,co} dy[q(p,tap)][co] w[tap][co][ci]
 //   weights  dw[tap][co][ci] = sum_q dy[q][co] x[p(q,tap)][ci]
@@ -41,13 +41,6 @@ static int cuda_status(const char* where) {
   return -(int)e;
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 
 // Geometry of one convolution (all extents of the output / input grids).
 struct Conv {
@@ -67,113 +60,8 @@ __device__ __forceinline__ long long vox(int n, int z, int y, int x, int Z, int 
   return (((long long)n * Z + z) * Y + y) * X + x;
 }
 
-constexpr int kWarps = 4;
-
 #include "wr_net_tc_conv.inc"
 
-// ---------------------------------------------------------------------------
-// weight gradient: per (tap, chunk of output voxels) a [cout_p x cin] partial,
-// accumulated into float32 dw with atomics.  Operands are staged in shared
-// memory transposed so that the reduction index (voxel) is contiguous.
-// ---------------------------------------------------------------------------
-
-constexpr int kWgVox = 32;        // voxels per staged chunk (two k16 steps)
-constexpr int kWgChunks = 16;     // chunks per CTA
-
-__global__ void __launch_bounds__(kWarps * 32) k_conv_wgrad(Conv c, const __nv_bfloat16* __restrict__ x1,
-                                                            const __nv_bfloat16* __restrict__ x2,
-                                                            const __nv_bfloat16* __restrict__ dy,
-                                                            float* __restrict__ dw, float* __restrict__ db) {
-  extern __shared__ __nv_bfloat16 sm[];
-  const int cop = c.cout_p, cin = c.cin;
-  __nv_bfloat16* sdy = sm;                          // [cop][kWgVox]
-  __nv_bfloat16* sx = sm + cop * kWgVox;            // [cin][kWgVox]
-  const int tap = blockIdx.y;
-  const int kz = tap / 9 - 1, ky = (tap / 3) % 3 - 1, kx = tap % 3 - 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
-  // output tiles: (cop/16) m-tiles x (cin/8) n-tiles, distributed over warps
-  const int mtiles = cop / 16, ntiles = cin / 8, tiles = mtiles * ntiles;
-  constexpr int kMaxTiles = 4 * 14 / kWarps + 1;   // cop <= 64, cin <= 112
-  float acc[kMaxTiles][4];
-  for (int i = 0; i < kMaxTiles; ++i)
-    for (int k = 0; k < 4; ++k) acc[i][k] = 0.f;
-  float bsum = 0.f;
-  for (int chunk = 0; chunk < kWgChunks; ++chunk) {
-    const long long q0 = ((long long)blockIdx.x * kWgChunks + chunk) * kWgVox;
-    if (q0 >= nvox) break;
-    __syncthreads();
-    // stage dy (transposed) and the tap-shifted input (transposed)
-    for (int i = threadIdx.x; i < kWgVox * cop; i += blockDim.x) {
-      const int v = i / cop, co = i - v * cop;
-      const long long q = q0 + v;
-      sdy[co * kWgVox + v] = q < nvox ? dy[q * cop + co] : __float2bfloat16(0.f);
-    }
-    for (int i = threadIdx.x; i < kWgVox * cin; i += blockDim.x) {
-      const int v = i / cin, ci = i - v * cin;
-      const long long q = q0 + v;
-      __nv_bfloat16 val = __float2bfloat16(0.f);
-      if (q < nvox) {
-        long long qq = q;
-        const int ox = (int)(qq % c.ox); qq /= c.ox;
-        const int oy = (int)(qq % c.oy); qq /= c.oy;
-        const int oz = (int)(qq % c.oz); const int n = (int)(qq / c.oz);
-        const int z = c.stride * oz + kz, yy = c.stride * oy + ky, xx = c.stride * ox + kx;
-        if (z >= 0 && z < c.iz && yy >= 0 && yy < c.iy && xx >= 0 && xx < c.ix) {
-          if (ci < c.c1) {
-            const long long p = c.up1 ? vox(n, z >> 1, yy >> 1, xx >> 1, (c.iz + 1) / 2, (c.iy + 1) / 2, (c.ix + 1) / 2)
-                                      : vox(n, z, yy, xx, c.iz, c.iy, c.ix);
-            val = x1[p * c.c1 + ci];
-          } else {
-            val = x2[vox(n, z, yy, xx, c.iz, c.iy, c.ix) * c.c2 + (ci - c.c1)];
-          }
-        }
-      }
-      sx[ci * kWgVox + v] = val;
-    }
-    __syncthreads();
-    if (tap == 13 && db != nullptr)
-      for (int co = threadIdx.x; co < c.cout; co += blockDim.x)
-        for (int v = 0; v < kWgVox; ++v) bsum += __bfloat162float(sdy[co * kWgVox + v]);
-    int slot = 0;
-    for (int tile = warp; tile < tiles; tile += kWarps, ++slot) {
-      const int mt = tile / ntiles, nt = tile - mt * ntiles;
-      for (int ks = 0; ks < kWgVox / 16; ++ks) {
-        uint32_t a[4];
-        const __nv_bfloat16* ap = sdy + (mt * 16) * kWgVox + ks * 16;
-        a[0] = *reinterpret_cast<const uint32_t*>(ap + g * kWgVox + 2 * t);
-        a[1] = *reinterpret_cast<const uint32_t*>(ap + (g + 8) * kWgVox + 2 * t);
-        a[2] = *reinterpret_cast<const uint32_t*>(ap + g * kWgVox + 2 * t + 8);
-        a[3] = *reinterpret_cast<const uint32_t*>(ap + (g + 8) * kWgVox + 2 * t + 8);
-        const __nv_bfloat16* bp = sx + (nt * 8 + g) * kWgVox + ks * 16;
-        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(bp + 2 * t);
-        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(bp + 2 * t + 8);
-        mma_bf16(acc[slot], a, b0, b1);
-      }
-    }
-  }
-  int slot = 0;
-  for (int tile = warp; tile < tiles; tile += kWarps, ++slot) {
-    const int mt = tile / ntiles, nt = tile - mt * ntiles;
-    for (int h = 0; h < 2; ++h) {
-      const int co = mt * 16 + g + 8 * h;
-      const int ci = nt * 8 + 2 * t;
-      float* o = dw + ((size_t)tap * cop + co) * cin + ci;
-      atomicAdd(o, acc[slot][2 * h]);
-      atomicAdd(o + 1, acc[slot][2 * h + 1]);
-    }
-  }
-  if (tap == 13 && db != nullptr)
-    for (int co = threadIdx.x; co < c.cout; co += blockDim.x) atomicAdd(db + co, bsum);
-}
-
-// ---------------------------------------------------------------------------
-// small kernels
-// ---------------------------------------------------------------------------
-
-// dpre = grad * LeakyReLU'(y) (y is the activation output, whose sign equals
-// the pre-activation's), bf16, channels padded to cout_p with zeros
 __global__ void k_act_backward(const float* __restrict__ grad, const __nv_bfloat16* __restrict__ y, int act,
                                __nv_bfloat16* __restrict__ dpre, long long nvox, int cout, int cout_p) {
   const long long total = nvox * cout_p;
@@ -474,6 +362,20 @@ static int launch_tc(const Conv& c, long long rows, int kc, const void* x1, cons
   return WR_OK;
 }
 
+template <int NT>
+static int launch_wgrad_tc(const Conv& c, const void* x1, const void* x2, const void* dy, float* dw, float* db,
+                           cudaStream_t s) {
+  int* err = tc_err_ptr();
+  if (!err) return fail(WR_E_PARAM, "no CUDA device for the tensor-core convolution");
+  const size_t smem = tc_wgrad_smem_bytes(16 * NT);
+  cudaFuncSetAttribute(k_conv_wgrad_tc<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
+  const dim3 grid((unsigned)((nvox + kWgK * kWgStages - 1) / (kWgK * kWgStages)), 27);
+  k_conv_wgrad_tc<NT><<<grid, kTcThreads, smem, s>>>(c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2,
+                                                     (const __nv_bfloat16*)dy, dw, db, err);
+  return WR_OK;
+}
+
 }  // namespace wrnet
 
 using namespace wrnet;
@@ -539,10 +441,13 @@ int wr_net_conv3d_wgrad(const WrConvGeom* geom, const void* x1, const void* x2, 
   if (rc) return rc;
   if (!x1 || !dy || !dw || (c.c2 && !x2)) return fail(WR_E_NULL, "a required pointer is NULL");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const long long nvox = (long long)c.n * c.oz * c.oy * c.ox;
-  dim3 grid((unsigned)((nvox + kWgVox * kWgChunks - 1) / (kWgVox * kWgChunks)), 27);
-  k_conv_wgrad<<<grid, kWarps * 32, (size_t)(c.cout_p + c.cin) * kWgVox * 2, s>>>(
-      c, (const __nv_bfloat16*)x1, (const __nv_bfloat16*)x2, (const __nv_bfloat16*)dy, dw, db);
+  switch (c.cout_p / 16) {
+    case 1: rc = launch_wgrad_tc<1>(c, x1, x2, dy, dw, db, s); break;
+    case 2: rc = launch_wgrad_tc<2>(c, x1, x2, dy, dw, db, s); break;
+    case 3: rc = launch_wgrad_tc<3>(c, x1, x2, dy, dw, db, s); break;
+    default: rc = launch_wgrad_tc<4>(c, x1, x2, dy, dw, db, s); break;
+  }
+  if (rc) return rc;
   return cuda_status("wr_net_conv3d_wgrad");
 }
 
