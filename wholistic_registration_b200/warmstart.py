@@ -388,6 +388,61 @@ class WarmStartRegistrar:
         return motion
 
 
+def time_network(shape=(128, 1024, 1024), train_shape=(64, 256, 256), reps=5, device=None, net=None):
+    """Milliseconds (CUDA events) of the network's inference on a (z, y, x)
+    pair of ``shape`` (pooling, forward, up-sampling of the field) and of one
+    training step at ``train_shape`` (pooling, forward, loss, backward, Adam;
+    the target field is zero here, so no registration is timed)."""
+    from . import synthetic
+
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if net is None:
+        net = WarmStartNet(dev)
+        if os.path.exists(DEFAULT_WEIGHTS):
+            net.load()
+
+    def ev(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    blobs = max(200, int(20000 * np.prod(shape) / (128 * 1024 * 1024)))
+    t, m, _ = synthetic.make_pair(shape, 3, n_blobs=blobs, max_disp=(8.0, 8.0, 3.0), device=dev)
+    t, m = t.contiguous(), m.contiguous()
+    field = torch.empty(shape + (3,), dtype=torch.float32, device=dev)
+    out[f"inference {'x'.join(map(str, shape))}"] = ev(lambda: net.predict(t, m, out=field), reps)
+    t, m, _ = synthetic.make_pair(train_shape, 4, n_blobs=2000, max_disp=(8.0, 8.0, 3.0), device=dev)
+    t, m = t.float().contiguous(), m.float().contiguous()
+    z, y, x = train_shape
+    g0 = (z, y // POOL, x // POOL)
+    target = torch.zeros((int(np.prod(g0)), 3), dtype=torch.float32, device=dev)
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+
+    def step():
+        net.prepare(t, m, keep_fp32=True)
+        pred = net.forward()
+        net.zero_grad()
+        _lib.check("wr_net_flow_loss", net.lib.wr_net_flow_loss(
+            pred.data_ptr(), target.data_ptr(), net._t4.data_ptr(), net._m4.data_ptr(), net.grad["out"].data_ptr(),
+            loss.data_ptr(), 1, *g0, float(POOL), 1.0, 1.0, net._stream()))
+        net.backward()
+        net.adam_step(1e-6)
+
+    out[f"training step {'x'.join(map(str, train_shape))}"] = ev(step, reps)
+    flag = ctypes.c_int(-1)
+    _lib.check("wr_net_tc_error", net.lib.wr_net_tc_error(ctypes.byref(flag)))
+    if flag.value:
+        raise RuntimeError("a tensor-core convolution gave up waiting for its MMAs")
+    return out
+
+
 SWEEP_REFINE = ((0, 2), (0, 4), (0, 10), (1, 2), (1, 4), (1, 6), (2, 4), (2, 6), (2, 10), (3, 4))
 SWEEP_STARTS = ("zero", "network", "truth", "plain")
 
@@ -485,6 +540,16 @@ def main(argv=None):
     import sys
 
     argv = sys.argv[1:] if argv is None else argv
+    if argv[:1] == ["time"]:
+        ap = argparse.ArgumentParser(description="time the network: inference on a pair, one training step")
+        ap.add_argument("--shape", default="128x1024x1024", help="z x y x x of the inference pair")
+        ap.add_argument("--train-shape", default="64x256x256")
+        ap.add_argument("--reps", type=int, default=5)
+        args = ap.parse_args(argv[1:])
+        for name, ms in time_network(tuple(int(v) for v in args.shape.split("x")),
+                                     tuple(int(v) for v in args.train_shape.split("x")), args.reps).items():
+            print(f"{name}: {ms:.3f} ms")
+        return
     if argv[:1] == ["sweep"]:
         ap = argparse.ArgumentParser(description="what a warm start can buy (see sweep())")
         ap.add_argument("--shape", default="128x1024x1024")
