@@ -183,6 +183,34 @@ WR_API int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, con
                                    void* stream, WrProfile* prof);
 
 /*
+ * Snapshots getMotion keeps in its error_log (utils/calFlow3d_Wei_v1.py:
+ * 329-353, 451-470): at every iteration `it` of level l with
+ * it % save_ite == 0, taken before that iteration's update, the level's dense
+ * motion ("motion_current") and the moving level warped by it
+ * ("data_mov_corrected", trilinear with edge clamping); once per level the
+ * level's reference and moving images ("data_ref", "data_mov").  All device
+ * float32 (z, y_l, x_l[, 3]) arrays, x_l / y_l the level's extents; slot s of
+ * level l holds iteration s * save_ite (capacity slots per level; the level
+ * evaluated stats.evals[l] times, so ceil(evals / save_ite) slots are
+ * written, at most capacity).  Any pointer may be NULL.
+ */
+typedef struct {
+  int32_t save_ite;
+  int32_t capacity;
+  float* motion[WR_MAX_LEVELS];
+  float* warped[WR_MAX_LEVELS];
+  float* level_ref[WR_MAX_LEVELS];
+  float* level_mov[WR_MAX_LEVELS];
+} WrSnapshots;
+
+/* wr_lk_register that also fills `snap` (getMotion's error_log snapshots);
+   snap may be NULL. */
+WR_API int wr_lk_register_snapshots(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                                    const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                                    float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                                    void* stream, const WrSnapshots* snap);
+
+/*
  * One frame of a batched registration (wr_lk_register_batch).  mov and ref
  * have the same shape and dtype; shapes may differ between frames.
  */

@@ -151,6 +151,30 @@ def make_bench_case(ref, out_dir, name):
     print(f"{name}: {t1 - t0:.0f} s, error {err:.6f}, evals/level {counts}", flush=True)
 
 
+def make_snapshot_case(ref, out_dir):
+    """getMotion with save_ite = 2: the error_log snapshots (motion_current,
+    data_mov_corrected) of every second iteration and the level images."""
+    cf3 = ref["calFlow3d_Wei_v1"]
+    prep = ref["preprocess"]
+    zyx = (6, 48, 56)
+    tmpl, mov, _ = _pair_xyz(zyx, 41, 150, (2.5, 2.5, 0.8))
+    excl = np.ascontiguousarray(~synthetic.ellipsoid_inclusion(zyx, 0.8).numpy().transpose(2, 1, 0))
+    factor = prep.getSmPnltNormFctr(tmpl.astype(np.float64), {"mask_ref": excl})
+    option = {"mask_ref": excl.copy(), "mask_mov": excl.copy(), "layer": 1, "iter": 6, "r": 3, "zRatio": 1.0,
+              "movRange": 5.0, "motion": None, "smoothPenalty": float(factor * 0.08), "tol": 1e-3, "save_ite": 2}
+    motion, err, _, log = cf3.getMotion(mov.copy(), tmpl.copy(), option)
+    rec = {"mov": mov, "ref": tmpl, "excl": excl, "motion": motion.astype(np.float32),
+           "smooth_penalty": np.float64(factor * 0.08)}
+    for lk, lv in log.items():
+        rec[f"{lk}/currentError"] = np.asarray(lv["currentError"], np.float64)
+        rec[f"{lk}/motion_current"] = np.stack([np.asarray(a, np.float32) for a in lv["motion_current"]])
+        rec[f"{lk}/data_mov_corrected"] = np.stack([np.asarray(a, np.float32) for a in lv["data_mov_corrected"]])
+        rec[f"{lk}/data_ref"] = np.asarray(lv["data_ref"], np.float32)
+        rec[f"{lk}/data_mov"] = np.asarray(lv["data_mov"], np.float32)
+        print(f"snapshots {lk}: evals {len(lv['currentError'])}, snapshots {len(lv['motion_current'])}")
+    np.savez_compressed(os.path.join(out_dir, "snapshots.npz"), **rec)
+
+
 def make_primitive_cases(ref, out_dir):
     imr = ref["imresize"]
     cf3 = ref["calFlow3d_Wei_v1"]
@@ -608,11 +632,14 @@ def main():
     ap.add_argument("--ref", default=os.environ.get("WR_REFERENCE_ROOT"),
                     help="root of the reference checkout (default: $WR_REFERENCE_ROOT)")
     ap.add_argument("--only", choices=["primitives", "motion", "masks", "xres", "xreshr", "xresopt", "refblock",
-                                       "bench", "wrappers"], default=None)
+                                       "bench", "wrappers", "snapshots"], default=None)
     ap.add_argument("--case", default=None, help="with --only bench: one case of BENCH_CASES")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference root is required (--ref or WR_REFERENCE_ROOT)")
+    if args.only == "snapshots":
+        make_snapshot_case(load_reference(args.ref), HERE)
+        return
     if args.only == "wrappers":
         make_wrapper_cases(args.ref, HERE)
         return

@@ -44,6 +44,7 @@ EXPORTS = (
     "wr_lk_register",
     "wr_lk_register_profiled",
     "wr_lk_register_warp",
+    "wr_lk_register_snapshots",
     "wr_lk_batch_workspace_size",
     "wr_lk_register_batch",
     "wr_lk_batch_each_workspace_size",
@@ -146,6 +147,18 @@ class WrProfile(ctypes.Structure):
     ]
 
 
+class WrSnapshots(ctypes.Structure):
+    """getMotion's error_log snapshots (include/wr_b200.h): device float32 arrays per level."""
+    _fields_ = [
+        ("save_ite", ctypes.c_int32),
+        ("capacity", ctypes.c_int32),
+        ("motion", ctypes.c_void_p * MAX_LEVELS),
+        ("warped", ctypes.c_void_p * MAX_LEVELS),
+        ("level_ref", ctypes.c_void_p * MAX_LEVELS),
+        ("level_mov", ctypes.c_void_p * MAX_LEVELS),
+    ]
+
+
 class WrLKItem(ctypes.Structure):
     _fields_ = [
         ("mov", WrVolume),
@@ -199,6 +212,7 @@ def load():
         lib.wr_lk_register.argtypes = [ctypes.POINTER(WrVolume), ctypes.POINTER(WrVolume), vp, vp,
                                        ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
         lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
+        lib.wr_lk_register_snapshots.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrSnapshots)]
         lib.wr_lk_batch_workspace_size.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams),
                                                    ctypes.POINTER(sz)]
         lib.wr_lk_register_batch.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams), vp, sz, vp]

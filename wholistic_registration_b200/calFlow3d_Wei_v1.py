@@ -126,11 +126,55 @@ class _LazyCoords:
         return self._build()[idx]
 
 
+def _snapshot_buffers(shape_zyx, params, save_ite, device):
+    """Device buffers for getMotion's error_log snapshots: per level, one slot
+    per iteration index that is a multiple of save_ite."""
+    if save_ite < 1:
+        raise ValueError("option['save_ite'] must be >= 1")
+    z, y, x = shape_zyx
+    cap = -(-params.iter // save_ite)
+    snap = _lib.WrSnapshots()
+    snap.save_ite, snap.capacity = save_ite, cap
+    bufs = {}
+    for l in range(params.layer + 1):
+        yl, xl = int(y / 2 ** l), int(x / 2 ** l)
+        b = {"motion": torch.empty((cap, z, yl, xl, 3), dtype=torch.float32, device=device),
+             "warped": torch.empty((cap, z, yl, xl), dtype=torch.float32, device=device),
+             "ref": torch.empty((z, yl, xl), dtype=torch.float32, device=device),
+             "mov": torch.empty((z, yl, xl), dtype=torch.float32, device=device)}
+        snap.motion[l], snap.warped[l] = b["motion"].data_ptr(), b["warped"].data_ptr()
+        snap.level_ref[l], snap.level_mov[l] = b["ref"].data_ptr(), b["mov"].data_ptr()
+        bufs[l] = b
+    return snap, bufs
+
+
+def _fill_snapshots(log, st, snaps, save_ite, on_device):
+    """The reference's error_log snapshot entries (utils/calFlow3d_Wei_v1.py:
+    329-353, 451-470) in its (x, y, z[, 3]) layout."""
+    _, bufs = snaps
+    xyz = (lambda t: t.permute(2, 1, 0)) if on_device else (lambda t: t.cpu().numpy().transpose(2, 1, 0))
+    xyz3 = (lambda t: t.permute(2, 1, 0, 3)) if on_device else (lambda t: t.cpu().numpy().transpose(2, 1, 0, 3))
+    for l, b in bufs.items():
+        n = min(-(-int(st.evals[l]) // save_ite), b["motion"].shape[0])
+        entry = log[f"layer_{l}"]
+        entry["motion_current"] = [xyz3(b["motion"][k]) for k in range(n)]
+        entry["data_mov_corrected"] = [xyz(b["warped"][k]) for k in range(n)]
+        entry["data_ref"] = xyz(b["ref"])
+        entry["data_mov"] = xyz(b["mov"])
+
+
 def getMotion(dat_mov, dat_ref, option, verbose=False):
     """Pyramid patch-wise Lucas-Kanade registration of ``dat_mov`` onto ``dat_ref``.
 
     Same contract as utils/calFlow3d_Wei_v1.py:295-673; returns
     ``(motion (x,y,z,3) float32, currentError, coords_new, error_log)``.
+    ``error_log`` holds the per-level error and motion-change lists; with
+    ``option["keep_snapshots"] = True`` it also holds the reference's
+    snapshots — "motion_current" and "data_mov_corrected" at every iteration
+    that is a multiple of ``option["save_ite"]`` (taken before that
+    iteration's update) and the level images "data_ref" / "data_mov", all
+    float32 — which cost a device-to-host copy of about three times the
+    volume's float32 motion per level, so they are opt-in.
     """
     on_device = isinstance(dat_mov, torch.Tensor) and dat_mov.is_cuda
     device = dat_mov.device if on_device else torch.device("cuda", torch.cuda.current_device())
@@ -146,8 +190,12 @@ def getMotion(dat_mov, dat_ref, option, verbose=False):
     mask_ref = _device_mask(option.get("mask_ref"), shape_xyz, device)
     init = _device_motion(option.get("motion"), shape_xyz, device)
     reg = _registrar(tuple(mov.shape), params, device)
-    motion = reg.register(mov, ref, mask_mov, mask_ref, init)
+    snaps = _snapshot_buffers(tuple(mov.shape), params, int(option.get("save_ite", 100)), device) \
+        if option.get("keep_snapshots") else None
+    motion = reg.register(mov, ref, mask_mov, mask_ref, init, snapshots=snaps[0] if snaps else None)
     log, current_error = stats_to_log(reg.stats(), params.layer + 1)
+    if snaps:
+        _fill_snapshots(log, reg.stats(), snaps, int(option.get("save_ite", 100)), on_device)
     if verbose:
         for k, v in log.items():
             for i, e in enumerate(v["currentError"]):

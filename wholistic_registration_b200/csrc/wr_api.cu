@@ -641,10 +641,26 @@ static void finish_frame(const Plan& P, void* ws, const T* mov, float* out, floa
   if (stats) cudaMemcpyAsync(stats, &st->stats, sizeof(WrLKStats), cudaMemcpyDeviceToDevice, s);
 }
 
+// error_log snapshot of one iteration slot (motion and warped moving level)
+template <int PREC>
+static void snapshot(int mode, const LKState* st, const FieldSrc& f, const void* movg, const LevelPlan& L,
+                     float* motion, float* warped, cudaStream_t s) {
+  const typename Store<PREC>::V4* g = static_cast<const typename Store<PREC>::V4*>(movg);
+  const int grid = row_grid((long long)L.nz * L.ny);
+  switch (mode) {
+    case FIELD_CP: k_snapshot<FIELD_CP, PREC><<<grid, kRowBlock, 0, s>>>(st, f, g, L.nx, L.ny, L.nz, motion, warped); break;
+    case FIELD_UP: k_snapshot<FIELD_UP, PREC><<<grid, kRowBlock, 0, s>>>(st, f, g, L.nx, L.ny, L.nz, motion, warped); break;
+    case FIELD_DENSE:
+      k_snapshot<FIELD_DENSE, PREC><<<grid, kRowBlock, 0, s>>>(st, f, g, L.nx, L.ny, L.nz, motion, warped);
+      break;
+    default: k_snapshot<FIELD_ZERO, PREC><<<grid, kRowBlock, 0, s>>>(st, f, g, L.nx, L.ny, L.nz, motion, warped);
+  }
+}
+
 template <typename T, int PREC>
 static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const T* ref, const uint8_t* mmov,
                         const uint8_t* mref, const float* init, float* out, float* warped, WrLKStats* stats, void* ws,
-                        cudaStream_t s, WrProfile* prof) {
+                        cudaStream_t s, WrProfile* prof, const WrSnapshots* snap = nullptr) {
   int recorded = 0;
   LKState* st = at_off<LKState>(ws, P.state);
   prepare_frame<T, PREC>(P, p, mov, ref, mmov, mref, init, ws, s);
@@ -658,11 +674,20 @@ static int run_register(const Plan& P, const WrLKParams* p, const T* mov, const 
     IterArgs a = begin_level(P, l, ws, init != nullptr, mask, mmov != nullptr, &mode0, s);
     const FieldSrc f0 = a.field0;
     const int forced = p->forced_updates[l];
+    if (snap && (snap->level_ref[l] || snap->level_mov[l]))
+      k_level_images<PREC><<<grid_for(L.n), kThreads, 0, s>>>(static_cast<const typename Store<PREC>::V1*>(a.ref),
+                                                              static_cast<const typename Store<PREC>::V4*>(a.mov.g),
+                                                              L.n, snap->level_ref[l], snap->level_mov[l]);
     for (int it = 0; it < P.iter; ++it) {
       const int mode = it == 0 ? mode0 : FIELD_CP;
       // the launch after the level's first update also measures max |new - initial|
       const int diff0 = it == 1 ? mode0 : kNoDiff;
       a.field = it == 0 ? f0 : field_src(P, l, FIELD_CP, ws);
+      if (snap && snap->save_ite > 0 && it % snap->save_ite == 0 && it / snap->save_ite < snap->capacity) {
+        const size_t slot = (size_t)(it / snap->save_ite) * L.n;
+        snapshot<PREC>(mode, st, a.field, a.mov.g, L, snap->motion[l] ? snap->motion[l] + 3 * slot : nullptr,
+                       snap->warped[l] ? snap->warped[l] + slot : nullptr, s);
+      }
       const size_t smem = accumulate_smem(P.w, diff0 == FIELD_UP);
       const bool rec = prof && recorded < prof->capacity;
       if (rec) cudaEventRecord((cudaEvent_t)prof->acc_begin[recorded], s);
@@ -873,17 +898,17 @@ static int noalloc_partials(double** out) {
 template <int PREC>
 static int dispatch_dtype(const Plan& P, const WrLKParams* p, const WrVolume* mov, const WrVolume* ref,
                           const uint8_t* mmov, const uint8_t* mref, const float* init, float* out, float* warped,
-                          WrLKStats* stats, void* ws, cudaStream_t s, WrProfile* prof) {
+                          WrLKStats* stats, void* ws, cudaStream_t s, WrProfile* prof, const WrSnapshots* snap) {
   switch (mov->dtype) {
     case WR_U16:
       return run_register<uint16_t, PREC>(P, p, (const uint16_t*)mov->data, (const uint16_t*)ref->data, mmov, mref,
-                                          init, out, warped, stats, ws, s, prof);
+                                          init, out, warped, stats, ws, s, prof, snap);
     case WR_U8:
       return run_register<uint8_t, PREC>(P, p, (const uint8_t*)mov->data, (const uint8_t*)ref->data, mmov, mref, init,
-                                         out, warped, stats, ws, s, prof);
+                                         out, warped, stats, ws, s, prof, snap);
     default:
       return run_register<float, PREC>(P, p, (const float*)mov->data, (const float*)ref->data, mmov, mref, init, out,
-                                       warped, stats, ws, s, prof);
+                                       warped, stats, ws, s, prof, snap);
   }
 }
 
@@ -1023,7 +1048,7 @@ int wr_lk_register(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl
 static int register_common(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
                            const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
                            float* motion_out, float* warped_out, WrLKStats* stats, void* workspace,
-                           size_t workspace_bytes, void* stream, WrProfile* prof) {
+                           size_t workspace_bytes, void* stream, WrProfile* prof, const WrSnapshots* snap = nullptr) {
   int rc;
   if ((rc = check_volume(mov, "mov"))) return rc;
   if ((rc = check_volume(ref, "ref"))) return rc;
@@ -1043,13 +1068,13 @@ static int register_common(const WrVolume* mov, const WrVolume* ref, const uint8
   switch (p->precision) {
     case WR_PREC_F16:
       return dispatch_dtype<WR_PREC_F16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
-                                         warped_out, stats, workspace, s, prof);
+                                         warped_out, stats, workspace, s, prof, snap);
     case WR_PREC_BF16:
       return dispatch_dtype<WR_PREC_BF16>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
-                                          warped_out, stats, workspace, s, prof);
+                                          warped_out, stats, workspace, s, prof, snap);
     default:
       return dispatch_dtype<WR_PREC_F32>(P, p, mov, ref, excl_mask_mov, excl_mask_ref, motion_init, motion_out,
-                                         warped_out, stats, workspace, s, prof);
+                                         warped_out, stats, workspace, s, prof, snap);
   }
 }
 
@@ -1059,6 +1084,15 @@ int wr_lk_register_profiled(const WrVolume* mov, const WrVolume* ref, const uint
                             void* stream, WrProfile* prof) {
   return register_common(mov, ref, excl_mask_mov, excl_mask_ref, p, motion_init, motion_out, nullptr, stats,
                          workspace, workspace_bytes, stream, prof);
+}
+
+int wr_lk_register_snapshots(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,
+                             const uint8_t* excl_mask_ref, const WrLKParams* p, const float* motion_init,
+                             float* motion_out, WrLKStats* stats, void* workspace, size_t workspace_bytes,
+                             void* stream, const WrSnapshots* snap) {
+  if (snap && (snap->save_ite < 1 || snap->capacity < 0)) return fail(WR_E_PARAM, "snapshots: save_ite >= 1, capacity >= 0");
+  return register_common(mov, ref, excl_mask_mov, excl_mask_ref, p, motion_init, motion_out, nullptr, stats,
+                         workspace, workspace_bytes, stream, nullptr, snap);
 }
 
 int wr_lk_register_warp(const WrVolume* mov, const WrVolume* ref, const uint8_t* excl_mask_mov,

@@ -1503,6 +1503,59 @@ __global__ void k_dense_init_pack(float4* out, const float* c0, const float* c1,
 }
 
 // final motion (z, y, x, 3)
+// getMotion's error_log snapshot of one iteration (utils/calFlow3d_Wei_v1.py:
+// 451-470): the level's dense motion (z, y, x, 3) and the moving level warped
+// by it (trilinear, taps clamped to the level); nothing when the level has
+// stopped before this iteration.
+template <int MODE, int PREC>
+__global__ void k_snapshot(const LKState* st, FieldSrc f, const typename Store<PREC>::V4* __restrict__ movg, int nx,
+                           int ny, int nz, float* __restrict__ motion, float* __restrict__ warped) {
+  typedef Store<PREC> S;
+  if (!*(volatile const int*)&st->active) return;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    WR_FOR_COLS(nx, x) {
+      const float3 m = eval_field<MODE>(f, x, y, z);
+      const size_t i = ((size_t)z * ny + y) * nx + x;
+      if (motion) {
+        motion[3 * i] = m.x;
+        motion[3 * i + 1] = m.y;
+        motion[3 * i + 2] = m.z;
+      }
+      if (warped) {
+        int x0, y0, z0;
+        float tx, ty, tz;
+        split_coord((float)x + m.x, x0, tx);
+        split_coord((float)y + m.y, y0, ty);
+        split_coord((float)z + m.z, z0, tz);
+        const int xs[2] = {clampi(x0, 0, nx - 1), clampi(x0 + 1, 0, nx - 1)};
+        const int ys[2] = {clampi(y0, 0, ny - 1), clampi(y0 + 1, 0, ny - 1)};
+        const int zs[2] = {clampi(z0, 0, nz - 1), clampi(z0 + 1, 0, nz - 1)};
+        float acc = 0.f;
+        for (int c = 0; c < 2; ++c)
+          for (int b = 0; b < 2; ++b)
+            for (int a = 0; a < 2; ++a) {
+              const float wgt = (a ? tx : 1.f - tx) * (b ? ty : 1.f - ty) * (c ? tz : 1.f - tz);
+              acc = fmaf(wgt, S::load_m(movg + ((size_t)zs[c] * ny + ys[b]) * nx + xs[a]), acc);
+            }
+        warped[i] = acc;
+      }
+    }
+  }
+}
+
+// a level's reference and moving images as float32 (error_log "data_ref" / "data_mov")
+template <int PREC>
+__global__ void k_level_images(const typename Store<PREC>::V1* __restrict__ ref,
+                               const typename Store<PREC>::V4* __restrict__ movg, long long n, float* ref_out,
+                               float* mov_out) {
+  typedef Store<PREC> S;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (ref_out) ref_out[i] = S::load1(ref + i);
+    if (mov_out) mov_out[i] = S::load_m(movg + i);
+  }
+}
+
 template <int MODE>
 __global__ void k_write_motion(float* __restrict__ out, FieldSrc f, int nx, int ny, int nz) {
   WR_FOR_ROWS(nz * ny, row) {

@@ -144,7 +144,7 @@ class LKRegistrar:
 
     def register(self, mov: torch.Tensor, ref: torch.Tensor, mask_mov=None, mask_ref=None,
                  motion_init=None, out=None, stream=None, profile=None, reuse_reference=False,
-                 warped_out=None) -> torch.Tensor:
+                 warped_out=None, snapshots=None) -> torch.Tensor:
         """Motion (z, y, x, 3) float32 registering ``mov`` onto ``ref``.
 
         Masks are (z, y, x) uint8/bool exclusion masks (True = excluded) or
@@ -183,6 +183,13 @@ class LKRegistrar:
         args = (ctypes.byref(vm), ctypes.byref(vr), ptrs[0], ptrs[1], ctypes.byref(self._cp), init_ptr,
                 out.data_ptr(), self.stats_dev.data_ptr(), self._ws_ptr, self.workspace_bytes, _stream_ptr(stream))
         prof = ctypes.byref(profile.begin_call()) if profile is not None else None
+        if snapshots is not None:
+            # getMotion's error_log snapshots (a _lib.WrSnapshots of device buffers)
+            if warped_out is not None or profile is not None:
+                raise ValueError("snapshots cannot be combined with warped_out or profile")
+            _lib.check("wr_lk_register_snapshots",
+                       self.lib.wr_lk_register_snapshots(*args, ctypes.byref(snapshots)))
+            return out
         if warped_out is not None:
             _require_cuda(warped_out, "warped_out")
             if tuple(warped_out.shape) != self.shape or warped_out.dtype != torch.float32 \
