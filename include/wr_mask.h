@@ -50,6 +50,16 @@ WR_API int wr_get_mask(const WrVolume* vol, double thres_factor, double percenti
  * error_flag (device, optional) is nonzero if a union-find retry loop hit its
  * bound (it does not on any input; the flag makes the bound observable).
  */
+/*
+ * Frame correlation of pick_initial_reference (utils/reference.py:60-78):
+ * `frames` is t rows of d float32 values (device); writes each row's mean
+ * (`means`, t doubles) and the Gram matrix of the demeaned rows (`gram`,
+ * t x t doubles, symmetric), both summed in float64 in a fixed order.  The
+ * caller normalises it by the square roots of its diagonal as the reference
+ * does.  1 <= t <= 4096.
+ */
+WR_API int wr_frame_gram(const float* frames, int32_t t, int64_t d, double* means, double* gram, void* stream);
+
 WR_API int wr_bwareafilt3(const uint8_t* mask_in, int32_t nz, int32_t ny, int32_t nx, int64_t min_size,
                           int64_t max_size, uint8_t* mask_out, int32_t* n_components, int32_t* error_flag,
                           void* workspace, size_t workspace_bytes, void* stream);

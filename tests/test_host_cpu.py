@@ -111,39 +111,18 @@ def test_xres_wrong_region_options_validated():
     assert rc_big == rc_big2 == 0 and big_on - big_off > 2 * (146 * 146 * 24)
 
 
-def test_compute_reference_from_block_matches_reference():
-    """compute_reference_from_block (utils/reference.py:102-124) against the
-    reference's own function run on the same block (fixture from
-    tests/golden/make_golden.py): the same frames picked, in order, and the
-    same reference volume (float32 correlation GEMM, float64 means) for a
-    single channel, dual channel with sqrt and log2 transforms, and k = 0.
-    Torch runs on CPU tensors here; the path is plain torch."""
-    import os
-
+def test_pick_initial_reference_needs_a_cuda_tensor():
+    """The template picking's frame correlation runs in the library's kernel
+    (wr_frame_gram); CPU tensors are refused, not computed on the host."""
     import numpy as np
+    import pytest
     import torch
 
-    from wholistic_registration_b200.registration import compute_reference_from_block
+    from wholistic_registration_b200.registration import pick_initial_reference
 
-    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_block.npz")))
-    mem, ca = torch.from_numpy(d["mem"]), torch.from_numpy(d["ca"])
-    for name in ("single", "dual_sqrt", "dual_log2", "dual_k0"):
-        dual, k = d[f"{name}_params"]
-        config = {"channels": {"k": float(k), "function": str(d[f"{name}_function"]), "dual_channel": bool(dual)}}
-        ref, idx = compute_reference_from_block(mem, config, ca if dual else None)
-        np.testing.assert_array_equal(idx, d[f"{name}_idx"], err_msg=name)
-        np.testing.assert_allclose(ref, d[f"{name}_ref"], rtol=1e-12, atol=1e-9, err_msg=name)
-    # float32 frames: the reference's mean (and its transform) stays float32
-    mem32, ca32 = torch.from_numpy(d["mem_f32"]), torch.from_numpy(d["ca_f32"])
-    for name in ("single", "dual_sqrt", "dual_log2", "dual_k0"):
-        dual, k = d[f"{name}_params"]
-        config = {"channels": {"k": float(k), "function": str(d[f"{name}_function"]), "dual_channel": bool(dual)}}
-        ref, idx = compute_reference_from_block(mem32, config, ca32 if dual else None)
-        want = d[f"f32_{name}_ref"]
-        assert ref.dtype == want.dtype == np.float32, (name, ref.dtype)
-        np.testing.assert_array_equal(idx, d[f"f32_{name}_idx"], err_msg=name)
-        # float32 sums in the same order; log2 / sqrt within a few float32 ulps
-        np.testing.assert_allclose(ref, want, rtol=1e-6, atol=0, err_msg=name)
+    frames = torch.from_numpy(np.random.default_rng(0).uniform(0, 100, (4, 3, 16, 16)).astype(np.float32))
+    with pytest.raises(ValueError, match="CUDA"):
+        pick_initial_reference(frames, max_corr_frames=2)
 
 
 def test_get_motion_v2_wrong_region_options(monkeypatch):

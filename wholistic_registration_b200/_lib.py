@@ -69,6 +69,7 @@ EXPORTS = (
     "wr_net_pool_flow",
     "wr_net_upsample_flow",
     "wr_mask_last_error",
+    "wr_frame_gram",
     "wr_mask_workspace_size",
     "wr_get_mask",
     "wr_bwareafilt3",
@@ -213,6 +214,7 @@ def load():
                                        ctypes.POINTER(WrLKParams), vp, vp, vp, vp, sz, vp]
         lib.wr_lk_register_profiled.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrProfile)]
         lib.wr_lk_register_snapshots.argtypes = lib.wr_lk_register.argtypes + [ctypes.POINTER(WrSnapshots)]
+        lib.wr_frame_gram.argtypes = [vp, i32, ctypes.c_int64, vp, vp, vp]
         lib.wr_lk_batch_workspace_size.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams),
                                                    ctypes.POINTER(sz)]
         lib.wr_lk_register_batch.argtypes = [ctypes.POINTER(WrLKItem), i32, ctypes.POINTER(WrLKParams), vp, sz, vp]
@@ -273,7 +275,7 @@ def check(fn, code):
         lib = load()
         if fn.startswith("wr_net"):
             raw = lib.wr_net_last_error()
-        elif fn in ("wr_get_mask", "wr_bwareafilt3") or fn.startswith("wr_mask"):
+        elif fn in ("wr_get_mask", "wr_bwareafilt3", "wr_frame_gram") or fn.startswith("wr_mask"):
             raw = lib.wr_mask_last_error()
         else:
             raw = lib.wr_last_error()

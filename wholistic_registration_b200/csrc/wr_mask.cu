@@ -444,6 +444,57 @@ static void get_mask(const T* v, int nz, int ny, int nx, double thres, double pc
   k_dilate<<<g, kThreads, 0, s>>>(tmp, out, nz, ny, nx, 2);
 }
 
+// ---------------------------------------------------------------------------
+// frame correlation of pick_initial_reference (utils/reference.py:60-78):
+// per-frame means, then the demeaned Gram matrix, both accumulated in float64
+// in a fixed order (deterministic).  One block per frame / per frame pair.
+// ---------------------------------------------------------------------------
+
+constexpr int kGramThreads = 256;
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  return t;   // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kGramThreads) k_frame_means(const float* __restrict__ x, long long d,
+                                                             double* __restrict__ means) {
+  __shared__ double red[kGramThreads / 32];
+  const float* row = x + (long long)blockIdx.x * d;
+  double s = 0.0;
+  for (long long k = threadIdx.x; k < d; k += blockDim.x) s += (double)row[k];
+  const double t = block_sum_d(s, red);
+  if (threadIdx.x == 0) means[blockIdx.x] = t / (double)d;
+}
+
+// pair p = (i, j), j >= i, enumerated row by row
+__global__ void __launch_bounds__(kGramThreads) k_frame_gram(const float* __restrict__ x, int t, long long d,
+                                                            const double* __restrict__ means,
+                                                            double* __restrict__ gram) {
+  __shared__ double red[kGramThreads / 32];
+  int i = 0, p = blockIdx.x;
+  while (p >= t - i) {
+    p -= t - i;
+    ++i;
+  }
+  const int j = i + p;
+  const float* a = x + (long long)i * d;
+  const float* b = x + (long long)j * d;
+  const double ma = means[i], mb = means[j];
+  double s = 0.0;
+  for (long long k = threadIdx.x; k < d; k += blockDim.x) s += ((double)a[k] - ma) * ((double)b[k] - mb);
+  const double v = block_sum_d(s, red);
+  if (threadIdx.x == 0) {
+    gram[(long long)i * t + j] = v;
+    gram[(long long)j * t + i] = v;
+  }
+}
+
 }  // namespace wrmask
 
 using namespace wrmask;
@@ -521,6 +572,18 @@ int wr_bwareafilt3(const uint8_t* mask_in, int32_t nz, int32_t ny, int32_t nx, i
   k_cc_filter<<<g, kThreads, 0, s>>>(L, count, n, (long long)min_size, (long long)max_size, mask_out, kept);
   if (n_components) cudaMemcpyAsync(n_components, kept, sizeof(int), cudaMemcpyDeviceToDevice, s);
   if (error_flag) cudaMemcpyAsync(error_flag, err, sizeof(int), cudaMemcpyDeviceToDevice, s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(-(int)e, cudaGetErrorString(e));
+  return 0;
+}
+
+int wr_frame_gram(const float* frames, int32_t t, int64_t d, double* means, double* gram, void* stream) {
+  if (!frames || !means || !gram) return fail(WR_E_NULL, "a required pointer is NULL");
+  if (t < 1 || t > 4096 || d < 1) return fail(WR_E_SHAPE, "need 1 <= t <= 4096 frames of d >= 1 values");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_frame_means<<<t, kGramThreads, 0, s>>>(frames, d, means);
+  const long long pairs = (long long)t * (t + 1) / 2;
+  k_frame_gram<<<(unsigned)pairs, kGramThreads, 0, s>>>(frames, t, d, means, gram);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(-(int)e, cudaGetErrorString(e));
   return 0;

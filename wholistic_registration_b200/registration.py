@@ -10,8 +10,9 @@ the outlier masks of the template and of every frame (``getMask`` +
 ``getMotion`` and ``correctMotion`` of the membrane channel, the calcium
 channel and the mixed frame, with the mean squared error before and after.
 Every step runs on the GPU: the registration and the masks in the sm_100a
-library, the template picking's frame-by-frame correlation as one cuBLAS
-float32 GEMM.  Inputs may be NumPy arrays (returned as NumPy, like the
+library, the template picking's frame-by-frame correlation as the
+library's demeaned Gram kernel (``wr_frame_gram``, float64 sums).  Inputs
+may be NumPy arrays (returned as NumPy, like the
 reference) or CUDA tensors (returned as CUDA tensors).
 """
 
@@ -21,6 +22,8 @@ import os
 
 import numpy as np
 import torch
+
+from . import _lib
 
 from .mask import bwareafilt3_wei, getMask
 from .registrar import LKParams, LKRegistrar, penalty_factor, warp
@@ -56,8 +59,9 @@ def transform(image, k=1, method="raw"):
 
 def pick_initial_reference(frames: torch.Tensor, max_corr_frames: int = 20, spatial_ds: int = 4):
     """utils/reference.py:19-99 on the device: the frames' correlation matrix
-    over the central three z planes (x and y subsampled by ``spatial_ds``) as
-    one float32 GEMM, the frame whose ``max_corr_frames`` best correlations
+    over the central three z planes (x and y subsampled by ``spatial_ds``)
+    from the library's demeaned Gram kernel (the reference's float32 GEMM,
+    summed here in float64), the frame whose ``max_corr_frames`` best correlations
     have the largest mean, and the full-resolution mean of that frame's best
     correlated frames.  Returns (reference, indices)."""
     if frames.dim() == 4:
@@ -69,14 +73,15 @@ def pick_initial_reference(frames: torch.Tensor, max_corr_frames: int = 20, spat
     else:
         raise ValueError("frames must be [T,Y,X] or [T,Z,Y,X]")
     small = used[:, :, ::spatial_ds, ::spatial_ds].to(torch.float32).contiguous()
+    if not small.is_cuda:
+        raise ValueError("pick_initial_reference runs on a CUDA device: frames must be a CUDA tensor")
     flat = small.reshape(T, -1)
-    dem = flat - flat.mean(dim=1, keepdim=True)
-    prev_tf32 = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False     # a float32 GEMM, as the reference's
-    try:
-        cc = dem @ dem.T
-    finally:
-        torch.backends.cuda.matmul.allow_tf32 = prev_tf32
+    # the demeaned frames' Gram matrix (the reference's float32 GEMM), summed in float64 by wr_frame_gram
+    lib = _lib.load()
+    means = torch.empty(T, dtype=torch.float64, device=flat.device)
+    cc = torch.empty((T, T), dtype=torch.float64, device=flat.device)
+    _lib.check("wr_frame_gram", lib.wr_frame_gram(flat.data_ptr(), T, flat.shape[1], means.data_ptr(), cc.data_ptr(),
+                                                  torch.cuda.current_stream(flat.device).cuda_stream))
     diag = torch.sqrt(torch.diagonal(cc)) + 1e-12
     cc = cc / (diag[:, None] * diag[None, :])
     ncorr = min(max_corr_frames, T - 1)
