@@ -337,10 +337,16 @@ __global__ void k_cc_union(const uint8_t* __restrict__ m, int* L, int nz, int ny
   }
 }
 
+// Each voxel's label becomes its root.  The walk to the root writes nothing:
+// a path-halving store racing with another thread's root store could put a
+// non-root ancestor back into that thread's label after the root went in,
+// and the filter reads the label as the root.  Root stores alone keep every
+// chain an ancestor chain.
 __global__ void k_cc_flatten_count(int* L, int* __restrict__ count, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     if (L[i] < 0) continue;
-    const int root = uf_find(L, (int)i);
+    int root = (int)i;
+    for (int q = L[root]; q != root; q = L[root]) root = q;
     L[i] = root;
     atomicAdd(&count[root], 1);
   }
