@@ -612,6 +612,21 @@ static IterArgs begin_level(const Plan& P, int l, void* ws, bool has_init, bool 
   a.zratio = L.zratio;
   a.nz_magic = host_div_magic(L.nz, L.nblk);
   a.ntx_magic = host_div_magic(L.ntx, (long long)L.ntx * L.nty);
+  // level constants of the sampling loop (tap clamps, plane strides, face tests)
+  a.nxm1 = L.nx - 1;
+  a.nym1 = L.ny - 1;
+  a.nxm2 = L.nx - 2;
+  a.nym2 = L.ny - 2;
+  a.bzmax = L.nz > 2 ? L.nz - 2 : 0;
+  a.plane = (uint32_t)L.nx * (uint32_t)L.ny;
+  a.oz1 = L.nz > 1 ? a.plane : 0u;   // a single slice reads its only plane twice
+  a.fnx = (float)L.nx;
+  a.fny = (float)L.ny;
+  a.fnz = (float)L.nz;
+  a.fnxm1 = (float)(L.nx - 1);
+  a.fnym1 = (float)(L.ny - 1);
+  a.fnzm1 = (float)(L.nz - 1);
+  a.fzmax = L.nz > 1 ? 1.f : 0.f;
   a.field = f0;
   a.field0 = f0;
   *mode0 = m0;

@@ -852,6 +852,11 @@ struct IterArgs {
   int r, w, ntx, nty;
   float zratio;
   uint32_t nz_magic, ntx_magic;        // div_magic multipliers of nz and ntx for the tile indexes
+  // level constants of the sampling loop, read as kernel parameters rather
+  // than recomputed from nx, ny, nz in the loop
+  int nxm1, nym1, nxm2, nym2, bzmax;
+  uint32_t plane, oz1;
+  float fnx, fny, fnz, fnxm1, fnym1, fnzm1, fzmax;
 };
 
 // warped moving exclusion mask > 0, evaluated exactly (float64 sum, float32 result)
