@@ -237,10 +237,17 @@ static bool resample_x_si(const SITaps& si, const Tin* in, Tout* out, int nrows,
   void (*kern)(const SITaps, const Tin*, Tout*, int, int, int, const double*, const int32_t*);
   if constexpr (std::is_same<Tin, uint8_t>::value && std::is_same<A, double>::value &&
                 std::is_same<Tout, double>::value) {
-    const size_t nwords = (nx_in + 31) / 32;
-    smem = (size_t)kStageWarps * (((size_t)nx_in + 15) / 16 * 16 + 8 * (nwords + 1));
+    smem = (size_t)kStageWarps * mask_stage_bytes(nx_in);
     kern = k_resample_x_mask<S>;
   } else {
+    if (si.c0 == kPPFirstTap<S> && nx_in <= kPPMaxIn && aligned(in, S * sizeof(Tin))) {
+      // rows staged relative to the first tap, static shared memory
+      long long g = (nrows + kStageWarps - 1) / kStageWarps;
+      if (g > 148LL * 32) g = 148LL * 32;
+      k_resample_x_pp<S, Tin, A, Tout><<<(int)g, dim3(32, kStageWarps), 0, s>>>(si, in, out, nrows, nx_in, nx_out,
+                                                                             w, idx);
+      return true;
+    }
     smem = (size_t)kStageWarps * S * si.ls * sizeof(A);
     kern = k_resample_x_si<S, Tin, A, Tout>;
   }
@@ -270,6 +277,13 @@ template <int S, typename Tin, typename A, typename Tout>
 static bool resample_y_si(const SITaps& si, const Tin* in, Tout* out, int nz, int ny_in, int ny_out, int nx,
                           const double* w, const int32_t* idx, cudaStream_t s) {
   if (si.s != S || si.P != 4 * S + 2) return false;
+  // V adjacent columns per lane: 16-byte loads of float32 / float64 inputs
+  constexpr int V = sizeof(Tin) >= 8 ? 2 : 4;
+  if (nx % V == 0 && aligned(in, V * sizeof(Tin))) {
+    k_resample_y_si_v<S, V, Tin, A, Tout><<<row_grid((long long)nz * ny_out), kRowBlock, 0, s>>>(
+        si, in, out, nz, ny_in, ny_out, nx, w, idx);
+    return true;
+  }
   k_resample_y_si<S, Tin, A, Tout><<<row_grid((long long)nz * ny_out), kRowBlock, 0, s>>>(si, in, out, nz, ny_in,
                                                                                        ny_out, nx, w, idx);
   return true;

@@ -260,13 +260,113 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_si(
   }
 }
 
+// First tap of an interior output of the antialiased bicubic table for an
+// integer down-scale factor S: taps s * o + kPPFirstTap<S> + t, t < 4S + 2
+// (utils/imresize.py:60-82 with width 4S; the host checks the table against it).
+template <int S> constexpr int kPPFirstTap = -(3 * S / 2) - 1;
+constexpr int kPPMaxIn = 1024;   // longest row of k_resample_x_pp
+
+// S consecutive inputs as one vector load (the row start and S * sizeof(T)
+// are multiples of the vector size).
+template <typename T, int S>
+__device__ __forceinline__ void load_group(const T* __restrict__ p, T (&v)[S]) {
+  constexpr int B = (int)sizeof(T) * S;
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int c = 0; c < B / 16; ++c) {
+      const int4 q = __ldg(reinterpret_cast<const int4*>(p) + c);
+      memcpy(&v[c * (16 / (int)sizeof(T))], &q, 16);
+    }
+  } else if constexpr (B == 8) {
+    const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
+    memcpy(v, &q, 8);
+  } else if constexpr (B == 4) {
+    const unsigned q = __ldg(reinterpret_cast<const unsigned*>(p));
+    memcpy(v, &q, 4);
+  } else {
+#pragma unroll
+    for (int j = 0; j < S; ++j) v[j] = __ldg(p + j);
+  }
+}
+
+// The x pass with each row staged in polyphase order relative to the first
+// tap: input e sits in phase (e - C0) mod S at index (e - C0) div S, phases
+// LS elements apart.  A lane loads S consecutive inputs as one vector and
+// stores each to its own phase at the lane's index (no bank conflicts), and
+// tap t of interior output o sits at phase t mod S, index o + t div S: every
+// staged address is a compile-time offset from the lane's column, so neither
+// the staging nor the taps need address arithmetic.  Taps are summed in tap
+// order as in k_resample_x_si, so the outputs are the same.  Rows of at most
+// kPPMaxIn inputs; edge outputs read the table.
+template <int S, typename Tin, typename A, typename Tout>
+__global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_pp(
+    const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out, int nrows, int nx_in,
+    int nx_out, const double* __restrict__ w, const int32_t* __restrict__ idx) {
+  constexpr int NP = 4 * S + 2;
+  constexpr int C0 = kPPFirstTap<S>;
+  constexpr int LS = kPPMaxIn / S + 2;   // covers index (kPPMaxIn - 1 - C0) div S
+  __shared__ A stage[kStageWarps][S * LS];
+  A* buf = stage[threadIdx.y];
+  const int lane = threadIdx.x;
+  const int ngroups = nx_in / S;
+  for (int row = blockIdx.x * kStageWarps + threadIdx.y; row < nrows; row += gridDim.x * kStageWarps) {
+    const Tin* src = in + (size_t)row * nx_in;
+    // U groups per lane in flight (16 S-element vectors per warp row and step)
+    constexpr int U = 16 / S;
+    for (int m0 = 0; m0 < ngroups; m0 += 32 * U) {
+      Tin v[U][S];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int m = m0 + 32 * u + lane;
+        if (m < ngroups) load_group<Tin, S>(src + (size_t)S * m, v[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int m = m0 + 32 * u + lane;
+        if (m < ngroups) {
+#pragma unroll
+          for (int j = 0; j < S; ++j) {
+            const int pj = ((j - C0) % S + S) % S;                       // phase of input S m + j
+            const int qj = (j - C0 >= 0) ? (j - C0) / S : -((C0 - j + S - 1) / S);
+            buf[pj * LS + m + qj] = (A)v[u][j];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    Tout* dst = out + (size_t)row * nx_out;
+    for (int xo = lane; xo < nx_out; xo += 32) {
+      A acc = 0;
+      if (xo >= si.lo && xo < si.hi) {
+        const A* b = buf + xo;
+#pragma unroll
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), b[(t % S) * LS + t / S]);
+      } else {
+        for (int t = 0; t < NP; ++t)
+          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo), (A)__ldg(src + __ldg(idx + (size_t)t * nx_out + xo)));
+      }
+      dst[xo] = (Tout)acc;
+    }
+    __syncwarp();
+  }
+}
+
 // The x pass of a uint8 mask in float64, exact.  In a row holding only 0 and
 // 1, a tap with 0 adds an exact zero and a tap with 1 adds its weight, so an
 // output is the tap-order float64 sum of the weights of its set taps: 0 when
 // none is set, si.wsum (the same sum over every tap) when all are; only
 // windows that are mixed sum their taps.  Rows with other values take the
 // plain product sums.  The row is staged as bytes plus ballot words and
-// their prefix popcounts.
+// their prefix popcounts.  Rows whose length is a multiple of 32 (row starts
+// 16-byte aligned) load each 32-input word as two 16-byte vectors in one lane
+// and build its bits with per-byte compares; other rows load bytes and ballot.
+// Per warp: the row bytes (rounded up to 16), then the words and prefixes
+// (rounded up to 16 bytes): mask_stage_bytes.
+__host__ __device__ inline size_t mask_stage_bytes(int nx_in) {
+  const size_t nwords = ((size_t)nx_in + 31) / 32;
+  return ((size_t)nx_in + 15) / 16 * 16 + (8 * (nwords + 1) + 15) / 16 * 16;
+}
+
 template <int S>
 __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
     const __grid_constant__ SITaps si, const uint8_t* __restrict__ in, double* __restrict__ out, int nrows,
@@ -275,7 +375,8 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
   extern __shared__ __align__(16) unsigned char stage_raw[];
   const int nwords = (nx_in + 31) / 32;
   const int row_bytes = (nx_in + 15) & ~15;
-  unsigned char* base = stage_raw + (size_t)threadIdx.y * (row_bytes + 8 * (nwords + 1));
+  unsigned char* base = stage_raw + (size_t)threadIdx.y * mask_stage_bytes(nx_in);
+  const bool vec = (nx_in & 31) == 0 && ((uintptr_t)in & 15) == 0;
   uint8_t* bytes = base;
   unsigned* words = reinterpret_cast<unsigned*>(base + row_bytes);
   unsigned* prefix = words + nwords + 1;   // set taps before word k
@@ -286,20 +387,39 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
     bool nonbinary = false;
     for (int k0 = 0; k0 < nwords; k0 += 32) {
       // lane j ends with word k0 + j: bit i = element (k0 + j) * 32 + i is set
-      uint8_t v[32];
-#pragma unroll
-      for (int b = 0; b < 32; ++b) {
-        const int e = (k0 + b) * 32 + lane;
-        v[b] = e < nx_in ? __ldg(src + e) : (uint8_t)0;
-      }
       unsigned mine = 0;
+      if (vec) {
+        const int kw = k0 + lane;
+        if (kw < nwords) {
+          const uint4* p = reinterpret_cast<const uint4*>(src + 32 * (size_t)kw);
+          const uint4 q0 = __ldg(p), q1 = __ldg(p + 1);
+          const unsigned c[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
-      for (int b = 0; b < 32; ++b) {
-        const int e = (k0 + b) * 32 + lane;
-        if (e < nx_in) bytes[e] = v[b];
-        nonbinary |= v[b] > 1;
-        const unsigned wv = __ballot_sync(0xffffffffu, v[b] != 0);
-        if (lane == b) mine = wv;
+          for (int j = 0; j < 8; ++j) {
+            // bytes 0..3 of chunk j (elements 4j .. 4j + 3): nonzero flags to bits 4j .. 4j + 3
+            const unsigned nz = __vcmpne4(c[j], 0u) & 0x01010101u;
+            mine |= ((nz * 0x01020408u) >> 24) << (4 * j);
+            nonbinary |= __vcmpgtu4(c[j], 0x01010101u) != 0u;
+          }
+          uint4* d = reinterpret_cast<uint4*>(bytes + 32 * kw);
+          d[0] = q0;
+          d[1] = q1;
+        }
+      } else {
+        uint8_t v[32];
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const int e = (k0 + b) * 32 + lane;
+          v[b] = e < nx_in ? __ldg(src + e) : (uint8_t)0;
+        }
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const int e = (k0 + b) * 32 + lane;
+          if (e < nx_in) bytes[e] = v[b];
+          nonbinary |= v[b] > 1;
+          const unsigned wv = __ballot_sync(0xffffffffu, v[b] != 0);
+          if (lane == b) mine = wv;
+        }
       }
       const int k = k0 + lane;
       const unsigned c = __popc(mine);
@@ -403,6 +523,49 @@ __global__ void k_resample_y_si(const __grid_constant__ SITaps si, const Tin* __
 #pragma unroll
         for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), v[t]);
         dst[x] = (Tout)acc;
+      }
+    } else {
+      const double* wr = w + (size_t)yo * NP;
+      const int32_t* ir = idx + (size_t)yo * NP;
+      WR_FOR_COLS(nx, x) {
+        A acc = 0;
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, __ldg(wr + t), (A)__ldg(plane + (size_t)__ldg(ir + t) * nx + x));
+        dst[x] = (Tout)acc;
+      }
+    }
+  }
+}
+
+// The y pass with V adjacent columns per lane: each tap row is one vector
+// load of V inputs (V times fewer loads in flight for the same bytes), the V
+// outputs summed in tap order as in k_resample_y_si.  Rows whose length is a
+// multiple of V with the row starts aligned to V elements; edge output rows
+// read the table.
+template <int S, int V, typename Tin, typename A, typename Tout>
+__global__ void k_resample_y_si_v(const __grid_constant__ SITaps si, const Tin* __restrict__ in,
+                                  Tout* __restrict__ out, int nz, int ny_in, int ny_out, int nx,
+                                  const double* __restrict__ w, const int32_t* __restrict__ idx) {
+  constexpr int NP = 4 * S + 2;
+  const int ng = nx / V;
+  WR_FOR_ROWS(nz * ny_out, row) {
+    const int z = row / ny_out, yo = row - z * ny_out;
+    const Tin* plane = in + (size_t)z * ny_in * nx;
+    Tout* dst = out + (size_t)row * nx;
+    if (yo >= si.lo && yo < si.hi) {
+      const Tin* r0 = plane + (size_t)(S * yo + si.c0) * nx;
+      WR_FOR_COLS(ng, xg) {
+        A acc[V];
+#pragma unroll
+        for (int c = 0; c < V; ++c) acc[c] = 0;
+#pragma unroll
+        for (int t = 0; t < NP; ++t) {
+          Tin v[V];
+          load_group<Tin, V>(r0 + (size_t)t * nx + V * xg, v);
+#pragma unroll
+          for (int c = 0; c < V; ++c) acc[c] = Acc<A>::madd(acc[c], Acc<A>::si_weight(si, t), (A)v[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < V; ++c) dst[V * xg + c] = (Tout)acc[c];
       }
     } else {
       const double* wr = w + (size_t)yo * NP;
@@ -551,7 +714,7 @@ __global__ void k_mask_bits_u8x4(const uint8_t* __restrict__ mref_u8, const uint
       if (keep_ref_bit) b = __ldg(reinterpret_cast<const unsigned*>(bits + i)) & 0x01010101u;
       else if (mref_u8) {
         const unsigned r = __ldg(reinterpret_cast<const unsigned*>(mref_u8 + i));
-        for (int j = 0; j < 4; ++j) b |= ((r >> (8 * j)) & 0xffu) ? (1u << (8 * j)) : 0u;
+        b = __vcmpne4(r, 0u) & 0x01010101u;   // bit 0 of each byte: nonzero
       }
       if (mmov) {
         // per row of the cell (y, z), (y+1, z), (y, z+1), (y+1, z+1): 4 nonzero flags in bits 0..3
@@ -561,8 +724,8 @@ __global__ void k_mask_bits_u8x4(const uint8_t* __restrict__ mref_u8, const uint
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
           const unsigned v = __ldg(reinterpret_cast<const unsigned*>(mmov + i + offs[r]));
-          unsigned f = 0;
-          for (int j = 0; j < 4; ++j) f |= ((v >> (8 * j)) & 0xffu) ? (1u << j) : 0u;
+          // nonzero flags of bytes 0..3 gathered into bits 0..3
+          const unsigned f = ((__vcmpne4(v, 0u) & 0x01010101u) * 0x01020408u) >> 24;
           unsigned nxt = __shfl_down_sync(0xffffffffu, f, 1) & 1u;          // next lane's first element
           if (lane == 31) nxt = __ldg(mmov + ahead + offs[r]) != 0 ? 1u : 0u;
           if (x + 4 >= nx) nxt = (f >> 3) & 1u;                             // edge clamp
@@ -1141,8 +1304,25 @@ __device__ __forceinline__ void decide_body(LKState* st, const double* __restric
                                             double sps, int level, int it, int iter, double tol, int forced) {
   if (!st->active) return;
   __shared__ double red[2][1024];
+  // each thread's chain errpart[t] + errpart[t + blockDim] + ... in index
+  // order, eight loads issued ahead of their additions
   double e = 0.0, p = 0.0;
-  for (long long i = threadIdx.x; i < nblk; i += blockDim.x) {
+  const long long step = blockDim.x;
+  long long i = threadIdx.x;
+  for (; i + 7 * step < nblk; i += 8 * step) {
+    double ev[8], pv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      ev[k] = errpart[i + k * step];
+      pv[k] = penpart[i + k * step];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      e += ev[k];
+      p += pv[k];
+    }
+  }
+  for (; i < nblk; i += step) {
     e += errpart[i];
     p += penpart[i];
   }
