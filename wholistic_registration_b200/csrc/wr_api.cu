@@ -240,7 +240,8 @@ static bool resample_x_si(const SITaps& si, const Tin* in, Tout* out, int nrows,
     smem = (size_t)kStageWarps * mask_stage_bytes(nx_in);
     kern = k_resample_x_mask<S>;
   } else {
-    if (si.c0 == kPPFirstTap<S> && nx_in <= kPPMaxIn && aligned(in, S * sizeof(Tin))) {
+    if (si.c0 == kPPFirstTap<S> && nx_in <= kPPMaxIn && si.lo + (nx_out - si.hi) <= kPPMaxEdge &&
+        aligned(in, S * sizeof(Tin))) {
       // rows staged relative to the first tap, static shared memory
       long long g = (nrows + kStageWarps - 1) / kStageWarps;
       if (g > 148LL * 32) g = 148LL * 32;
@@ -375,10 +376,14 @@ static void build_pyramid(const Plan& P, void* ws, const T* mov, const T* ref, c
     }
     // one exclusion mask for both volumes: its resize is already in levd
     if (mref_u8 && !reuse_ref && !same_mask) resize_to_level<uint8_t, double, double>(P, L, ws, mref_u8, 1, 0, tmpd, levd, s);
-    if (any_mask)
+    const double* mref_lev = (mref_u8 && !reuse_ref) ? levd : nullptr;
+    const float* mmov_lev = mmov_u8 ? mmov : nullptr;
+    if (any_mask && L.nx % 4 == 0 && aligned(mref_lev, 16) && aligned(mmov_lev, 16))
+      k_mask_bits_f4<<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(mref_lev, mmov_lev, bits, L.nz, L.ny,
+                                                                           L.nx, reuse_ref ? 1 : 0);
+    else if (any_mask)
       k_mask_bits<float><<<row_grid((long long)L.nz * L.ny), kRowBlock, 0, s>>>(
-          (mref_u8 && !reuse_ref) ? levd : nullptr, nullptr, mmov_u8 ? mmov : nullptr, nullptr, bits, L.nz, L.ny, L.nx,
-          reuse_ref ? 1 : 0);
+          mref_lev, nullptr, mmov_lev, nullptr, bits, L.nz, L.ny, L.nx, reuse_ref ? 1 : 0);
   }
 }
 

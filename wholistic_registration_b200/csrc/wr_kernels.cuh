@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_si(
 // (utils/imresize.py:60-82 with width 4S; the host checks the table against it).
 template <int S> constexpr int kPPFirstTap = -(3 * S / 2) - 1;
 constexpr int kPPMaxIn = 1024;   // longest row of k_resample_x_pp
+constexpr int kPPMaxEdge = 16;   // most edge outputs of a k_resample_x_pp row
 
 // S consecutive inputs as one vector load (the row start and S * sizeof(T)
 // are multiples of the vector size).
@@ -297,7 +298,9 @@ __device__ __forceinline__ void load_group(const T* __restrict__ p, T (&v)[S]) {
 // staged address is a compile-time offset from the lane's column, so neither
 // the staging nor the taps need address arithmetic.  Taps are summed in tap
 // order as in k_resample_x_si, so the outputs are the same.  Rows of at most
-// kPPMaxIn inputs; edge outputs read the table.
+// kPPMaxIn inputs.  The few edge outputs (reflected taps) read the staged row
+// too: their weights and staged positions are tabulated in shared memory once
+// per block, so no output waits on global memory after the row is staged.
 template <int S, typename Tin, typename A, typename Tout>
 __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_pp(
     const __grid_constant__ SITaps si, const Tin* __restrict__ in, Tout* __restrict__ out, int nrows, int nx_in,
@@ -306,6 +309,19 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_pp(
   constexpr int C0 = kPPFirstTap<S>;
   constexpr int LS = kPPMaxIn / S + 2;   // covers index (kPPMaxIn - 1 - C0) div S
   __shared__ A stage[kStageWarps][S * LS];
+  __shared__ A edge_w[kPPMaxEdge * NP];
+  __shared__ int edge_pos[kPPMaxEdge * NP];
+  // edge outputs: o < lo (k = o) and o >= hi (k = lo + o - hi); the host
+  // checks that there are at most kPPMaxEdge
+  const int nedge = si.lo + (nx_out - si.hi);
+  for (int q = threadIdx.y * 32 + threadIdx.x; q < nedge * NP; q += 32 * kStageWarps) {
+    const int k = q / NP, t = q - k * NP;
+    const int o = k < si.lo ? k : si.hi + (k - si.lo);
+    edge_w[q] = (A)__ldg(w + (size_t)t * nx_out + o);
+    const int d = __ldg(idx + (size_t)t * nx_out + o) - C0;   // >= 0: C0 < 0 <= idx
+    edge_pos[q] = (d % S) * LS + d / S;
+  }
+  __syncthreads();
   A* buf = stage[threadIdx.y];
   const int lane = threadIdx.x;
   const int ngroups = nx_in / S;
@@ -342,8 +358,8 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_pp(
 #pragma unroll
         for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, Acc<A>::si_weight(si, t), b[(t % S) * LS + t / S]);
       } else {
-        for (int t = 0; t < NP; ++t)
-          acc = Acc<A>::madd(acc, __ldg(w + (size_t)t * nx_out + xo), (A)__ldg(src + __ldg(idx + (size_t)t * nx_out + xo)));
+        const int k = xo < si.lo ? xo : si.lo + (xo - si.hi);
+        for (int t = 0; t < NP; ++t) acc = Acc<A>::madd(acc, edge_w[k * NP + t], buf[edge_pos[k * NP + t]]);
       }
       dst[xo] = (Tout)acc;
     }
@@ -742,6 +758,56 @@ __global__ void k_mask_bits_u8x4(const uint8_t* __restrict__ mref_u8, const uint
           mf[j] = (fl[0] >> j) & 1u ? 1.f : 0.f;
         }
         if (mmov_f && x < nx) *reinterpret_cast<float4*>(mmov_f + base + x) = make_float4(mf[0], mf[1], mf[2], mf[3]);
+      }
+      if (x < nx) *reinterpret_cast<unsigned*>(bits + base + x) = b;
+    }
+  }
+}
+
+// k_mask_bits for levels >= 1 (float64 reference mask, float moving mask)
+// with four voxels per lane (nx a multiple of 4, rows 16-byte aligned): the
+// same bits, with 16-byte loads and the x + 1 corners from the next lane.
+__global__ void k_mask_bits_f4(const double* __restrict__ mref_d, const float* __restrict__ mmov,
+                               uint8_t* __restrict__ bits, int nz, int ny, int nx, int keep_ref_bit) {
+  const int lane = threadIdx.x;
+  WR_FOR_ROWS(nz * ny, row) {
+    const int z = row / ny, y = row - z * ny;
+    const size_t base = (size_t)row * nx;
+    const size_t dy = (size_t)(min(y + 1, ny - 1) - y) * nx, dz = (size_t)(min(z + 1, nz - 1) - z) * nx * ny;
+    for (int x0 = 0; x0 < nx; x0 += 128) {
+      const int x = x0 + 4 * lane, xc = min(x, nx - 4);
+      const size_t i = base + xc;
+      unsigned b = 0;
+      if (keep_ref_bit) {
+        b = __ldg(reinterpret_cast<const unsigned*>(bits + i)) & 0x01010101u;
+      } else if (mref_d) {
+        const double2 r0 = __ldg(reinterpret_cast<const double2*>(mref_d + i));
+        const double2 r1 = __ldg(reinterpret_cast<const double2*>(mref_d + i) + 1);
+        b = (r0.x > 0.0 ? 1u : 0u) | (r0.y > 0.0 ? 0x100u : 0u) | (r1.x > 0.0 ? 0x10000u : 0u) |
+            (r1.y > 0.0 ? 0x1000000u : 0u);
+      }
+      if (mmov) {
+        // per row of the cell (y, z), (y+1, z), (y, z+1), (y+1, z+1): 4 flags in bits 0..3
+        unsigned fl[4];
+        const size_t offs[4] = {0, dy, dz, dz + dy};
+        const size_t ahead = base + min(x0 + 128, nx - 1);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(mmov + i + offs[r]));
+          const unsigned f = (v.x > 0.f ? 1u : 0u) | (v.y > 0.f ? 2u : 0u) | (v.z > 0.f ? 4u : 0u) | (v.w > 0.f ? 8u : 0u);
+          unsigned nxt = __shfl_down_sync(0xffffffffu, f, 1) & 1u;          // next lane's first element
+          if (lane == 31) nxt = __ldg(mmov + ahead + offs[r]) > 0.f ? 1u : 0u;
+          if (x + 4 >= nx) nxt = (f >> 3) & 1u;                             // edge clamp
+          fl[r] = f | (nxt << 4);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const unsigned pair = 3u << j;   // columns j, j+1
+          const unsigned any = (fl[0] | fl[1] | fl[2] | fl[3]) & pair;
+          const unsigned all = (fl[0] & fl[1] & fl[2] & fl[3]) & pair;
+          const unsigned code = any == 0 ? 0u : (all == pair ? 1u : 2u);
+          b |= code << (8 * j + 1);
+        }
       }
       if (x < nx) *reinterpret_cast<unsigned*>(bits + base + x) = b;
     }
@@ -1304,25 +1370,8 @@ __device__ __forceinline__ void decide_body(LKState* st, const double* __restric
                                             double sps, int level, int it, int iter, double tol, int forced) {
   if (!st->active) return;
   __shared__ double red[2][1024];
-  // each thread's chain errpart[t] + errpart[t + blockDim] + ... in index
-  // order, eight loads issued ahead of their additions
   double e = 0.0, p = 0.0;
-  const long long step = blockDim.x;
-  long long i = threadIdx.x;
-  for (; i + 7 * step < nblk; i += 8 * step) {
-    double ev[8], pv[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      ev[k] = errpart[i + k * step];
-      pv[k] = penpart[i + k * step];
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      e += ev[k];
-      p += pv[k];
-    }
-  }
-  for (; i < nblk; i += step) {
+  for (long long i = threadIdx.x; i < nblk; i += blockDim.x) {
     e += errpart[i];
     p += penpart[i];
   }
