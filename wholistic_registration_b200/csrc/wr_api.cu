@@ -237,7 +237,7 @@ static bool resample_x_si(const SITaps& si, const Tin* in, Tout* out, int nrows,
   void (*kern)(const SITaps, const Tin*, Tout*, int, int, int, const double*, const int32_t*);
   if constexpr (std::is_same<Tin, uint8_t>::value && std::is_same<A, double>::value &&
                 std::is_same<Tout, double>::value) {
-    smem = (size_t)kStageWarps * mask_stage_bytes(nx_in);
+    smem = (size_t)kStageWarps * mask_stage_bytes(nx_in) + mask_edge_bytes<S>();
     kern = k_resample_x_mask<S>;
   } else {
     if (si.c0 == kPPFirstTap<S> && nx_in <= kPPMaxIn && si.lo + (nx_out - si.hi) <= kPPMaxEdge &&

@@ -377,11 +377,14 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_pp(
 // 16-byte aligned) load each 32-input word as two 16-byte vectors in one lane
 // and build its bits with per-byte compares; other rows load bytes and ballot.
 // Per warp: the row bytes (rounded up to 16), then the words and prefixes
-// (rounded up to 16 bytes): mask_stage_bytes.
+// (rounded up to 16 bytes): mask_stage_bytes; after the warps' stages, the
+// edge table: mask_edge_bytes.
 __host__ __device__ inline size_t mask_stage_bytes(int nx_in) {
   const size_t nwords = ((size_t)nx_in + 31) / 32;
   return ((size_t)nx_in + 15) / 16 * 16 + (8 * (nwords + 1) + 15) / 16 * 16;
 }
+template <int S>
+constexpr size_t mask_edge_bytes() { return (size_t)kPPMaxEdge * (4 * S + 2) * (8 + 4); }
 
 template <int S>
 __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
@@ -396,6 +399,22 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
   uint8_t* bytes = base;
   unsigned* words = reinterpret_cast<unsigned*>(base + row_bytes);
   unsigned* prefix = words + nwords + 1;   // set taps before word k
+  // edge outputs (o < lo: k = o; o >= hi: k = lo + o - hi) read the staged
+  // bytes through a per-block table of weights and input positions when
+  // there are at most kPPMaxEdge of them (after the per-warp stages)
+  double* edge_w = reinterpret_cast<double*>(stage_raw + (size_t)kStageWarps * mask_stage_bytes(nx_in));
+  int* edge_i = reinterpret_cast<int*>(edge_w + kPPMaxEdge * NP);
+  const int nedge = si.lo + (nx_out - si.hi);
+  const bool edge_tab = nedge <= kPPMaxEdge;
+  if (edge_tab) {
+    for (int q = threadIdx.y * 32 + threadIdx.x; q < nedge * NP; q += 32 * kStageWarps) {
+      const int k = q / NP, t = q - k * NP;
+      const int o = k < si.lo ? k : si.hi + (k - si.lo);
+      edge_w[q] = __ldg(w + (size_t)t * nx_out + o);
+      edge_i[q] = __ldg(idx + (size_t)t * nx_out + o);
+    }
+  }
+  __syncthreads();
   const int lane = threadIdx.x;
   for (int row = blockIdx.x * kStageWarps + threadIdx.y; row < nrows; row += gridDim.x * kStageWarps) {
     const uint8_t* src = in + (size_t)row * nx_in;
@@ -474,6 +493,10 @@ __global__ void __launch_bounds__(32 * kStageWarps) k_resample_x_mask(
               if (bytes[e0 + t]) acc = __dadd_rn(acc, si.w[t]);
           }
         }
+      } else if (edge_tab) {
+        const int k = xo < si.lo ? xo : si.lo + (xo - si.hi);
+        for (int t = 0; t < NP; ++t)
+          acc = __dadd_rn(acc, __dmul_rn(edge_w[k * NP + t], (double)bytes[edge_i[k * NP + t]]));
       } else {
         for (int t = 0; t < NP; ++t)
           acc = __dadd_rn(acc, __dmul_rn(__ldg(w + (size_t)t * nx_out + xo),
