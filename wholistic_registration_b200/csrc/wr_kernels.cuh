@@ -1848,10 +1848,13 @@ __device__ __forceinline__ float warp_sample(const T* __restrict__ src, int nx, 
   const int xa = clampi(x0, 0, nx - 1), xb = clampi(x0 + 1, 0, nx - 1);
   const int ya = clampi(y0, 0, ny - 1), yb = clampi(y0 + 1, 0, ny - 1);
   const int za = clampi(z0, 0, nz - 1), zb = clampi(z0 + 1, 0, nz - 1);
-  const double c000 = load_f<T>(src, za * sz + ya * sy + xa), c001 = load_f<T>(src, za * sz + ya * sy + xb);
-  const double c010 = load_f<T>(src, za * sz + yb * sy + xa), c011 = load_f<T>(src, za * sz + yb * sy + xb);
-  const double c100 = load_f<T>(src, zb * sz + ya * sy + xa), c101 = load_f<T>(src, zb * sz + ya * sy + xb);
-  const double c110 = load_f<T>(src, zb * sz + yb * sy + xa), c111 = load_f<T>(src, zb * sz + yb * sy + xb);
+  // one base address and the three tap offsets (0 where a tap is clamped)
+  const T* p = src + (za * sz + ya * sy + xa);
+  const size_t ox = (size_t)(xb - xa), oy = (size_t)(yb - ya) * sy, oz = (size_t)(zb - za) * sz;
+  const double c000 = load_f<T>(p, 0), c001 = load_f<T>(p, ox);
+  const double c010 = load_f<T>(p, oy), c011 = load_f<T>(p, oy + ox);
+  const double c100 = load_f<T>(p, oz), c101 = load_f<T>(p, oz + ox);
+  const double c110 = load_f<T>(p, oz + oy), c111 = load_f<T>(p, oz + oy + ox);
   const double wx0 = 1.0 - tx, wy0 = 1.0 - ty, wz0 = 1.0 - tz;
   const double v = wx0 * wy0 * wz0 * c000 + tx * wy0 * wz0 * c001 + wx0 * ty * wz0 * c010 + tx * ty * wz0 * c011 +
                    wx0 * wy0 * tz * c100 + tx * wy0 * tz * c101 + wx0 * ty * tz * c110 + tx * ty * tz * c111;
