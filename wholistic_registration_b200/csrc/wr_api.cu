@@ -786,11 +786,13 @@ static void launch_batch(int mode, int diff0, const BatchIter& b, long long ntil
 }
 
 // Tiles from which a frame-level of a batch takes its own launch of the
-// single-volume iteration kernel: eight rounds of a full-GPU persistent grid.
-// Smaller frame-levels share one launch (k_lk_accumulate_batch), which fills
-// the GPU with several frames but reads each frame's parameters by a runtime
-// index (11 % more instructions per voxel, measured on an uneven batch).
-constexpr long long kOwnLaunchTiles = 8LL * 148 * 4;
+// single-volume iteration kernel: four rounds of a full-GPU persistent grid
+// (1184 and 4736 measured the same on the uneven batch, 4736 2 % slower on 16
+// frames of 64x256x256).  Smaller frame-levels share one launch
+// (k_lk_accumulate_batch), which fills the GPU with several frames but reads
+// each frame's parameters by a runtime index (11 % more instructions per
+// voxel, measured on an uneven batch).
+constexpr long long kOwnLaunchTiles = 4LL * 148 * 4;
 
 // Frames may differ in shape, patch radius, number of levels, iterations and
 // every other solver parameter except the precision and the launch-shape
