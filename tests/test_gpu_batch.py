@@ -218,3 +218,24 @@ def test_batch_holds_64_frames():
         torch.testing.assert_close(motions[i], alone, rtol=0, atol=0)
     with pytest.raises(ValueError):
         BatchRegistrar([(4, 48, 40)] * 65, plist[0])
+
+
+def test_batch_mixing_own_launches_and_shared_launches():
+    """A frame-level with enough tiles takes its own launch of the
+    single-volume kernel inside the batched call, smaller ones share the
+    batched launch (level 0 of the first frame: 16 x 52 x 52 tiles of 5 x 5);
+    both give exactly the frames' results alone."""
+    _need()
+    from wholistic_registration_b200.batch import BatchRegistrar
+
+    shapes = [(16, 256, 256), (8, 64, 64), (12, 128, 96)]
+    frames = _frames(90, shapes)
+    plist = [_params(r=2, layer=2, iter=6), _params(r=4, layer=1, iter=6), _params(r=3, layer=2, iter=5)]
+    br = BatchRegistrar(shapes, plist, warp=True)
+    motions, warps = br.register([f[1] for f in frames], [f[0] for f in frames], [f[2] for f in frames],
+                                 [f[2] for f in frames])
+    for i, (f, p) in enumerate(zip(frames, plist)):
+        ref_m, ref_w, ref_e = _alone([f], p, warp=True)
+        torch.testing.assert_close(motions[i], ref_m[0], rtol=0, atol=0)
+        torch.testing.assert_close(warps[i], ref_w[0], rtol=0, atol=0)
+        assert [br.stats()[i].evals[l] for l in range(p.layer + 1)] == ref_e[0]
